@@ -1,0 +1,791 @@
+// efvm_api.cu — the C-ABI of include/efvm.h: context lifecycle, device
+// memory, the per-substage phase order of one app.run(), CUDA-graph captured
+// RK3 steps, strided state upload/download and the IBM geometry set-up.
+//
+// The IBM geometry that the reference rebuilds every substage (ghost list,
+// image points, markers; crates/cfd_ibm/src/lib.rs:155-254,566-598) is static
+// for a fixed body, so it is built once per efvm_set_cylinders: the solid mask
+// on the device, the ghost list and marker sample points on the host with the
+// same one-rounding-per-operation arithmetic as the reference's Rust.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "efvm_internal.h"
+
+using namespace efvm;
+
+struct efvm_ctx {
+    efvm_grid grid;
+    efvm_params params;
+    Geometry g;
+    Physics ph;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double* U[3] = {nullptr, nullptr, nullptr};  // U0 (= u^n), U1, U2
+    uint8_t* mask = nullptr;
+    double* yw = nullptr;                          // viscous y weights
+    DevState* st = nullptr;                        // device
+    double* partial = nullptr;                     // reduction partials
+    int n_partial = 0;
+    double* staging = nullptr;
+    size_t staging_bytes = 0;
+    // host mirror of the RK state machine (the device holds the authoritative clock)
+    int rk_stage = 0;
+    int euler_cur = 0;  // Euler ping-pong buffer index
+    bool lam_stale = true;
+    bool ghosts_stale = true;
+    bool control_dirty = true;
+    // IBM
+    bool ibm = false;
+    bool geom_dirty = false;
+    std::vector<double> cyl_host;  // cx, cy, r per body
+    double stagnant[5] = {0, 0, 0, 0, 0};  // MaskConsts.stagnant
+    double ambient[5] = {0, 0, 0, 0, 0};   // MaskConsts.ambient
+    double* cyl_dev = nullptr;
+    IbmGhostDev* ghosts_dev = nullptr;
+    MarkerDev* markers_dev = nullptr;
+    double* zg0 = nullptr;
+    double* zfill = nullptr;
+    double* force_out = nullptr;
+    double* force_partials = nullptr;
+    unsigned int* force_counter = nullptr;
+    double* history = nullptr;
+    long long history_cap = 0;
+    Ibm ibm_desc{};
+    int64_t n_solid = 0;
+    // CUDA graph of one RK3 step
+    cudaGraphExec_t graph_exec = nullptr;
+    bool graph_valid = false;
+    bool graph_with_history = false;
+    int graph_kernels = 0;
+    uint64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(efvm_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                     \
+    do {                                                                                        \
+        cudaError_t e__ = (call);                                                               \
+        if (e__ != cudaSuccess)                                                                 \
+            return fail(ctx, e__ == cudaErrorMemoryAllocation ? EFVM_ERR_OOM : EFVM_ERR_CUDA,   \
+                        std::string(#call) + ": " + cudaGetErrorString(e__));                   \
+    } while (0)
+
+// Host arithmetic with one rounding per operation (built with -ffp-contract=off).
+double centre_h(double lo, double h, int i) { return lo + ((double)i + 0.5) * h; }
+
+// FIELD locate() restricted to x/y (see the oracle header for the inferred rule):
+// f = (p - lo)/h - 0.5, low corner floor(f), fraction f - floor(f); valid when
+// the 2x2 block stays inside the raw array (ghosts included).
+bool locate_h(const Geometry& g, double px, double py, int& li, int& lj, double& tx, double& ty) {
+    const double fx = (px - g.lo[0]) / g.h[0] - 0.5;
+    const double fy = (py - g.lo[1]) / g.h[1] - 0.5;
+    const double flx = std::floor(fx), fly = std::floor(fy);
+    li = (int)flx;
+    lj = (int)fly;
+    tx = fx - flx;
+    ty = fy - fly;
+    const bool okx = li + NG >= 0 && li + NG + 1 < g.nx + 2 * NG;
+    const bool oky = lj + NG >= 0 && lj + NG + 1 < g.ny + 2 * NG;
+    return okx && oky;
+}
+
+cudaStream_t S(efvm_ctx* c) { return c->stream; }
+
+double* cur_buf(efvm_ctx* c) {
+    if (c->params.integrator == EFVM_INTEGRATOR_EULER) return c->U[c->euler_cur];
+    return c->U[c->rk_stage];
+}
+
+int ensure_staging(efvm_ctx* c, size_t bytes) {
+    if (c->staging_bytes >= bytes) return EFVM_OK;
+    if (c->staging) cudaFree(c->staging);
+    c->staging = nullptr;
+    c->staging_bytes = 0;
+    CUDA_TRY(c, cudaMalloc(&c->staging, bytes));
+    c->staging_bytes = bytes;
+    return EFVM_OK;
+}
+
+int sync_control(efvm_ctx* c, int stop_at_t, double t_stop, long long hist_cap) {
+    c->launches += launch_set_control(c->st, 1, stop_at_t, t_stop, hist_cap, S(c));
+    c->control_dirty = stop_at_t != 0 || hist_cap != 0;
+    return EFVM_OK;
+}
+
+// Build the IBM ghost list and marker sample points after the device mask flip.
+int build_ibm_lists(efvm_ctx* c) {
+    const Geometry& g = c->g;
+    std::vector<uint8_t> m((size_t)g.nx * g.ny);
+    CUDA_TRY(c, cudaMemcpy2DAsync(m.data(), g.nx, c->mask + (size_t)YO * g.pitch + XO, g.pitch, g.nx, g.ny,
+                                  cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    const int ncyl = (int)(c->cyl_host.size() / 3);
+    std::vector<IbmGhostDev> ghosts;
+    c->n_solid = 0;
+    for (int j = 0; j < g.ny; ++j)
+        for (int i = 0; i < g.nx; ++i) {
+            if (!m[(size_t)j * g.nx + i]) continue;
+            ++c->n_solid;
+            // compute_cylinder_ghosts, crates/cfd_ibm/src/lib.rs:187-254: a solid cell
+            // with >= 1 non-solid face neighbour.  The 2-D mesh's two z neighbours are
+            // ghost layers, which are never solid, so every solid cell qualifies.
+            const double cc[2] = {centre_h(g.lo[0], g.h[0], i), centre_h(g.lo[1], g.h[1], j)};
+            double best_abs = std::numeric_limits<double>::max(), best_signed = 0.0;
+            double nrm[2] = {1.0, 0.0};
+            for (int b = 0; b < ncyl; ++b) {
+                const double dx = cc[0] - c->cyl_host[3 * b], dy = cc[1] - c->cyl_host[3 * b + 1];
+                const double r = std::sqrt(dx * dx + dy * dy);
+                const double s = r - c->cyl_host[3 * b + 2];
+                if (std::fabs(s) < best_abs) {
+                    best_abs = std::fabs(s);
+                    best_signed = s;
+                    if (r < 1e-12) { nrm[0] = 1.0; nrm[1] = 0.0; }
+                    else { nrm[0] = dx / r; nrm[1] = dy / r; }
+                }
+            }
+            const double push = 2.0 * (-best_signed);
+            const double ip[2] = {cc[0] + push * nrm[0], cc[1] + push * nrm[1]};
+            IbmGhostDev gh{};
+            gh.cell = (long long)j * g.nx + i;
+            gh.valid = locate_h(g, ip[0], ip[1], gh.lo_i, gh.lo_j, gh.tx, gh.ty) ? 1 : 0;
+            ghosts.push_back(gh);
+        }
+    // compute_cylinder_markers, crates/cfd_ibm/src/lib.rs:566-598 (n_theta = 64, n_z = 1)
+    std::vector<MarkerDev> markers;
+    const double PI = 3.141592653589793;
+    const double z_lo = centre_h(g.lo[2], g.h[2], 0) - 0.5 * g.h[2];
+    const double z_hi = centre_h(g.lo[2], g.h[2], 0) + 0.5 * g.h[2];
+    const double lz = z_hi - z_lo;
+    const int n_theta = 64, n_z = 1;
+    const double offset = g.h[0];  // marker_force_system: sample offset = spacing(0, 0)
+    for (int b = 0; b < ncyl; ++b) {
+        const double cx = c->cyl_host[3 * b], cy = c->cyl_host[3 * b + 1], r = c->cyl_host[3 * b + 2];
+        const double area = 2.0 * PI * r * lz / (double)(n_theta * n_z);
+        for (int it = 0; it < n_theta; ++it) {
+            const double theta = 2.0 * PI * ((double)it + 0.5) / (double)n_theta;
+            const double nx = std::cos(theta), ny = std::sin(theta);
+            MarkerDev mk{};
+            mk.normal[0] = nx;
+            mk.normal[1] = ny;
+            mk.normal[2] = 0.0;
+            mk.area = area;
+            const double px = cx + r * nx, py = cy + r * ny;
+            const double sx = px + offset * nx, sy = py + offset * ny;
+            mk.valid = locate_h(g, sx, sy, mk.lo_i, mk.lo_j, mk.tx, mk.ty) ? 1 : 0;
+            markers.push_back(mk);
+        }
+    }
+    if (c->ghosts_dev) cudaFree(c->ghosts_dev);
+    if (c->markers_dev) cudaFree(c->markers_dev);
+    if (c->zg0) cudaFree(c->zg0);
+    if (c->zfill) cudaFree(c->zfill);
+    c->ghosts_dev = nullptr;
+    c->markers_dev = nullptr;
+    c->zg0 = c->zfill = nullptr;
+    const size_t ng = std::max<size_t>(ghosts.size(), 1), nm = std::max<size_t>(markers.size(), 1);
+    CUDA_TRY(c, cudaMalloc(&c->ghosts_dev, ng * sizeof(IbmGhostDev)));
+    CUDA_TRY(c, cudaMalloc(&c->markers_dev, nm * sizeof(MarkerDev)));
+    if (c->force_partials) cudaFree(c->force_partials);
+    c->force_partials = nullptr;
+    const size_t nblocks = 1 + (ghosts.size() + 255) / 256;
+    CUDA_TRY(c, cudaMalloc(&c->force_partials, nblocks * 6 * sizeof(double)));
+    CUDA_TRY(c, cudaMalloc(&c->zg0, ng * 4 * sizeof(double)));
+    CUDA_TRY(c, cudaMalloc(&c->zfill, 3 * ng * 4 * sizeof(double)));
+    CUDA_TRY(c, cudaMemsetAsync(c->zg0, 0, ng * 4 * sizeof(double), S(c)));
+    CUDA_TRY(c, cudaMemsetAsync(c->zfill, 0, 3 * ng * 4 * sizeof(double), S(c)));
+    if (!ghosts.empty())
+        CUDA_TRY(c, cudaMemcpyAsync(c->ghosts_dev, ghosts.data(), ghosts.size() * sizeof(IbmGhostDev),
+                                    cudaMemcpyHostToDevice, S(c)));
+    if (!markers.empty())
+        CUDA_TRY(c, cudaMemcpyAsync(c->markers_dev, markers.data(), markers.size() * sizeof(MarkerDev),
+                                    cudaMemcpyHostToDevice, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    Ibm& d = c->ibm_desc;
+    d.enabled = 1;
+    d.n_ghost = (int)ghosts.size();
+    d.n_markers = (int)markers.size();
+    d.ghosts = c->ghosts_dev;
+    d.markers = c->markers_dev;
+    d.sample_offset = offset;
+    d.zg0 = c->zg0;
+    d.zfill = c->zfill;
+    d.force_out = c->force_out;
+    d.history = nullptr;
+    d.partials = c->force_partials;
+    d.counter = c->force_counter;
+    return EFVM_OK;
+}
+
+// Setup-phase work that precedes a step boundary's first stage, in the
+// reference's Setup order: CFL (SolverPlugin) before the geometry refresh
+// (CylinderIbmPlugin), then Halo/Boundary for a state that changed on the host.
+int prologue(efvm_ctx* c) {
+    if (c->rk_stage == 0 && c->lam_stale && c->ph.fixed_dt <= 0.0) {
+        c->launches += launch_cfl(c->g, c->ph, cur_buf(c), c->st, S(c));
+        c->lam_stale = false;
+    }
+    if (c->ibm && c->geom_dirty) {
+        c->launches += launch_geometry(c->g, c->cyl_dev, (int)(c->cyl_host.size() / 3), c->stagnant, c->ambient,
+                                       cur_buf(c), c->mask, S(c));
+        int rc = build_ibm_lists(c);
+        if (rc) return rc;
+        c->geom_dirty = false;
+        c->ghosts_stale = true;
+        c->graph_valid = false;
+    }
+    if (c->ghosts_stale) {
+        c->launches += launch_fill_ghosts(c->g, c->ph, cur_buf(c), S(c));
+        c->ghosts_stale = false;
+    }
+    return EFVM_OK;
+}
+
+// Launch the kernels of one substage at RK stage `stage` (0..2, or 3 = Euler).
+void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool with_setup) {
+    if (with_setup) c->launches += launch_step_setup(c->ph, c->st, S(c));
+    Ibm ib = c->ibm_desc;
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, uin, c->mask, c->st, stage, 1, 0, stage, S(c));
+    StageArgs a{};
+    a.g = c->g;
+    a.ph = c->ph;
+    a.uin = uin;
+    a.u0 = c->U[0];
+    a.uout = uout;
+    a.mask = c->ibm ? c->mask : nullptr;
+    a.yw = c->yw;
+    a.st = c->st;
+    a.stage = stage;
+    a.completes_step = (stage == 2 || stage == 3) ? 1 : 0;
+    a.want_cfl = a.completes_step && c->ph.fixed_dt <= 0.0;
+    c->launches += launch_stage(a, 0, 0, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, uout, c->mask, c->st, stage, 0, 1, stage, S(c));
+}
+
+int capture_step_graph(efvm_ctx* c) {
+    if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+    }
+    const uint64_t before = c->launches;
+    cudaGraph_t graph;
+    CUDA_TRY(c, cudaStreamBeginCapture(S(c), cudaStreamCaptureModeThreadLocal));
+    enqueue_substage(c, 0, c->U[0], c->U[1], true);
+    enqueue_substage(c, 1, c->U[1], c->U[2], false);
+    enqueue_substage(c, 2, c->U[2], c->U[0], false);
+    cudaError_t e = cudaStreamEndCapture(S(c), &graph);
+    c->graph_kernels = (int)(c->launches - before);
+    c->launches = before;
+    if (e != cudaSuccess) return fail(c, EFVM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(c, EFVM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    c->graph_valid = true;
+    return EFVM_OK;
+}
+
+int read_state(efvm_ctx* c, DevState& s) {
+    CUDA_TRY(c, cudaMemcpyAsync(&s, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    return EFVM_OK;
+}
+
+bool bc_supported(int k) { return k >= EFVM_BC_SUPERSONIC_OUTFLOW && k <= EFVM_BC_PRESSURE_OUTLET; }
+
+}  // namespace
+
+extern "C" {
+
+int efvm_abi_version(void) { return EFVM_ABI_VERSION; }
+
+const char* efvm_last_error(const efvm_ctx* ctx) {
+    if (ctx) return ctx->err.c_str();
+    return g_last_error.c_str();
+}
+
+int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out) {
+    if (!grid || !params || !out) return fail(nullptr, EFVM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    const efvm_grid& gr = *grid;
+    if (gr.nz != 1) return fail(nullptr, EFVM_ERR_UNSUPPORTED, "only 2-D meshes (nz == 1) are supported");
+    if (gr.ng != 2) return fail(nullptr, EFVM_ERR_UNSUPPORTED, "only ng == 2 ghost layers are supported");
+    if (gr.nx < 2 || gr.ny < 1) return fail(nullptr, EFVM_ERR_INVALID_ARG, "nx must be >= 2 and ny >= 1");
+    for (int a = 0; a < 3; ++a)
+        if (!(gr.hi[a] > gr.lo[a])) return fail(nullptr, EFVM_ERR_INVALID_ARG, "bounds_hi must exceed bounds_lo");
+    for (int a = 0; a < 3; ++a) {
+        const bool lo_p = gr.bc[2 * a].kind == EFVM_BC_PERIODIC, hi_p = gr.bc[2 * a + 1].kind == EFVM_BC_PERIODIC;
+        if (lo_p != hi_p)
+            return fail(nullptr, EFVM_ERR_INVALID_ARG,
+                        "invalid periodic boundary configuration: periodic boundary on axis " + std::to_string(a) +
+                            " requires both sides");
+    }
+    for (int s = 0; s < 6; ++s)
+        if (!bc_supported(gr.bc[s].kind)) return fail(nullptr, EFVM_ERR_INVALID_ARG, "unknown boundary kind");
+    if ((gr.bc[EFVM_XLO].kind == EFVM_BC_PERIODIC && gr.nx < 2) || (gr.bc[EFVM_YLO].kind == EFVM_BC_PERIODIC && gr.ny < 2))
+        return fail(nullptr, EFVM_ERR_INVALID_ARG, "a periodic axis needs at least 2 cells (two ghost layers wrap)");
+    if (gr.bc[EFVM_ZLO].kind == EFVM_BC_PERIODIC)
+        return fail(nullptr, EFVM_ERR_UNSUPPORTED, "a periodic z axis has no meaning on a 2-D mesh");
+    const efvm_params& p = *params;
+    if (!(p.gamma > 1.0) || !(p.r_gas > 0.0)) return fail(nullptr, EFVM_ERR_INVALID_ARG, "gamma must exceed 1, r_gas > 0");
+    if (!(p.cfl > 0.0) && !(p.fixed_dt > 0.0)) return fail(nullptr, EFVM_ERR_INVALID_ARG, "cfl or fixed_dt must be > 0");
+    if (p.flux_scheme < 0 || p.flux_scheme > 2 || p.reconstruction < 0 || p.reconstruction > 1 || p.limiter < 0 ||
+        p.limiter > 1 || p.integrator < 0 || p.integrator > 1 || p.precision < 0 || p.precision > 1 ||
+        p.periodic_seam < 0 || p.periodic_seam > 1 || p.viscosity_model < 0 || p.viscosity_model > 1)
+        return fail(nullptr, EFVM_ERR_INVALID_ARG, "enum field out of range");
+    if (p.sponge && !(p.sponge_x_end > p.sponge_x_start))
+        return fail(nullptr, EFVM_ERR_INVALID_ARG, "sponge_x_end must exceed sponge_x_start");
+
+    efvm_ctx* c = new efvm_ctx();
+    c->grid = gr;
+    c->params = p;
+    cudaGetDevice(&c->device);
+    Geometry& g = c->g;
+    g.nx = gr.nx;
+    g.ny = gr.ny;
+    g.pitch = ((XO + gr.nx + NG) + 7) / 8 * 8;
+    g.plane = ((long long)(gr.ny + 2 * YO) * g.pitch + 31) / 32 * 32;
+    const int n[3] = {gr.nx, gr.ny, gr.nz};
+    for (int a = 0; a < 3; ++a) {
+        g.lo[a] = gr.lo[a];
+        g.hi[a] = gr.hi[a];
+        g.h[a] = (gr.hi[a] - gr.lo[a]) / (double)n[a];
+    }
+    g.cell_volume = g.h[0] * g.h[1] * g.h[2];
+    g.inv_x = (g.h[1] * g.h[2]) / g.cell_volume;
+    g.inv_y = (g.h[0] * g.h[2]) / g.cell_volume;
+    Physics& ph = c->ph;
+    ph.gamma = p.gamma;
+    ph.r_gas = p.r_gas;
+    ph.cfl = p.cfl;
+    ph.fixed_dt = p.fixed_dt;
+    ph.flux_scheme = p.flux_scheme;
+    ph.reconstruction = p.reconstruction;
+    ph.limiter = p.limiter;
+    ph.integrator = p.integrator;
+    ph.viscous = p.viscous;
+    ph.viscosity_model = p.viscosity_model;
+    ph.mu = p.mu;
+    ph.precision = p.precision;
+    ph.periodic_seam = p.periodic_seam;
+    ph.periodic_x = gr.bc[EFVM_XLO].kind == EFVM_BC_PERIODIC;
+    ph.periodic_y = gr.bc[EFVM_YLO].kind == EFVM_BC_PERIODIC;
+    for (int s = 0; s < 4; ++s) {
+        ph.bc[s].kind = gr.bc[s].kind;
+        ph.bc[s].rho = gr.bc[s].rho;
+        ph.bc[s].u = gr.bc[s].u;
+        ph.bc[s].v = gr.bc[s].v;
+        ph.bc[s].w = gr.bc[s].w;
+        ph.bc[s].p = gr.bc[s].p;
+        ph.bc[s].t = gr.bc[s].t;
+    }
+    ph.parabolic_inflow = p.parabolic_inflow;
+    ph.inflow_u_max = p.inflow_u_max;
+    ph.inflow_height = p.inflow_height;
+    ph.inflow_rho = p.inflow_rho;
+    ph.sponge = p.sponge;
+    ph.sponge_x_start = p.sponge_x_start;
+    ph.sponge_x_end = p.sponge_x_end;
+    ph.sponge_sigma = p.sponge_sigma;
+    ph.sponge_u_max = p.sponge_u_max;
+    ph.sponge_height = p.sponge_height;
+    ph.sponge_rho = p.sponge_rho;
+    ph.sponge_p = p.sponge_p;
+    ph.body_force_x = p.body_force_x;
+    ph.dx_inv2 = 1.0 / (g.h[0] * g.h[0]);
+    ph.cp = p.gamma * p.r_gas / (p.gamma - 1.0);
+    ph.cfl_visc_sum = 1.0 / (g.h[0] * g.h[0]) + 1.0 / (g.h[1] * g.h[1]) + 1.0 / (g.h[2] * g.h[2]);
+
+    auto cleanup_fail = [&](int code) {
+        efvm_destroy(c);
+        return code;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        fail(nullptr, EFVM_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+        delete c;
+        return EFVM_ERR_CUDA;
+    }
+    const size_t state_bytes = (size_t)4 * g.plane * sizeof(double);
+    for (int k = 0; k < 3; ++k) {
+        e = cudaMalloc(&c->U[k], state_bytes);
+        if (e != cudaSuccess) {
+            fail(nullptr, EFVM_ERR_OOM, std::string("cudaMalloc state: ") + cudaGetErrorString(e));
+            return cleanup_fail(EFVM_ERR_OOM);
+        }
+        cudaMemsetAsync(c->U[k], 0, state_bytes, c->stream);
+    }
+    e = cudaMalloc(&c->mask, (size_t)g.plane);
+    if (e != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc mask"));
+    cudaMemsetAsync(c->mask, 0, (size_t)g.plane, c->stream);
+    // viscous_system's pre-inverted y weights from centroid distances,
+    // crates/cfd_solver/src/lib.rs:484-493
+    std::vector<double> yw(3 * (size_t)g.ny);
+    for (int j = 0; j < g.ny; ++j) {
+        const double hm = centre_h(g.lo[1], g.h[1], j) - centre_h(g.lo[1], g.h[1], j - 1);
+        const double hp = centre_h(g.lo[1], g.h[1], j + 1) - centre_h(g.lo[1], g.h[1], j);
+        yw[j] = 1.0 / hm;
+        yw[g.ny + j] = 1.0 / hp;
+        yw[2 * g.ny + j] = 2.0 / (hm + hp);
+    }
+    if (cudaMalloc(&c->yw, yw.size() * sizeof(double)) != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
+    cudaMemcpyAsync(c->yw, yw.data(), yw.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (cudaMalloc(&c->st, sizeof(DevState)) != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
+    DevState s0{};
+    s0.active = 1;
+    cudaMemcpyAsync(c->st, &s0, sizeof(DevState), cudaMemcpyHostToDevice, c->stream);
+    c->n_partial = 296;
+    if (cudaMalloc(&c->partial, 2 * c->n_partial * sizeof(double)) != cudaSuccess)
+        return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
+    if (cudaMalloc(&c->force_out, 12 * sizeof(double)) != cudaSuccess)
+        return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
+    if (cudaMalloc(&c->force_counter, sizeof(unsigned int)) != cudaSuccess)
+        return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
+    cudaMemsetAsync(c->force_counter, 0, sizeof(unsigned int), c->stream);
+    cudaMemsetAsync(c->force_out, 0, 12 * sizeof(double), c->stream);
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e)));
+    *out = c;
+    return EFVM_OK;
+}
+
+int efvm_destroy(efvm_ctx* c) {
+    if (!c) return EFVM_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    for (int k = 0; k < 3; ++k) cudaFree(c->U[k]);
+    cudaFree(c->mask);
+    cudaFree(c->yw);
+    cudaFree(c->st);
+    cudaFree(c->partial);
+    cudaFree(c->staging);
+    cudaFree(c->cyl_dev);
+    cudaFree(c->ghosts_dev);
+    cudaFree(c->markers_dev);
+    cudaFree(c->zg0);
+    cudaFree(c->zfill);
+    cudaFree(c->force_out);
+    cudaFree(c->force_partials);
+    cudaFree(c->force_counter);
+    cudaFree(c->history);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return EFVM_OK;
+}
+
+static int transfer_state(efvm_ctx* c, double* base, int64_t si, int64_t sj, int64_t sv, bool upload) {
+    if (!c || !base) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    const Geometry& g = c->g;
+    // the host span the strides address, [min offset, max offset]
+    int64_t lo = 0, hi = 0;
+    const int64_t corners[3] = {(int64_t)(g.nx - 1) * si, (int64_t)(g.ny - 1) * sj, 4 * sv};
+    for (int k = 0; k < 3; ++k) {
+        lo += std::min<int64_t>(0, corners[k]);
+        hi += std::max<int64_t>(0, corners[k]);
+    }
+    const int64_t span = hi - lo + 1;
+    const bool dense = span == (int64_t)g.nx * g.ny * 5;
+    int rc = ensure_staging(c, (size_t)span * sizeof(double));
+    if (rc) return rc;
+    double* host0 = base + lo;
+    double* dev0 = c->staging - lo;  // device pointer of element offset 0
+    double* q = cur_buf(c);
+    if (upload) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->staging, host0, (size_t)span * sizeof(double), cudaMemcpyHostToDevice, S(c)));
+        c->launches += launch_pack(g, dev0, si, sj, sv, q, 1, S(c));
+        c->lam_stale = true;
+        c->ghosts_stale = true;
+    } else {
+        if (!dense)  // keep the caller's values in the gaps of a sparse layout
+            CUDA_TRY(c, cudaMemcpyAsync(c->staging, host0, (size_t)span * sizeof(double), cudaMemcpyHostToDevice, S(c)));
+        c->launches += launch_pack(g, dev0, si, sj, sv, q, 0, S(c));
+        CUDA_TRY(c, cudaMemcpyAsync(host0, c->staging, (size_t)span * sizeof(double), cudaMemcpyDeviceToHost, S(c)));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    CUDA_TRY(c, cudaGetLastError());
+    return EFVM_OK;
+}
+
+int efvm_upload_state(efvm_ctx* c, const double* base, int64_t si, int64_t sj, int64_t sv) {
+    return transfer_state(c, const_cast<double*>(base), si, sj, sv, true);
+}
+
+int efvm_download_state(efvm_ctx* c, double* base, int64_t si, int64_t sj, int64_t sv) {
+    return transfer_state(c, base, si, sj, sv, false);
+}
+
+int efvm_get_solver_state(efvm_ctx* c, efvm_solver_state* out) {
+    if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    DevState s;
+    int rc = read_state(c, s);
+    if (rc) return rc;
+    out->dt = s.dt;
+    out->time = s.time;
+    out->step = s.step;
+    out->rk_stage = c->rk_stage;
+    out->completed_full_step = s.completed;
+    if (s.nonphysical) return fail(c, EFVM_ERR_NONPHYSICAL, "the state went non-physical (rho<=0, p<=0 or NaN)");
+    return EFVM_OK;
+}
+
+int efvm_set_solver_state(efvm_ctx* c, const efvm_solver_state* in) {
+    if (!c || !in) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (in->rk_stage < 0 || in->rk_stage > 2) return fail(c, EFVM_ERR_INVALID_ARG, "rk_stage must be 0..2");
+    DevState s;
+    int rc = read_state(c, s);
+    if (rc) return rc;
+    s.dt = in->dt;
+    s.time = in->time;
+    s.step = in->step;
+    s.rk_stage = in->rk_stage;
+    s.completed = in->completed_full_step;
+    CUDA_TRY(c, cudaMemcpyAsync(c->st, &s, sizeof(DevState), cudaMemcpyHostToDevice, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    c->rk_stage = in->rk_stage;
+    c->lam_stale = true;
+    return EFVM_OK;
+}
+
+int efvm_substep(efvm_ctx* c) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (c->control_dirty) sync_control(c, 0, 0.0, 0);
+    int rc = prologue(c);
+    if (rc) return rc;
+    if (c->params.integrator == EFVM_INTEGRATOR_EULER) {
+        double* in = c->U[c->euler_cur];
+        double* outb = c->U[c->euler_cur ^ 1];
+        enqueue_substage(c, 3, in, outb, true);
+        c->euler_cur ^= 1;
+    } else {
+        const int s = c->rk_stage;
+        double* in = c->U[s];
+        double* outb = c->U[(s + 1) % 3];
+        enqueue_substage(c, s, in, outb, s == 0);
+        c->rk_stage = (s + 1) % 3;
+    }
+    CUDA_TRY(c, cudaGetLastError());
+    return EFVM_OK;
+}
+
+int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, double* force_history,
+              efvm_step_info* info) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (n_steps < 0) return fail(c, EFVM_ERR_INVALID_ARG, "n_steps must be >= 0");
+    if (c->params.integrator != EFVM_INTEGRATOR_EULER && c->rk_stage != 0)
+        return fail(c, EFVM_ERR_INVALID_ARG, "efvm_step must start at a step boundary (rk_stage == 0)");
+    DevState s_before;
+    int rc = read_state(c, s_before);
+    if (rc) return rc;
+    const int subs = c->params.integrator == EFVM_INTEGRATOR_EULER ? 1 : 3;
+    const long long cap = force_history && c->ibm ? (long long)subs * n_steps : 0;
+    if (cap > c->history_cap) {
+        cudaFree(c->history);
+        c->history = nullptr;
+        c->history_cap = 0;
+        CUDA_TRY(c, cudaMalloc(&c->history, (size_t)cap * 6 * sizeof(double)));
+        c->history_cap = cap;
+        c->graph_valid = false;
+    }
+    c->ibm_desc.history = cap ? c->history : nullptr;
+    if (c->graph_with_history != (cap != 0)) c->graph_valid = false;
+    c->graph_with_history = cap != 0;
+    sync_control(c, stop_at_t, t_stop, cap);
+    rc = prologue(c);
+    if (rc) return rc;
+    if (c->params.integrator == EFVM_INTEGRATOR_EULER) {
+        for (int64_t k = 0; k < n_steps; ++k) {
+            double* in = c->U[c->euler_cur];
+            double* outb = c->U[c->euler_cur ^ 1];
+            enqueue_substage(c, 3, in, outb, true);
+            c->euler_cur ^= 1;
+        }
+    } else {
+        if (!c->graph_valid) {
+            rc = capture_step_graph(c);
+            if (rc) return rc;
+        }
+        const int64_t chunk = 64;
+        for (int64_t k = 0; k < n_steps; ++k) {
+            CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, S(c)));
+            c->launches += c->graph_kernels;
+            if (stop_at_t && (k + 1) % chunk == 0 && k + 1 < n_steps) {
+                DevState s;
+                rc = read_state(c, s);
+                if (rc) return rc;
+                if (!s.active) break;
+            }
+        }
+    }
+    CUDA_TRY(c, cudaGetLastError());
+    DevState s;
+    rc = read_state(c, s);
+    if (rc) return rc;
+    if (cap && s.hist_pos > 0)
+        CUDA_TRY(c, cudaMemcpy(force_history, c->history, (size_t)s.hist_pos * 6 * sizeof(double),
+                               cudaMemcpyDeviceToHost));
+    else if (force_history && !c->ibm)
+        std::memset(force_history, 0, (size_t)subs * n_steps * 6 * sizeof(double));
+    if (info) {
+        info->steps_done = (int64_t)(s.step - s_before.step);
+        info->substeps_done = info->steps_done * subs;
+        info->time = s.time;
+        info->dt = s.dt;
+        info->stopped_at_t_stop = (stop_at_t && s.time >= t_stop) ? 1 : 0;
+    }
+    c->control_dirty = true;
+    if (s.nonphysical) return fail(c, EFVM_ERR_NONPHYSICAL, "the state went non-physical (rho<=0, p<=0 or NaN)");
+    return EFVM_OK;
+}
+
+int efvm_cfl(efvm_ctx* c, double* dt_out) {
+    if (!c || !dt_out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (c->ph.fixed_dt > 0.0) {
+        *dt_out = c->ph.fixed_dt;
+        return EFVM_OK;
+    }
+    c->launches += launch_cfl(c->g, c->ph, cur_buf(c), c->st, S(c));
+    DevState s;
+    int rc = read_state(c, s);
+    if (rc) return rc;
+    double lam;
+    std::memcpy(&lam, &s.lam[s.lam_idx], sizeof(double));
+    *dt_out = lam > 0.0 ? c->ph.cfl / lam : std::numeric_limits<double>::infinity();
+    if (c->rk_stage == 0) c->lam_stale = false;
+    else c->lam_stale = true;
+    return EFVM_OK;
+}
+
+int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const double fs[5]) {
+    if (!c || (n > 0 && (!cyl || !fs)) || n < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid cylinder arguments");
+    if (n == 0) {
+        c->ibm = false;
+        c->graph_valid = false;
+        return EFVM_OK;
+    }
+    c->cyl_host.clear();
+    for (int b = 0; b < n; ++b) {
+        if (!(cyl[b].radius > 0.0)) return fail(c, EFVM_ERR_INVALID_ARG, "cylinder radius must be > 0");
+        c->cyl_host.push_back(cyl[b].cx);
+        c->cyl_host.push_back(cyl[b].cy);
+        c->cyl_host.push_back(cyl[b].radius);
+    }
+    // MaskConsts of CylinderIbmPlugin::build, crates/cfd_ibm/src/lib.rs:665-669:
+    // stagnant = freestream at rest (same rho and internal energy), ambient = freestream
+    const double ke = 0.5 * (fs[1] * fs[1] + fs[2] * fs[2] + fs[3] * fs[3]) / fs[0];
+    const double st5[5] = {fs[0], 0.0, 0.0, 0.0, fs[4] - ke};
+    std::memcpy(c->stagnant, st5, sizeof(st5));
+    std::memcpy(c->ambient, fs, 5 * sizeof(double));
+    if (c->cyl_dev) cudaFree(c->cyl_dev);
+    c->cyl_dev = nullptr;
+    CUDA_TRY(c, cudaMalloc(&c->cyl_dev, c->cyl_host.size() * sizeof(double)));
+    CUDA_TRY(c, cudaMemcpy(c->cyl_dev, c->cyl_host.data(), c->cyl_host.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->ibm = true;
+    c->geom_dirty = true;
+    c->graph_valid = false;
+    return EFVM_OK;
+}
+
+static int read_forces(efvm_ctx* c, double* out, int offset) {
+    if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (!c->ibm) {
+        for (int d = 0; d < 6; ++d) out[d] = 0.0;
+        return EFVM_OK;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(out, c->force_out + offset, 6 * sizeof(double), cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    return EFVM_OK;
+}
+
+int efvm_marker_force(efvm_ctx* c, double out[6]) { return read_forces(c, out, 0); }
+int efvm_wall_force(efvm_ctx* c, double out[6]) { return read_forces(c, out, 6); }
+
+int efvm_ibm_counts(efvm_ctx* c, int64_t* n_solid, int64_t* n_ghost) {
+    if (!c || !n_solid || !n_ghost) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (c->ibm && c->geom_dirty) {
+        int rc = prologue(c);
+        if (rc) return rc;
+    }
+    *n_solid = c->ibm ? c->n_solid : 0;
+    *n_ghost = c->ibm ? c->ibm_desc.n_ghost : 0;
+    return EFVM_OK;
+}
+
+int efvm_get_solid_mask(efvm_ctx* c, uint8_t* out) {
+    if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (c->ibm && c->geom_dirty) {
+        int rc = prologue(c);
+        if (rc) return rc;
+    }
+    const Geometry& g = c->g;
+    CUDA_TRY(c, cudaMemcpy2DAsync(out, g.nx, c->mask + (size_t)YO * g.pitch + XO, g.pitch, g.nx, g.ny,
+                                  cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    return EFVM_OK;
+}
+
+int efvm_density_error(efvm_ctx* c, const efvm_vortex* v, double out[2]) {
+    if (!c || !v || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    c->launches += launch_density_error(c->g, *v, cur_buf(c), c->st, c->partial, c->n_partial, S(c));
+    std::vector<double> part(2 * (size_t)c->n_partial);
+    CUDA_TRY(c, cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    double sum = 0.0, mx = 0.0;
+    for (int b = 0; b < c->n_partial; ++b) {
+        sum += part[2 * b];
+        mx = std::max(mx, part[2 * b + 1]);
+    }
+    // volume-weighted mean over uniform cells
+    out[0] = sum / ((double)c->g.nx * (double)c->g.ny);
+    out[1] = mx;
+    return EFVM_OK;
+}
+
+int efvm_init_vortex(efvm_ctx* c, const efvm_vortex* v) {
+    if (!c || !v) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    c->launches += launch_init_vortex(c->g, *v, cur_buf(c), S(c));
+    c->lam_stale = true;
+    c->ghosts_stale = true;
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    return EFVM_OK;
+}
+
+int efvm_total_mass(efvm_ctx* c, double* out) {
+    if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    c->launches += launch_total_mass(c->g, cur_buf(c), c->partial, c->n_partial, S(c));
+    std::vector<double> part((size_t)c->n_partial);
+    CUDA_TRY(c, cudaMemcpyAsync(part.data(), c->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    double sum = 0.0;
+    for (double x : part) sum += x;
+    *out = sum;
+    return EFVM_OK;
+}
+
+int efvm_get_stream(efvm_ctx* c, void** stream) {
+    if (!c || !stream) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    *stream = (void*)c->stream;
+    return EFVM_OK;
+}
+
+int efvm_launch_count(efvm_ctx* c, uint64_t* out) {
+    if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    *out = c->launches;
+    return EFVM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,149 @@
+// efvm_internal.h — device data layout and kernel parameters shared by the
+// CUDA kernels (efvm_kernels.cu) and the C-ABI host code (efvm_api.cu).
+//
+// HBM layout of one conserved state (structure of arrays, FP64):
+//   4 planes (rho, rho_u, rho_v, rho_e), each (ny + 2*YO) rows x `pitch`
+//   doubles; interior cell (i, j) sits at row YO + j, column XO + i.  Columns
+//   XO-2, XO-1 and XO+nx, XO+nx+1 are the two ghost layers of FIELD's ng = 2
+//   (rows likewise).  XO = 4 makes every interior row start on a 32-byte
+//   sector; the pitch is a multiple of 8 doubles.  rho_w is identically zero in
+//   2-D and is not stored.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/efvm.h"
+
+namespace efvm {
+
+constexpr int XO = 4;  // column of interior cell i = 0
+constexpr int YO = 2;  // row of interior cell j = 0
+constexpr int NG = 2;  // FIELD ghost layers
+
+// Per-step device solver state (SolverState + the CFL reduction buffers).
+struct DevState {
+    double dt;
+    double time;
+    unsigned long long step;
+    int rk_stage;            // 0,1,2
+    int completed;           // StepBoundary.completed_full_step
+    unsigned long long lam[2];  // max wave speed (bits of a non-negative double)
+    int lam_idx;             // lam[lam_idx] is being accumulated / is current
+    int active;              // 0 once t_stop was reached (kernels become no-ops)
+    int stop_at_t;
+    int nonphysical;         // bit 0: rho<=0, bit 1: p<=0, bit 2: NaN
+    double t_stop;
+    long long hist_pos;      // next MarkerForce history slot
+    long long hist_cap;
+};
+
+// Boundary side description resolved for the device.
+struct DevBC {
+    int kind;
+    int pad;
+    double rho, u, v, w, p, t;
+};
+
+struct Geometry {
+    int nx, ny;
+    int pitch;            // doubles per row
+    long long plane;      // doubles per plane
+    double lo[3], hi[3];
+    double h[3];          // spacing dx, dy, dz
+    double inv_x, inv_y;  // face area / cell volume for x and y faces
+    double cell_volume;
+};
+
+struct Physics {
+    double gamma, r_gas;
+    double cfl, fixed_dt;
+    int flux_scheme, reconstruction, limiter, integrator;
+    int viscous, viscosity_model;
+    double mu;
+    int precision, periodic_seam;
+    int periodic_x, periodic_y;
+    DevBC bc[4];  // XLO, XHI, YLO, YHI
+    int parabolic_inflow;
+    double inflow_u_max, inflow_height, inflow_rho;
+    int sponge;
+    double sponge_x_start, sponge_x_end, sponge_sigma, sponge_u_max, sponge_height, sponge_rho, sponge_p;
+    double body_force_x;
+    double dx_inv2;       // 1/(dx*dx), viscous x weight
+    double cp;            // gamma*R/(gamma-1), for kappa = mu*cp/0.72
+    double cfl_visc_sum;  // 1/dx^2 + 1/dy^2 + 1/dz^2
+};
+
+// One solid cell that the IBM mirror refills every substage (IbmGhostCells).
+struct IbmGhostDev {
+    long long cell;          // interior linear index j*nx + i
+    int lo_i, lo_j;          // low corner of the bilinear block (interior indices, may be -1 / n)
+    double tx, ty;           // bilinear fractions
+    int valid;               // locate() succeeded
+    int pad;
+};
+
+// One surface marker (IbmMarker) with its sample point already located.
+struct MarkerDev {
+    double normal[3];
+    double area;
+    double wall_velocity[3];
+    int lo_i, lo_j;
+    double tx, ty;
+    int valid;
+    int pad;
+};
+
+struct Ibm {
+    int enabled;
+    int n_ghost;
+    int n_markers;
+    int pad;
+    const IbmGhostDev* ghosts;
+    const MarkerDev* markers;
+    double sample_offset;   // dx
+    // emulated z-ghost states of the solid cells (the 2-D mesh's z layers),
+    // used only by the staircase wall force: zg0 (saved at stage 1) and the
+    // pre-mirror fill of each RK stage (one buffer per stage)
+    double* zg0;            // n_ghost x 4
+    double* zfill;          // 3 x n_ghost x 4
+    double* force_out;      // 12 doubles: marker force (6) then wall force (6)
+    double* history;        // hist_cap x 6 (may be null)
+    double* partials;       // 6 doubles per force block (deterministic reduction)
+    unsigned int* counter;  // blocks finished in the current force launch
+};
+
+// Everything a stage kernel needs.
+struct StageArgs {
+    Geometry g;
+    Physics ph;
+    const double* __restrict__ uin;   // stage input (stencil)
+    const double* u0;                 // U^n (RK stages 2 and 3); may alias uout on stage 3
+    double* uout;
+    const uint8_t* __restrict__ mask; // solid mask (same layout as one plane, bytes) or null
+    const double* __restrict__ yw;    // 3*ny viscous y weights: y_im, y_ip, y_is
+    DevState* st;
+    int stage;                        // 0,1,2 for RK3; 3 = Euler
+    int completes_step;               // sponge + CFL + clock in the epilogue
+    int want_cfl;
+};
+
+// Host-side launch wrappers (efvm_kernels.cu); each returns the number of
+// kernels it launched.
+int launch_stage(const StageArgs& a, int tile_x, int tile_y, void* stream);
+int launch_fill_ghosts(const Geometry& g, const Physics& ph, double* q, void* stream);
+int launch_cfl(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream);
+int launch_step_setup(const Physics& ph, DevState* st, void* stream);
+int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double* stagnant, const double* ambient,
+                     double* q, uint8_t* mask, void* stream);
+int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, const uint8_t* mask, DevState* st,
+                int stage, int do_mirror, int do_forces, int force_stage, void* stream);
+int launch_pack(const Geometry& g, const double* host_like, int64_t si, int64_t sj, int64_t sv, double* q,
+                 int to_device, void* stream);
+int launch_init_vortex(const Geometry& g, const efvm_vortex& v, double* q, void* stream);
+int launch_density_error(const Geometry& g, const efvm_vortex& v, const double* q, const DevState* st,
+                          double* partial, int nblocks, void* stream);
+int launch_total_mass(const Geometry& g, const double* q, double* partial, int nblocks, void* stream);
+int launch_check_state(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream);
+int launch_set_control(DevState* st, int active, int stop_at_t, double t_stop, long long hist_cap, void* stream);
+
+}  // namespace efvm

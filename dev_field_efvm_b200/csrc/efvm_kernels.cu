@@ -1,0 +1,1026 @@
+// efvm_kernels.cu — sm_100a kernels of the explicit finite-volume step.
+//
+//   stage_kernel   one RK substage over a 2-D tile: MUSCL slopes, L/R face
+//                  states, one numerical flux per face (HLLC-Thornber /
+//                  textbook HLLC / Rusanov), flux divergence, viscous terms,
+//                  solid-cell zeroing, body force, SSP-RK3 (or Euler)
+//                  combination, and on the step's last stage the sponge, the
+//                  boundary-ghost refill of the output and the CFL wave-speed
+//                  max (one atomic per block).
+//   fill_ghosts    Halo + Boundary phases for a freshly uploaded state.
+//   step_setup     per-step dt = cfl / max wave speed, clock/stop bookkeeping.
+//   ibm_kernel     ghost-cell IBM mirror (bilinear image sample) and, after a
+//                  stage, the marker-integrated and staircase wall forces.
+//   geometry       cylinder solid mask and the stagnant/ambient re-seed.
+//   utilities      strided pack/unpack, vortex init, error and mass partials.
+//
+// The stencil path is HBM- and FP64-bound; no tensor cores are involved.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "efvm_internal.h"
+#include "efvm_math.cuh"
+
+namespace efvm {
+
+namespace {
+
+__device__ __forceinline__ long long cidx(const Geometry& g, int i, int j) {
+    return (long long)(YO + j) * g.pitch + (XO + i);
+}
+
+// Cell centre lo + (i + 0.5) h with one rounding per operation, as the host
+// computes it (no FMA), so geometry tests agree bit for bit.
+__device__ __forceinline__ double centre(double lo, double h, int i) {
+    return __dadd_rn(lo, __dmul_rn((double)i + 0.5, h));
+}
+
+// ---- 2-D conserved state in the grid frame ---------------------------------
+struct U4 {
+    double r, mx, my, E;
+};
+
+__device__ __forceinline__ U4 load4(const double* q, long long plane, long long o) {
+    return U4{q[o], q[plane + o], q[2 * plane + o], q[3 * plane + o]};
+}
+__device__ __forceinline__ void store4(double* q, long long plane, long long o, const U4& u) {
+    q[o] = u.r;
+    q[plane + o] = u.mx;
+    q[2 * plane + o] = u.my;
+    q[3 * plane + o] = u.E;
+}
+
+__device__ __forceinline__ double pressure_d(const U4& u, double gm1) {
+    return gm1 * (u.E - 0.5 * (u.mx * u.mx + u.my * u.my) / u.r);
+}
+
+// IdealGas::prim_to_cons (2-D, w = 0), crates/cfd_eos/src/lib.rs:55-59
+__device__ __forceinline__ U4 prim_to_cons(double rho, double u, double v, double p, double gm1) {
+    const double ke = 0.5 * rho * (u * u + v * v);
+    return U4{rho, rho * u, rho * v, p / gm1 + ke};
+}
+
+// Viscosity::mu, crates/cfd_eos/src/lib.rs:108-117 (Sutherland :75-80)
+__device__ __forceinline__ double viscosity(const Physics& ph, double t) {
+    if (ph.viscosity_model == EFVM_VISC_CONSTANT) return ph.mu;
+    const double MU_REF = 1.827e-5, T_REF = 291.15, S = 120.0;
+    return MU_REF * pow(t / T_REF, 1.5) * (T_REF + S) / (t + S);
+}
+
+// One boundary ghost from its interior neighbour (BoundaryCondition::ghost_at),
+// crates/cfd_boundary/src/lib.rs:172-362.  side = 0..3 (XLO, XHI, YLO, YHI).
+__device__ __forceinline__ U4 bc_ghost(const DevBC& bc, int side, const U4& in, double gm1) {
+    switch (bc.kind) {
+        case EFVM_BC_SLIP_WALL:
+        case EFVM_BC_SYMMETRY: {
+            const double n0 = side < 2 ? (side == 1 ? 1.0 : -1.0) : 0.0;
+            const double n1 = side >= 2 ? (side == 3 ? 1.0 : -1.0) : 0.0;
+            const double mn = in.mx * n0 + in.my * n1;
+            U4 g = in;
+            g.mx = in.mx - 2.0 * mn * n0;
+            g.my = in.my - 2.0 * mn * n1;
+            return g;
+        }
+        case EFVM_BC_NO_SLIP_WALL:
+            return U4{in.r, -in.mx, -in.my, in.E};
+        case EFVM_BC_SUPERSONIC_INFLOW: {
+            const double ke = 0.5 * bc.rho * (bc.u * bc.u + bc.v * bc.v + bc.w * bc.w);
+            return U4{bc.rho, bc.rho * bc.u, bc.rho * bc.v, bc.p / gm1 + ke};
+        }
+        case EFVM_BC_SUBSONIC_INFLOW: {
+            const double p_in = pressure_d(in, gm1);
+            const double ke = 0.5 * bc.rho * (bc.u * bc.u + bc.v * bc.v + bc.w * bc.w);
+            return U4{bc.rho, bc.rho * bc.u, bc.rho * bc.v, p_in / gm1 + ke};
+        }
+        case EFVM_BC_PRESSURE_OUTLET: {
+            const double inv = 1.0 / in.r;
+            const double u = in.mx * inv, v = in.my * inv;
+            return prim_to_cons(in.r, u, v, bc.p, gm1);
+        }
+        default:
+            return in;
+    }
+}
+
+// Boundary-ghost refill for the cell (i, j) whose new value is `u`: the Halo
+// (periodic wrap) and Boundary phases of the next substage, done by the thread
+// that owns the interior source cell (each ghost has exactly one writer).
+__device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& ph, double* q, int i, int j,
+                                             const U4& u) {
+    const long long P = g.plane;
+    const double gm1 = ph.gamma - 1.0;
+    if (ph.periodic_x) {
+        if (i >= g.nx - NG) store4(q, P, cidx(g, i - g.nx, j), u);
+        if (i < NG) store4(q, P, cidx(g, i + g.nx, j), u);
+    } else {
+        if (i == 0) {
+            store4(q, P, cidx(g, -1, j), bc_ghost(ph.bc[0], 0, u, gm1));
+            if (ph.parabolic_inflow) {
+                // parabolic_inflow_system, examples/cylinder_drag_validation/main.rs:151-177
+                const double y = centre(g.lo[1], g.h[1], j);
+                const double um = ph.inflow_u_max, hh = ph.inflow_height, rho = ph.inflow_rho;
+                const double uy = 4.0 * um * y * (hh - y) / (hh * hh);
+                const double p_in = pressure_d(u, gm1);
+                const U4 c = prim_to_cons(rho, uy, 0.0, p_in, gm1);
+                store4(q, P, cidx(g, -1, j), c);
+                store4(q, P, cidx(g, -2, j), c);
+            }
+        }
+        if (i == g.nx - 1) store4(q, P, cidx(g, g.nx, j), bc_ghost(ph.bc[1], 1, u, gm1));
+    }
+    if (ph.periodic_y) {
+        if (j >= g.ny - NG) store4(q, P, cidx(g, i, j - g.ny), u);
+        if (j < NG) store4(q, P, cidx(g, i, j + g.ny), u);
+    } else {
+        if (j == 0) store4(q, P, cidx(g, i, -1), bc_ghost(ph.bc[2], 2, u, gm1));
+        if (j == g.ny - 1) store4(q, P, cidx(g, i, g.ny), bc_ghost(ph.bc[3], 3, u, gm1));
+    }
+}
+
+// Local max wave speed of cfl_system, crates/cfd_solver/src/lib.rs:647-669.
+__device__ __forceinline__ double wave_speed(const Geometry& g, const Physics& ph, const U4& u) {
+    if (!(u.r > 0.0)) return 0.0;
+    const double gm1 = ph.gamma - 1.0;
+    const double inv = 1.0 / u.r;
+    const double vx = u.mx * inv, vy = u.my * inv;
+    const double p = pressure_d(u, gm1);
+    const double a = sqrt(ph.gamma * p / u.r);
+    double lam = (fabs(vx) + a) / g.h[0] + (fabs(vy) + a) / g.h[1] + (0.0 + a) / g.h[2];
+    if (ph.viscous) {
+        const double ke = 0.5 * u.r * (vx * vx + vy * vy);
+        const double pp = gm1 * (u.E - ke);
+        const double t = pp * inv / ph.r_gas;
+        const double nu = viscosity(ph, t) / u.r;
+        lam += 2.0 * nu * ph.cfl_visc_sum;
+    }
+    return lam;
+}
+
+__device__ __forceinline__ void block_max_atomic(double v, unsigned long long* target) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nw = (blockDim.x * blockDim.y + 31) / 32;
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid < 32) {
+        double w = tid < nw ? red[tid] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
+        if (tid == 0 && w > 0.0 && w == w) atomicMax(target, (unsigned long long)__double_as_longlong(w));
+    }
+}
+
+// Face state of one cell toward +x/+y (sgn = +1) or -x/-y (sgn = -1): centre
+// value, or centre +- half the limited slope (reconstruct_to_face and
+// limited_slope_cons, crates/cfd_solver/src/lib.rs:199-211,273-286).  m/c/p are
+// the previous/own/next cells along the face normal.  The FP32 path takes the
+// differences in FP64 and limits and extrapolates in FP32.
+template <class R>
+__device__ __forceinline__ R recon(double m, double c, double p, int limiter, bool rec, double sgn) {
+    if (!rec) return R(c);
+    if (sizeof(R) == sizeof(double)) {
+        const double s = limit<double>(limiter, p - c, c - m);
+        return R(c + s * sgn * 0.5);
+    } else {
+        const float s = limit<float>(limiter, (float)(p - c), (float)(c - m));
+        return R((float)c + s * (float)sgn * 0.5f);
+    }
+}
+
+__device__ __forceinline__ U4 shfl_up4(const U4& u, int d) {
+    return U4{__shfl_up_sync(0xffffffffu, u.r, d), __shfl_up_sync(0xffffffffu, u.mx, d),
+              __shfl_up_sync(0xffffffffu, u.my, d), __shfl_up_sync(0xffffffffu, u.E, d)};
+}
+__device__ __forceinline__ U4 shfl_down4(const U4& u, int d) {
+    return U4{__shfl_down_sync(0xffffffffu, u.r, d), __shfl_down_sync(0xffffffffu, u.mx, d),
+              __shfl_down_sync(0xffffffffu, u.my, d), __shfl_down_sync(0xffffffffu, u.E, d)};
+}
+template <class R>
+__device__ __forceinline__ Q4<R> shfl_up_q(const Q4<R>& u, int d) {
+    return Q4<R>{__shfl_up_sync(0xffffffffu, u.r, d), __shfl_up_sync(0xffffffffu, u.mn, d),
+                 __shfl_up_sync(0xffffffffu, u.mt, d), __shfl_up_sync(0xffffffffu, u.E, d)};
+}
+template <class R>
+__device__ __forceinline__ Q4<R> shfl_down_q(const Q4<R>& u, int d) {
+    return Q4<R>{__shfl_down_sync(0xffffffffu, u.r, d), __shfl_down_sync(0xffffffffu, u.mn, d),
+                 __shfl_down_sync(0xffffffffu, u.mt, d), __shfl_down_sync(0xffffffffu, u.E, d)};
+}
+
+// Primitive (u, v, T) of a state (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
+__device__ __forceinline__ void prim_uvt(const U4& u, double gm1, double r_gas, double& vu, double& vv, double& t) {
+    const double inv = 1.0 / u.r;
+    vu = u.mx * inv;
+    vv = u.my * inv;
+    const double ke = 0.5 * u.r * (vu * vu + vv * vv);
+    t = gm1 * (u.E - ke) * inv / r_gas;
+}
+
+constexpr int STRIP = 31;  // cells a warp owns per row (lane 31 supplies the right face)
+constexpr int WPB = 4;     // warps per block
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel.
+//
+// Each warp owns a strip of 31 columns and marches up `rows` rows of it.  Lane
+// l holds column i0+l and, per row, computes the x-face flux on the left of its
+// column and the y-face flux above it; the x neighbours come from warp
+// shuffles and the y-face flux below a row is carried from the previous row,
+// so every face is evaluated once per strip and no block barrier is needed.
+// Each lane then forms the flux divergence of its own cell (lanes 0..30),
+// adds the viscous terms, zeroes solid cells, applies the RK combination and,
+// on a step's last stage, the sponge, refills the boundary ghosts of the output
+// and takes the wave-speed max for the next step's CFL dt.
+// ---------------------------------------------------------------------------
+template <int SCHEME, int RECON, class R, int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
+    if (!a.st->active) return;
+    const Geometry& g = a.g;
+    const Physics& ph = a.ph;
+    const long long P = g.plane;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
+        // (no other thread reads time/step/rk_stage during this kernel)
+        DevState* st = a.st;
+        if (a.stage >= 2) {
+            st->rk_stage = 0;
+            st->completed = 1;
+            st->step += 1;
+            st->time += st->dt;
+        } else {
+            st->rk_stage = a.stage + 1;
+            st->completed = 0;
+        }
+    }
+    const int i0 = (blockIdx.x * WPB + warp) * STRIP;
+    const int jb = blockIdx.y * rows;
+    double lam = 0.0;
+    if (i0 < g.nx && jb < g.ny) {  // uniform across the warp
+        const int je = min(jb + rows, g.ny);
+        const int i = i0 + lane;
+        const int ic = min(i, g.nx + NG - 1);  // clamped load column (lanes past the grid)
+        const bool owner = lane < STRIP && i < g.nx;
+        const bool muscl = RECON == EFVM_RECON_MUSCL;
+        const bool true_seam = ph.periodic_seam == EFVM_SEAM_TRUE_PERIODIC;
+        const double gm1 = ph.gamma - 1.0;
+        const R rg = R(ph.gamma), rgm1 = R(gm1);
+        const double* __restrict__ uin = a.uin;
+        auto ld = [&](int ii, int jj) { return load4(uin, P, cidx(g, ii, jj)); };
+
+        // x-face recon flags of this lane's face (between columns i-1 and i)
+        bool rec_l = muscl, rec_r = muscl;
+        if (i == 0) {
+            rec_l = muscl && ph.periodic_x && true_seam;
+            rec_r = muscl && ph.periodic_x;
+        } else if (i == g.nx) {
+            rec_l = muscl && ph.periodic_x;
+            rec_r = muscl && ph.periodic_x && true_seam;
+        }
+
+        // y-face flux (grid frame) between rows j and j+1 at this lane's column
+        auto yflux = [&](int j) -> U4 {
+            bool rec_b = muscl, rec_t = muscl;
+            if (j == -1) {
+                rec_b = muscl && ph.periodic_y && true_seam;
+                rec_t = muscl && ph.periodic_y;
+            } else if (j + 1 == g.ny) {
+                rec_b = muscl && ph.periodic_y;
+                rec_t = muscl && ph.periodic_y && true_seam;
+            }
+            const U4 u0 = ld(ic, j), u1 = ld(ic, j + 1);
+            U4 um = u0, u2 = u1;
+            if (rec_b) um = ld(ic, j - 1);
+            if (rec_t) u2 = ld(ic, j + 2);
+            Q4<R> B, T;
+            B.r = recon<R>(um.r, u0.r, u1.r, ph.limiter, rec_b, 1.0);
+            B.mn = recon<R>(um.my, u0.my, u1.my, ph.limiter, rec_b, 1.0);
+            B.mt = recon<R>(um.mx, u0.mx, u1.mx, ph.limiter, rec_b, 1.0);
+            B.E = recon<R>(um.E, u0.E, u1.E, ph.limiter, rec_b, 1.0);
+            T.r = recon<R>(u0.r, u1.r, u2.r, ph.limiter, rec_t, -1.0);
+            T.mn = recon<R>(u0.my, u1.my, u2.my, ph.limiter, rec_t, -1.0);
+            T.mt = recon<R>(u0.mx, u1.mx, u2.mx, ph.limiter, rec_t, -1.0);
+            T.E = recon<R>(u0.E, u1.E, u2.E, ph.limiter, rec_t, -1.0);
+            const Q4<R> f = face_flux<SCHEME, R>(B, T, rg, rgm1);
+            return U4{(double)f.r, (double)f.mt, (double)f.mn, (double)f.E};
+        };
+
+        U4 gb = yflux(jb - 1);
+        for (int j = jb; j < je; ++j) {
+            const U4 gt = yflux(j);
+
+            // ---- x-face on the left of column i, row j ----
+            const U4 uc = ld(ic, j);
+            U4 ul = shfl_up4(uc, 1), ur = shfl_down4(uc, 1);
+            U4 ull = ul;  // column i-2 (lane 0 only)
+            if (lane == 0) {
+                ul = ld(i0 - 1, j);
+                if (muscl) ull = ld(i0 - 2, j);
+            }
+            if (lane == 31) ur = ld(min(i0 + 32, g.nx + NG - 1), j);
+            Q4<R> Pp, M;  // this column's +x and -x face states
+            Pp.r = recon<R>(ul.r, uc.r, ur.r, ph.limiter, muscl, 1.0);
+            Pp.mn = recon<R>(ul.mx, uc.mx, ur.mx, ph.limiter, muscl, 1.0);
+            Pp.mt = recon<R>(ul.my, uc.my, ur.my, ph.limiter, muscl, 1.0);
+            Pp.E = recon<R>(ul.E, uc.E, ur.E, ph.limiter, muscl, 1.0);
+            M.r = recon<R>(ul.r, uc.r, ur.r, ph.limiter, muscl, -1.0);
+            M.mn = recon<R>(ul.mx, uc.mx, ur.mx, ph.limiter, muscl, -1.0);
+            M.mt = recon<R>(ul.my, uc.my, ur.my, ph.limiter, muscl, -1.0);
+            M.E = recon<R>(ul.E, uc.E, ur.E, ph.limiter, muscl, -1.0);
+            Q4<R> Lp = shfl_up_q(Pp, 1);  // +x state of column i-1
+            if (lane == 0 && muscl) {
+                Lp.r = recon<R>(ull.r, ul.r, uc.r, ph.limiter, true, 1.0);
+                Lp.mn = recon<R>(ull.mx, ul.mx, uc.mx, ph.limiter, true, 1.0);
+                Lp.mt = recon<R>(ull.my, ul.my, uc.my, ph.limiter, true, 1.0);
+                Lp.E = recon<R>(ull.E, ul.E, uc.E, ph.limiter, true, 1.0);
+            }
+            const Q4<R> Lc{R(ul.r), R(ul.mx), R(ul.my), R(ul.E)};
+            const Q4<R> Rc{R(uc.r), R(uc.mx), R(uc.my), R(uc.E)};
+            const Q4<R> L = rec_l ? Lp : Lc;
+            const Q4<R> Rs = rec_r ? M : Rc;
+            const Q4<R> fx = face_flux<SCHEME, R>(L, Rs, rg, rgm1);
+            const Q4<R> fxr = shfl_down_q(fx, 1);  // face on the right of column i
+
+            if (owner) {
+                const long long o = cidx(g, i, j);
+                // Flux divergence in the reference's accumulation order: the face
+                // below (scattered when row j-1 was visited), the face on the
+                // left, then the cell's own +x and +y faces (for_each_face order,
+                // crates/cfd_solver/src/lib.rs:333-337).
+                const double fl[4] = {(double)fx.r, (double)fx.mn, (double)fx.mt, (double)fx.E};
+                const double fr[4] = {(double)fxr.r, (double)fxr.mn, (double)fxr.mt, (double)fxr.E};
+                const double gbv[4] = {gb.r, gb.mx, gb.my, gb.E};
+                const double gtv[4] = {gt.r, gt.mx, gt.my, gt.E};
+                double rhs[4];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    double acc = __dmul_rn(gbv[v], g.inv_y);
+                    acc = __dadd_rn(acc, __dmul_rn(fl[v], g.inv_x));
+                    acc = __dsub_rn(acc, __dmul_rn(fr[v], g.inv_x));
+                    acc = __dsub_rn(acc, __dmul_rn(gtv[v], g.inv_y));
+                    rhs[v] = acc;
+                }
+                const bool ibm = a.mask != nullptr;
+                const bool solid = ibm && a.mask[o];
+                if (ph.viscous && !solid) {
+                    // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D)
+                    double us, vs, ts;
+                    prim_uvt(uc, gm1, ph.r_gas, us, vs, ts);
+                    double nu[4], nv[4], nt[4];  // +x, -x, +y, -y
+                    const U4 nbs[4] = {ur, ul, ld(i, j + 1), ld(i, j - 1)};
+                    const long long no[4] = {o + 1, o - 1, o + g.pitch, o - g.pitch};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if (ibm && a.mask[no[k]]) {
+                            nu[k] = 0.0; nv[k] = 0.0; nt[k] = ts;
+                        } else {
+                            prim_uvt(nbs[k], gm1, ph.r_gas, nu[k], nv[k], nt[k]);
+                        }
+                    }
+                    const double y_im = a.yw[j], y_ip = a.yw[g.ny + j], y_is = a.yw[2 * g.ny + j];
+                    const double dxi2 = ph.dx_inv2;
+                    auto d2x = [&](double m, double p, double c) { return (p - 2.0 * c + m) * dxi2; };
+                    auto d2y = [&](double m, double p, double c) { return ((p - c) * y_ip - (c - m) * y_im) * y_is; };
+                    const double mu = viscosity(ph, ts);
+                    const double kappa = mu * ph.cp / 0.72;  // thermal_conductivity, crates/cfd_eos/src/lib.rs:83-87
+                    const double fxv = mu * (d2x(nu[1], nu[0], us) + d2y(nu[3], nu[2], us));
+                    const double fyv = mu * (d2x(nv[1], nv[0], vs) + d2y(nv[3], nv[2], vs));
+                    const double d2t = d2x(nt[1], nt[0], ts) + d2y(nt[3], nt[2], ts);
+                    rhs[1] += fxv;
+                    rhs[2] += fyv;
+                    rhs[3] += us * fxv + vs * fyv + kappa * d2t;
+                }
+                if (solid) rhs[0] = rhs[1] = rhs[2] = rhs[3] = 0.0;  // zero_solid_rhs, crates/cfd_ibm/src/lib.rs:293-301
+                if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
+                    rhs[1] += uc.r * ph.body_force_x;
+                    rhs[3] += ph.body_force_x * uc.mx;
+                }
+
+                // Rk3Integrator / EulerIntegrator::substep, crates/cfd_solver/src/integrate.rs:48-101
+                const double dt = a.st->dt;
+                const double ucv[4] = {uc.r, uc.mx, uc.my, uc.E};
+                double un[4];
+                if (a.stage == 1 || a.stage == 2) {
+                    const double w0 = a.stage == 1 ? 0.75 : (1.0 / 3.0);
+                    const double w1 = a.stage == 1 ? 0.25 : (2.0 / 3.0);
+#pragma unroll
+                    for (int v = 0; v < 4; ++v)
+                        un[v] = __dadd_rn(__dmul_rn(w0, a.u0[v * P + o]),
+                                          __dmul_rn(w1, __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt))));
+                } else {
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) un[v] = __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt));
+                }
+                U4 nw{un[0], un[1], un[2], un[3]};
+
+                if (a.completes_step && ph.sponge) {
+                    // outlet_sponge_system, examples/cylinder_drag_validation/main.rs:186-229
+                    const double cx = centre(g.lo[0], g.h[0], i);
+                    if (cx >= ph.sponge_x_start) {
+                        const double cy = centre(g.lo[1], g.h[1], j);
+                        const double inv_w = 1.0 / (ph.sponge_x_end - ph.sponge_x_start);
+                        const double s = fmin(fmax((cx - ph.sponge_x_start) * inv_w, 0.0), 1.0);
+                        const double f = fmin(ph.sponge_sigma * s * s * dt, 1.0);
+                        const double hh = ph.sponge_height;
+                        const double uy = 4.0 * ph.sponge_u_max * cy * (hh - cy) / (hh * hh);
+                        const U4 tg = prim_to_cons(ph.sponge_rho, uy, 0.0, ph.sponge_p, gm1);
+                        nw.r += f * (tg.r - nw.r);
+                        nw.mx += f * (tg.mx - nw.mx);
+                        nw.my += f * (tg.my - nw.my);
+                        nw.E += f * (tg.E - nw.E);
+                    }
+                }
+
+                store4(a.uout, P, o, nw);
+                write_ghosts(g, ph, a.uout, i, j, nw);
+
+                // non-physical state flag (rho<=0, p<=0, NaN)
+                const double pn = pressure_d(nw, gm1);
+                int bad = 0;
+                if (!(nw.r > 0.0)) bad |= 1;
+                if (!(pn > 0.0)) bad |= 2;
+                if (nw.r != nw.r || nw.mx != nw.mx || nw.my != nw.my || nw.E != nw.E) bad |= 4;
+                if (bad) atomicOr(&a.st->nonphysical, bad);
+
+                if (a.completes_step && a.want_cfl) lam = fmax(lam, wave_speed(g, ph, nw));
+            }
+            gb = gt;
+        }
+    }
+    // wave-speed max for the next step's CFL dt: one atomic per warp
+    if (a.completes_step && a.want_cfl) {
+        for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
+        if (lane == 0 && lam > 0.0 && lam == lam)
+            atomicMax(&a.st->lam[a.st->lam_idx], (unsigned long long)__double_as_longlong(lam));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CFL wave-speed max over the interior of one state (standalone pass)
+// ---------------------------------------------------------------------------
+__global__ void cfl_kernel(Geometry g, Physics ph, const double* __restrict__ q, DevState* st) {
+    double lam = 0.0;
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
+        const U4 u = load4(q, g.plane, cidx(g, i, j));
+        lam = fmax(lam, wave_speed(g, ph, u));
+    }
+    block_max_atomic(lam, &st->lam[st->lam_idx]);
+}
+
+__global__ void reset_lam_kernel(DevState* st) {
+    st->lam[st->lam_idx] = 0ull;
+}
+
+// Per-step Setup: dt from the wave-speed max (cfl_system's final lines,
+// crates/cfd_solver/src/lib.rs:671-676) or fixed_dt, and the stop test of the
+// case drivers' `if t >= T_FINAL break`.
+__global__ void step_setup_kernel(Physics ph, DevState* st) {
+    if (!st->active) return;
+    if (st->nonphysical) {
+        st->active = 0;
+        return;
+    }
+    if (st->stop_at_t && st->time >= st->t_stop) {
+        st->active = 0;
+        return;
+    }
+    double dt;
+    if (ph.fixed_dt > 0.0) {
+        dt = ph.fixed_dt;
+    } else {
+        const double lam = __longlong_as_double((long long)st->lam[st->lam_idx]);
+        dt = lam > 0.0 ? ph.cfl / lam : INFINITY;
+    }
+    st->dt = dt;
+    const int nxt = st->lam_idx ^ 1;
+    st->lam[nxt] = 0ull;
+    st->lam_idx = nxt;
+}
+
+// ---------------------------------------------------------------------------
+// Halo + Boundary for a whole state (after upload / geometry changes)
+// ---------------------------------------------------------------------------
+__global__ void fill_ghosts_y_kernel(Geometry g, Physics ph, double* q) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nx) return;
+    const long long P = g.plane;
+    const double gm1 = ph.gamma - 1.0;
+    if (ph.periodic_y) {
+        for (int k = 0; k < NG; ++k) {
+            store4(q, P, cidx(g, i, -NG + k), load4(q, P, cidx(g, i, g.ny - NG + k)));
+            store4(q, P, cidx(g, i, g.ny + k), load4(q, P, cidx(g, i, k)));
+        }
+    } else {
+        store4(q, P, cidx(g, i, -1), bc_ghost(ph.bc[2], 2, load4(q, P, cidx(g, i, 0)), gm1));
+        store4(q, P, cidx(g, i, g.ny), bc_ghost(ph.bc[3], 3, load4(q, P, cidx(g, i, g.ny - 1)), gm1));
+    }
+}
+__global__ void fill_ghosts_x_kernel(Geometry g, Physics ph, double* q) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= g.ny) return;
+    const long long P = g.plane;
+    const double gm1 = ph.gamma - 1.0;
+    if (ph.periodic_x) {
+        for (int k = 0; k < NG; ++k) {
+            store4(q, P, cidx(g, -NG + k, j), load4(q, P, cidx(g, g.nx - NG + k, j)));
+            store4(q, P, cidx(g, g.nx + k, j), load4(q, P, cidx(g, k, j)));
+        }
+    } else {
+        const U4 u0 = load4(q, P, cidx(g, 0, j));
+        store4(q, P, cidx(g, -1, j), bc_ghost(ph.bc[0], 0, u0, gm1));
+        if (ph.parabolic_inflow) {
+            const double y = centre(g.lo[1], g.h[1], j);
+            const double um = ph.inflow_u_max, hh = ph.inflow_height, rho = ph.inflow_rho;
+            const double uy = 4.0 * um * y * (hh - y) / (hh * hh);
+            const U4 c = prim_to_cons(rho, uy, 0.0, pressure_d(u0, gm1), gm1);
+            store4(q, P, cidx(g, -1, j), c);
+            store4(q, P, cidx(g, -2, j), c);
+        }
+        store4(q, P, cidx(g, g.nx, j), bc_ghost(ph.bc[1], 1, load4(q, P, cidx(g, g.nx - 1, j)), gm1));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// IBM
+// ---------------------------------------------------------------------------
+
+// refresh_cylinder_mask, crates/cfd_ibm/src/lib.rs:155-183 (static bodies: the
+// flip happens on the first call only).
+__global__ void geometry_kernel(Geometry g, const double* __restrict__ cyl, int ncyl, U4 stagnant, U4 ambient,
+                                double* q, uint8_t* mask) {
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
+        const double cx = centre(g.lo[0], g.h[0], i), cy = centre(g.lo[1], g.h[1], j);
+        bool inside = false;
+        for (int b = 0; b < ncyl && !inside; ++b) {
+            const double dx = __dsub_rn(cx, cyl[3 * b]), dy = __dsub_rn(cy, cyl[3 * b + 1]);
+            const double sd = __dsub_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy))), cyl[3 * b + 2]);
+            inside = sd < 0.0;
+        }
+        const long long o = cidx(g, i, j);
+        const bool was = mask[o] != 0;
+        if (inside && !was) {
+            mask[o] = 1;
+            store4(q, g.plane, o, stagnant);
+        } else if (!inside && was) {
+            mask[o] = 0;
+            store4(q, g.plane, o, ambient);
+        }
+    }
+}
+
+// sample_trilinear restricted to the z = centre plane (the z weight is exactly
+// 1 on the cell layer and 0 on the ghost layers), crates/cfd_ibm/src/lib.rs:106-149.
+__device__ __forceinline__ bool sample_bilinear(const Geometry& g, const Physics& ph, const double* q,
+                                                const uint8_t* mask, int lo_i, int lo_j, double tx, double ty,
+                                                double out[5]) {
+    const double gm1 = ph.gamma - 1.0;
+    double acc[5] = {0, 0, 0, 0, 0};  // rho, u, v, p, t
+    double total = 0.0;
+    for (int di = 0; di < 2; ++di) {
+        const double wx = di == 0 ? 1.0 - tx : tx;
+        for (int dj = 0; dj < 2; ++dj) {
+            const double wy = dj == 0 ? 1.0 - ty : ty;
+            const long long o = cidx(g, lo_i + di, lo_j + dj);
+            if (mask[o]) continue;
+            const U4 u = load4(q, g.plane, o);
+            if (!isfinite(u.r) || u.r <= 0.0) continue;
+            const double w = wx * wy;
+            const double inv = 1.0 / u.r;
+            const double vu = u.mx * inv, vv = u.my * inv;
+            const double ke = 0.5 * u.r * (vu * vu + vv * vv);
+            const double p = gm1 * (u.E - ke);
+            const double t = p * inv / ph.r_gas;
+            acc[0] += w * u.r;
+            acc[1] += w * vu;
+            acc[2] += w * vv;
+            acc[3] += w * p;
+            acc[4] += w * t;
+            total += w;
+        }
+    }
+    if (total < 1e-12) return false;
+    const double inv = 1.0 / total;
+    for (int k = 0; k < 5; ++k) out[k] = acc[k] * inv;
+    return true;
+}
+
+// Mirror (apply_ibm_ghost_bc, crates/cfd_ibm/src/lib.rs:258-289) of every solid
+// ghost cell, recording its pre-mirror value for the emulated z-ghost of the
+// staircase wall force.  One thread per ghost cell.
+__global__ void ibm_mirror_kernel(Geometry g, Physics ph, Ibm ib, double* q, const uint8_t* __restrict__ mask,
+                                  DevState* st, int stage) {
+    if (!st->active) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ib.n_ghost) return;
+    const IbmGhostDev gh = ib.ghosts[k];
+    const int j = (int)(gh.cell / g.nx), i = (int)(gh.cell - (long long)j * g.nx);
+    const long long o = cidx(g, i, j);
+    const U4 pre = load4(q, g.plane, o);
+    double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
+    zf[0] = pre.r; zf[1] = pre.mx; zf[2] = pre.my; zf[3] = pre.E;
+    if (stage == 0 || stage == 3) {
+        double* z0 = ib.zg0 + 4LL * k;
+        z0[0] = pre.r; z0[1] = pre.mx; z0[2] = pre.my; z0[3] = pre.E;
+    }
+    if (!gh.valid) return;
+    double img[5];
+    if (!sample_bilinear(g, ph, q, mask, gh.lo_i, gh.lo_j, gh.tx, gh.ty, img)) return;
+    // u_ghost = 2 u_wall - u_image with u_wall = 0; rho, p, T from the image
+    const U4 m = prim_to_cons(img[0], 2.0 * 0.0 - img[1], 2.0 * 0.0 - img[2], img[3], ph.gamma - 1.0);
+    store4(q, g.plane, o, m);
+}
+
+// Output phase: MarkerForce (compute_marker_loadings, crates/cfd_ibm/src/
+// lib.rs:442-480) in block 0 and WallForce (compute_wall_forces, :309-362) over
+// blocks 1..: each block reduces its share in a fixed order and writes 6
+// partial sums; the last block to finish adds the partials in block order
+// (deterministic), publishes both forces and appends the marker force to the
+// substage history.
+constexpr int FORCE_THREADS = 256;
+
+__global__ void __launch_bounds__(FORCE_THREADS) ibm_forces_kernel(Geometry g, Physics ph, Ibm ib,
+                                                                   const double* __restrict__ q,
+                                                                   const uint8_t* __restrict__ mask, DevState* st,
+                                                                   int stage) {
+    if (!st->active) return;
+    __shared__ double red[6][FORCE_THREADS];
+    __shared__ bool last;
+    const int tid = threadIdx.x;
+    const double gm1 = ph.gamma - 1.0;
+    double f[6] = {0, 0, 0, 0, 0, 0};
+    if (blockIdx.x == 0) {
+        for (int m = tid; m < ib.n_markers; m += blockDim.x) {
+            const MarkerDev mk = ib.markers[m];
+            if (!mk.valid) continue;
+            double img[5];
+            if (!sample_bilinear(g, ph, q, mask, mk.lo_i, mk.lo_j, mk.tx, mk.ty, img)) continue;
+            if (!(isfinite(img[3]) && isfinite(img[4]) && isfinite(img[1]) && isfinite(img[2]))) continue;
+            const double usd[3] = {img[1] - mk.wall_velocity[0], img[2] - mk.wall_velocity[1], 0.0 - mk.wall_velocity[2]};
+            const double udotn = usd[0] * mk.normal[0] + usd[1] * mk.normal[1] + usd[2] * mk.normal[2];
+            const double mu = viscosity(ph, img[4]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double ut = usd[d] - udotn * mk.normal[d];
+                f[d] += -img[3] * mk.normal[d] * mk.area;
+                f[3 + d] += mu * ut / ib.sample_offset * mk.area;
+            }
+        }
+    } else {
+        const int k = (blockIdx.x - 1) * blockDim.x + tid;
+        if (k < ib.n_ghost) {
+            const double dx = g.h[0], dy = g.h[1], dz = g.h[2];
+            const double face_area[3] = {dy * dz, dx * dz, dx * dy};
+            const double dn[3] = {dx, dy, dz};
+            const double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
+            const double* z0 = ib.zg0 + 4LL * k;
+            const long long cell = ib.ghosts[k].cell;
+            const int j = (int)(cell / g.nx), i = (int)(cell - (long long)j * g.nx);
+            // the six face neighbours of compute_wall_forces: +x, -x, +y, -y, then the
+            // two z-ghost layers of the 2-D mesh (never solid; their state is the
+            // slip-wall copy of this cell, RK-advanced with a zero rhs)
+#pragma unroll
+            for (int nb = 0; nb < 6; ++nb) {
+                U4 u;
+                int dim;
+                double sign;
+                if (nb < 4) {
+                    const int ni = i + (nb == 0 ? 1 : (nb == 1 ? -1 : 0));
+                    const int nj = j + (nb == 2 ? 1 : (nb == 3 ? -1 : 0));
+                    const long long o = cidx(g, ni, nj);
+                    if (mask[o]) continue;
+                    u = load4(q, g.plane, o);
+                    dim = nb < 2 ? 0 : 1;
+                    sign = (nb & 1) ? -1.0 : 1.0;
+                } else {
+                    double zv[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        if (stage == 1) zv[c] = 0.75 * z0[c] + 0.25 * (zf[c] + 0.0);
+                        else if (stage == 2) zv[c] = (1.0 / 3.0) * z0[c] + (2.0 / 3.0) * (zf[c] + 0.0);
+                        else zv[c] = zf[c] + 0.0;
+                    }
+                    u = U4{zv[0], zv[1], zv[2], zv[3]};
+                    dim = 2;
+                    sign = nb == 4 ? 1.0 : -1.0;
+                }
+                const double p = pressure_d(u, gm1);
+                f[dim] -= p * sign * face_area[dim];
+                const double inv = 1.0 / u.r;
+                const double vel0 = u.mx * inv, vel1 = u.my * inv;
+                const double ke = 0.5 * u.r * (vel0 * vel0 + vel1 * vel1);
+                const double t = gm1 * (u.E - ke) * inv / ph.r_gas;
+                const double mu = viscosity(ph, t);
+                const double vel[3] = {vel0, vel1, 0.0};
+#pragma unroll
+                for (int td = 0; td < 3; ++td)
+                    if (td != dim) f[3 + td] += mu * vel[td] / (0.5 * dn[dim]) * face_area[dim];
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 6; ++d) red[d][tid] = f[d];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (tid < s)
+#pragma unroll
+            for (int d = 0; d < 6; ++d) red[d][tid] += red[d][tid + s];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        double* part = ib.partials + 6LL * blockIdx.x;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) part[d] = red[d][0];
+        __threadfence();
+        const unsigned int done = atomicAdd(ib.counter, 1u);
+        last = done == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && tid == 0) {
+        __threadfence();
+        const volatile double* part = ib.partials;
+        double wall[6] = {0, 0, 0, 0, 0, 0};
+        for (int b = 1; b < (int)gridDim.x; ++b)
+            for (int d = 0; d < 6; ++d) wall[d] += part[6 * b + d];
+        for (int d = 0; d < 6; ++d) {
+            ib.force_out[d] = part[d];
+            ib.force_out[6 + d] = wall[d];
+        }
+        if (ib.history && st->hist_pos < st->hist_cap) {
+            for (int d = 0; d < 6; ++d) ib.history[6 * st->hist_pos + d] = part[d];
+            st->hist_pos += 1;
+        }
+        *ib.counter = 0u;  // ready for the next launch
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Utilities
+// ---------------------------------------------------------------------------
+
+// Strided AoS (5 doubles per cell: rho, rho_u, rho_v, rho_w, rho_e) <-> SoA.
+__global__ void pack_kernel(Geometry g, const double* src, int64_t si, int64_t sj, int64_t sv, double* q,
+                            double* dst, int to_device) {
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
+        const long long h = (long long)i * si + (long long)j * sj;
+        const long long o = cidx(g, i, j);
+        if (to_device) {
+            q[o] = src[h];
+            q[g.plane + o] = src[h + sv];
+            q[2 * g.plane + o] = src[h + 2 * sv];
+            q[3 * g.plane + o] = src[h + 4 * sv];
+        } else {
+            dst[h] = q[o];
+            dst[h + sv] = q[g.plane + o];
+            dst[h + 2 * sv] = q[2 * g.plane + o];
+            dst[h + 3 * sv] = 0.0;
+            dst[h + 4 * sv] = q[3 * g.plane + o];
+        }
+    }
+}
+
+__device__ __forceinline__ double vortex_rho(const efvm_vortex& v, double t, double x, double y, U4* cons) {
+    const double PI = 3.141592653589793;
+    const double cx = v.cx0 + v.mean_u * t, cy = v.cy0 + v.mean_v * t;
+    double dx = x - cx, dy = y - cy;
+    if (v.min_image) {
+        dx = dx - v.len_x * rint(dx / v.len_x);
+        dy = dy - v.len_y * rint(dy / v.len_y);
+    }
+    const double r2 = dx * dx + dy * dy;
+    const double f = exp(0.5 * (1.0 - r2));
+    const double du = -v.beta / (2.0 * PI) * dy * f;
+    const double dv = v.beta / (2.0 * PI) * dx * f;
+    const double dtemp = -(v.gamma - 1.0) * v.beta * v.beta / (8.0 * v.gamma * PI * PI) * exp(1.0 - r2);
+    const double temp = 1.0 + dtemp;
+    const double rho = pow(temp, 1.0 / (v.gamma - 1.0));
+    if (cons) {
+        const double p = pow(rho, v.gamma);
+        *cons = prim_to_cons(rho, v.mean_u + du, v.mean_v + dv, p, v.gamma - 1.0);
+    }
+    return rho;
+}
+
+__global__ void init_vortex_kernel(Geometry g, efvm_vortex v, double* q) {
+    const long long n = (long long)g.nx * g.ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
+        U4 c;
+        vortex_rho(v, 0.0, centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j), &c);
+        store4(q, g.plane, cidx(g, i, j), c);
+    }
+}
+
+// Per-block partials of sum |rho - rho_exact| and max |rho - rho_exact|.
+__global__ void density_error_kernel(Geometry g, efvm_vortex v, const double* __restrict__ q,
+                                     const DevState* st, double* partial) {
+    __shared__ double s1[256], s2[256];
+    const double t = st->time;
+    double a = 0.0, m = 0.0;
+    const long long n = (long long)g.nx * g.ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / g.nx), i = (int)(k - (long long)j * g.nx);
+        const double ex = vortex_rho(v, t, centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j), nullptr);
+        const double e = fabs(q[cidx(g, i, j)] - ex);
+        a += e;
+        m = fmax(m, e);
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            s1[threadIdx.x] += s1[threadIdx.x + s];
+            s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + s]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = s1[0];
+        partial[2 * blockIdx.x + 1] = s2[0];
+    }
+}
+
+__global__ void total_mass_kernel(Geometry g, const double* __restrict__ q, double* partial) {
+    __shared__ double s1[256];
+    double a = 0.0;
+    const long long n = (long long)g.nx * g.ny;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / g.nx), i = (int)(k - (long long)j * g.nx);
+        a += q[cidx(g, i, j)] * g.cell_volume;
+    }
+    s1[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) s1[threadIdx.x] += s1[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = s1[0];
+}
+
+__global__ void check_state_kernel(Geometry g, Physics ph, const double* __restrict__ q, DevState* st) {
+    const long long n = (long long)g.nx * g.ny;
+    const double gm1 = ph.gamma - 1.0;
+    int bad = 0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(k / g.nx), i = (int)(k - (long long)j * g.nx);
+        const U4 u = load4(q, g.plane, cidx(g, i, j));
+        if (!(u.r > 0.0)) bad |= 1;
+        if (!(pressure_d(u, gm1) > 0.0)) bad |= 2;
+        if (u.r != u.r || u.mx != u.mx || u.my != u.my || u.E != u.E) bad |= 4;
+    }
+    if (bad) atomicOr(&st->nonphysical, bad);
+}
+
+// ---------------------------------------------------------------------------
+// Host launch wrappers
+// ---------------------------------------------------------------------------
+static int grid_for(long long n, int block) {
+    long long b = (n + block - 1) / block;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)b;
+}
+
+// Rows per warp: enough warps for a few waves over the 148 SMs, at most 64
+// rows (each strip re-evaluates one y face at its first row).
+static int rows_per_warp(int nx, int ny) {
+    const long long strips = (nx + STRIP - 1) / STRIP;
+    const long long target_warps = 148LL * 16 * 3;
+    long long rows = (strips * ny) / target_warps;
+    if (rows < 4) rows = 4;
+    if (rows > 64) rows = 64;
+    return (int)rows;
+}
+
+template <int SCHEME, int RECON, class R>
+static void launch_stage_t(const StageArgs& a, cudaStream_t s) {
+    const int rows = rows_per_warp(a.g.nx, a.g.ny);
+    const int strips = (a.g.nx + STRIP - 1) / STRIP;
+    dim3 block(32 * WPB);
+    dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
+    // Resident blocks per SM, measured at 4096^2: the FP64 flux is fastest at 96
+    // registers/thread (5 blocks of 4 warps), the FP32 flux at 64 (8 blocks).
+    constexpr int MINB = sizeof(R) == sizeof(double) ? 5 : 8;
+    stage_kernel<SCHEME, RECON, R, MINB><<<grid, block, 0, s>>>(a, rows);
+}
+
+template <class R>
+static void launch_stage_r(const StageArgs& a, cudaStream_t s) {
+    const bool muscl = a.ph.reconstruction == EFVM_RECON_MUSCL;
+    switch (a.ph.flux_scheme) {
+        case EFVM_FLUX_RUSANOV:
+            muscl ? launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R>(a, s)
+                  : launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R>(a, s);
+            break;
+        case EFVM_FLUX_HLLC_TEXTBOOK:
+            muscl ? launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R>(a, s)
+                  : launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R>(a, s);
+            break;
+        default:
+            muscl ? launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R>(a, s)
+                  : launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R>(a, s);
+    }
+}
+
+int launch_stage(const StageArgs& a, int, int, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_r<float>(a, s);
+    else launch_stage_r<double>(a, s);
+    return 1;
+}
+
+int launch_fill_ghosts(const Geometry& g, const Physics& ph, double* q, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    fill_ghosts_x_kernel<<<(g.ny + 127) / 128, 128, 0, s>>>(g, ph, q);
+    fill_ghosts_y_kernel<<<(g.nx + 127) / 128, 128, 0, s>>>(g, ph, q);
+    return 2;
+}
+
+int launch_cfl(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    reset_lam_kernel<<<1, 1, 0, s>>>(st);
+    cfl_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, s>>>(g, ph, q, st);
+    return 2;
+}
+
+int launch_step_setup(const Physics& ph, DevState* st, void* stream) {
+    step_setup_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(ph, st);
+    return 1;
+}
+
+__global__ void set_control_kernel(DevState* st, int active, int stop_at_t, double t_stop, long long hist_cap) {
+    st->active = active;
+    st->stop_at_t = stop_at_t;
+    st->t_stop = t_stop;
+    st->hist_pos = 0;
+    st->hist_cap = hist_cap;
+}
+
+int launch_set_control(DevState* st, int active, int stop_at_t, double t_stop, long long hist_cap, void* stream) {
+    set_control_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(st, active, stop_at_t, t_stop, hist_cap);
+    return 1;
+}
+
+int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double* stagnant, const double* ambient,
+                    double* q, uint8_t* mask, void* stream) {
+    const U4 sg{stagnant[0], stagnant[1], stagnant[2], stagnant[4]};
+    const U4 am{ambient[0], ambient[1], ambient[2], ambient[4]};
+    geometry_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(g, cyl, ncyl, sg, am, q,
+                                                                                               mask);
+    return 1;
+}
+
+int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, const uint8_t* mask, DevState* st,
+               int stage, int do_mirror, int do_forces, int, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    int n = 0;
+    if (do_mirror && ib.n_ghost > 0) {
+        ibm_mirror_kernel<<<(ib.n_ghost + 127) / 128, 128, 0, s>>>(g, ph, ib, q, mask, st, stage);
+        ++n;
+    }
+    if (do_forces) {
+        const int blocks = 1 + (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS;
+        ibm_forces_kernel<<<blocks, FORCE_THREADS, 0, s>>>(g, ph, ib, q, mask, st, stage);
+        n += 1;
+    }
+    return n;
+}
+
+int launch_pack(const Geometry& g, const double* src, int64_t si, int64_t sj, int64_t sv, double* q, int to_device,
+                void* stream) {
+    pack_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, src, si, sj, sv, q, const_cast<double*>(src), to_device);
+    return 1;
+}
+
+int launch_init_vortex(const Geometry& g, const efvm_vortex& v, double* q, void* stream) {
+    init_vortex_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(g, v, q);
+    return 1;
+}
+
+int launch_density_error(const Geometry& g, const efvm_vortex& v, const double* q, const DevState* st,
+                         double* partial, int nblocks, void* stream) {
+    density_error_kernel<<<nblocks, 256, 0, (cudaStream_t)stream>>>(g, v, q, st, partial);
+    return 1;
+}
+
+int launch_total_mass(const Geometry& g, const double* q, double* partial, int nblocks, void* stream) {
+    total_mass_kernel<<<nblocks, 256, 0, (cudaStream_t)stream>>>(g, q, partial);
+    return 1;
+}
+
+int launch_check_state(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream) {
+    check_state_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(g, ph, q, st);
+    return 1;
+}
+
+}  // namespace efvm

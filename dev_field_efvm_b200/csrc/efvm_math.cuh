@@ -1,0 +1,164 @@
+// efvm_math.cuh — the gas model, numerical fluxes and limiters on the device,
+// templated on the arithmetic type R (double for the plain path, float for the
+// FP32-flux path).  Each function restates the reference routine it cites
+// (crates/cfd_eos/src/lib.rs, crates/cfd_riemann/src/lib.rs,
+// crates/cfd_solver/src/lib.rs) with the same evaluation order; the compiler
+// may fuse a multiply and an add into one FMA, which moves results by at most
+// an ulp per operation.
+//
+// 2-D specialisation: states carry (rho, m_n, m_t, E) in the frame of the face
+// normal; rho_w and w are identically zero, so every `+ w*w` / `+ rho_w^2`
+// term of the 3-D formulas adds an exact zero and is dropped.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace efvm {
+
+template <class R>
+struct Q4 {
+    R r, mn, mt, E;
+};
+
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double fmax_(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float fmax_(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fmin_(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float fmin_(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double fabs_(double a) { return fabs(a); }
+__device__ __forceinline__ float fabs_(float a) { return fabsf(a); }
+
+__device__ __forceinline__ double div_(double a, double b) { return a / b; }
+__device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+
+// Gas-dynamic quantities of one face state, each computed once per face side:
+// 1/rho, normal and tangential velocity, |v|^2, pressure and sound speed
+// (IdealGas::cons_to_prim / pressure / sound_speed, crates/cfd_eos/src/lib.rs:44-68,
+// with the kinetic energy taken from the velocities and one reciprocal of rho).
+template <class R>
+struct Side {
+    R inv, un, ut, q, p, a;
+};
+template <class R>
+__device__ __forceinline__ Side<R> side_of(const Q4<R>& u, R gamma, R gm1) {
+    Side<R> s;
+    s.inv = div_(R(1), u.r);
+    s.un = u.mn * s.inv;
+    s.ut = u.mt * s.inv;
+    s.q = s.un * s.un + s.ut * s.ut;
+    s.p = gm1 * (u.E - R(0.5) * u.r * s.q);
+    s.a = sqrt_(gamma * s.p * s.inv);
+    return s;
+}
+
+// physical_flux_inline along the face normal for a state with known normal
+// velocity and pressure, crates/cfd_riemann/src/lib.rs:21-43.
+template <class R>
+__device__ __forceinline__ Q4<R> physical_flux(R rho, R un, R ut, R E, R p) {
+    const R m = rho * un;
+    Q4<R> f;
+    f.r = m;
+    f.mn = m * un + p;
+    f.mt = (rho * ut) * un;
+    f.E = (E + p) * un;
+    return f;
+}
+
+// Rusanov::flux_inline, crates/cfd_riemann/src/lib.rs:222-240
+template <class R>
+__device__ __forceinline__ Q4<R> rusanov_flux(const Q4<R>& L, const Q4<R>& Rr, R gamma, R gm1) {
+    const Side<R> l = side_of(L, gamma, gm1), r = side_of(Rr, gamma, gm1);
+    const Q4<R> fl = physical_flux(L.r, l.un, l.ut, L.E, l.p);
+    const Q4<R> fr = physical_flux(Rr.r, r.un, r.ut, Rr.E, r.p);
+    const R hl = R(0.5) * fmax_(fabs_(l.un) + l.a, fabs_(r.un) + r.a);
+    Q4<R> f;
+    f.r = R(0.5) * (fl.r + fr.r) - hl * (Rr.r - L.r);
+    f.mn = R(0.5) * (fl.mn + fr.mn) - hl * (Rr.mn - L.mn);
+    f.mt = R(0.5) * (fl.mt + fr.mt) - hl * (Rr.mt - L.mt);
+    f.E = R(0.5) * (fl.E + fr.E) - hl * (Rr.E - L.E);
+    return f;
+}
+
+// Hllc::flux_with_thornber + thornber_reconstruct + star_state,
+// crates/cfd_riemann/src/lib.rs:395-506,619-644, in an equivalent form that
+// evaluates each quantity once:
+//  * the Thornber blend keeps rho and the internal energy, hence p and a, so
+//    the pressures and sound speeds of the blended states are those of the
+//    inputs (the reference's cached path relies on the same identity, :586-588);
+//  * the blended normal/tangential velocities are used directly instead of
+//    re-dividing the rebuilt momenta by rho;
+//  * the upwind side K (left for s_l >= 0 or s_* >= 0, else right) is selected
+//    first and one star state is built, F = F(U_K) + s_K (U*_K - U_K), with
+//    rho_* = f_K/(s_K - s_*) and p_K/(rho_K (s_K - u_K)) = p_K/f_K where
+//    f_K = rho_K (s_K - u_K) is the same factor that enters s_*.
+// The results agree with the literal evaluation to a few ulps.
+template <class R, bool THORNBER>
+__device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R gamma, R gm1) {
+    const Side<R> l = side_of(L, gamma, gm1), r = side_of(Rr, gamma, gm1);
+    R lcn = l.un, lct = l.ut, rcn = r.un, rct = r.ut, ELc = L.E, ERc = Rr.E;
+    if (THORNBER) {
+        const R vmax2 = fmax_(l.q, r.q);
+        const R amax = fmax_(l.a, r.a);
+        const R z = (vmax2 >= amax * amax) ? R(1) : div_(sqrt_(vmax2), amax);
+        const R avgn = R(0.5) * (l.un + r.un), avgt = R(0.5) * (l.ut + r.ut);
+        const R hz = R(0.5) * z;
+        const R dvn = hz * (l.un - r.un), dvt = hz * (l.ut - r.ut);
+        lcn = avgn + dvn;
+        lct = avgt + dvt;
+        rcn = avgn - dvn;
+        rct = avgt - dvt;
+        ELc = L.E + R(0.5) * L.r * ((lcn * lcn + lct * lct) - l.q);
+        ERc = Rr.E + R(0.5) * Rr.r * ((rcn * rcn + rct * rct) - r.q);
+    }
+    const R s_l = fmin_(lcn - l.a, rcn - r.a);
+    const R s_r = fmax_(lcn + l.a, rcn + r.a);
+    const R fac_l = L.r * (s_l - lcn);
+    const R fac_r = Rr.r * (s_r - rcn);
+    const R s_star = div_((r.p - l.p) + fac_l * lcn - fac_r * rcn, fac_l - fac_r);
+    const bool useL = (s_l >= R(0)) || (s_star >= R(0));
+    const R rK = useL ? L.r : Rr.r;
+    const R uK = useL ? lcn : rcn;
+    const R tK = useL ? lct : rct;
+    const R EK = useL ? ELc : ERc;
+    const R pK = useL ? l.p : r.p;
+    const R iK = useL ? l.inv : r.inv;
+    Q4<R> f = physical_flux(rK, uK, tK, EK, pK);
+    if (s_l < R(0) && (s_star >= R(0) || s_r >= R(0))) {  // one of the two star regions
+        const R sK = useL ? s_l : s_r;
+        const R facK = useL ? fac_l : fac_r;
+        const R rho_star = div_(facK, sK - s_star);
+        const R e_star = EK * iK + (s_star - uK) * (s_star + div_(pK, facK));
+        f.r = f.r + sK * (rho_star - rK);
+        f.mn = f.mn + sK * (rho_star * s_star - rK * uK);
+        f.mt = f.mt + sK * (rho_star * tK - rK * tK);
+        f.E = f.E + sK * (rho_star * e_star - EK);
+    }
+    return f;
+}
+
+template <int SCHEME, class R>
+__device__ __forceinline__ Q4<R> face_flux(const Q4<R>& L, const Q4<R>& Rr, R gamma, R gm1) {
+    if (SCHEME == EFVM_FLUX_RUSANOV) return rusanov_flux(L, Rr, gamma, gm1);
+    if (SCHEME == EFVM_FLUX_HLLC_TEXTBOOK) return hllc_flux<R, false>(L, Rr, gamma, gm1);
+    return hllc_flux<R, true>(L, Rr, gamma, gm1);
+}
+
+// minmod / monotonized_central, crates/cfd_solver/src/lib.rs:170-192
+template <class R>
+__device__ __forceinline__ R minmod(R a, R b) {
+    if (a * b <= R(0)) return R(0);
+    return fabs_(a) < fabs_(b) ? a : b;
+}
+template <class R>
+__device__ __forceinline__ R monotonized_central(R a, R b) {
+    if (a * b <= R(0)) return R(0);
+    const R s = a > R(0) ? R(1) : R(-1);
+    return s * fmin_(fmin_(R(2) * fabs_(a), R(2) * fabs_(b)), R(0.5) * fabs_(a + b));
+}
+template <class R>
+__device__ __forceinline__ R limit(int limiter, R fwd, R bwd) {
+    return limiter == EFVM_LIMITER_MC ? monotonized_central(fwd, bwd) : minmod(fwd, bwd);
+}
+
+}  // namespace efvm

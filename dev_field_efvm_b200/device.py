@@ -1,0 +1,207 @@
+"""ctypes binding of libefvm_b200.so (the C-ABI of include/efvm.h).
+
+This is the product path: every call goes to the CUDA library.  There is no
+CPU fallback; importing a context without the built library or without a CUDA
+device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libefvm_b200.so")
+_LIB = None
+
+# every entry point of include/efvm.h
+EXPORTS = (
+    "efvm_abi_version", "efvm_create", "efvm_destroy", "efvm_last_error", "efvm_upload_state",
+    "efvm_download_state", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
+    "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
+    "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
+)
+
+
+class EfvmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"efvm error {abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Load the library (build it first with ``python -m dev_field_efvm_b200.build``)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"{p} is missing: build it with `python -m dev_field_efvm_b200.build`")
+    L = C.CDLL(p)
+    vp, dp, i64, i32 = C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.c_int32
+    L.efvm_abi_version.restype = C.c_int
+    L.efvm_create.argtypes = [C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), C.POINTER(vp)]
+    L.efvm_destroy.argtypes = [vp]
+    L.efvm_last_error.restype = C.c_char_p
+    L.efvm_last_error.argtypes = [vp]
+    L.efvm_upload_state.argtypes = [vp, dp, i64, i64, i64]
+    L.efvm_download_state.argtypes = [vp, dp, i64, i64, i64]
+    L.efvm_get_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
+    L.efvm_set_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
+    L.efvm_substep.argtypes = [vp]
+    L.efvm_step.argtypes = [vp, i64, i32, C.c_double, dp, C.POINTER(abi.EfvmStepInfo)]
+    L.efvm_cfl.argtypes = [vp, dp]
+    L.efvm_set_cylinders.argtypes = [vp, C.POINTER(abi.EfvmCylinder), i32, dp]
+    L.efvm_marker_force.argtypes = [vp, dp]
+    L.efvm_wall_force.argtypes = [vp, dp]
+    L.efvm_ibm_counts.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
+    L.efvm_get_solid_mask.argtypes = [vp, C.POINTER(C.c_uint8)]
+    L.efvm_density_error.argtypes = [vp, C.POINTER(abi.EfvmVortex), dp]
+    L.efvm_init_vortex.argtypes = [vp, C.POINTER(abi.EfvmVortex)]
+    L.efvm_total_mass.argtypes = [vp, dp]
+    L.efvm_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.efvm_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
+    if L.efvm_abi_version() != abi.ABI_VERSION:
+        raise ImportError("libefvm_b200.so ABI version mismatch")
+    if path is None:
+        _LIB = L
+    return L
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Context:
+    """One case on the GPU: an efvm_ctx and its device state."""
+
+    def __init__(self, grid: abi.EfvmGrid, params: abi.EfvmParams):
+        self.L = load()
+        self.grid, self.params = grid, params
+        self.nx, self.ny = grid.nx, grid.ny
+        h = C.c_void_p()
+        rc = self.L.efvm_create(C.byref(grid), C.byref(params), C.byref(h))
+        if rc != abi.OK:
+            raise EfvmError(rc, self.L.efvm_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != abi.OK:
+            raise EfvmError(rc, self.L.efvm_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.efvm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # conserved state as an (ny, nx, 5) array: rho, rho_u, rho_v, rho_w, rho_e
+    def upload(self, u: np.ndarray) -> None:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.shape == (self.ny, self.nx, 5), u.shape
+        self._check(self.L.efvm_upload_state(self.h, _dp(u), 5, 5 * self.nx, 1))
+
+    def upload_ptr(self, ptr: int, si: int, sj: int, sv: int) -> None:
+        self._check(self.L.efvm_upload_state(self.h, C.cast(ptr, C.POINTER(C.c_double)), si, sj, sv))
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.ny, self.nx, 5))
+        self._check(self.L.efvm_download_state(self.h, _dp(out), 5, 5 * self.nx, 1))
+        return out
+
+    def download_ptr(self, ptr: int, si: int, sj: int, sv: int) -> None:
+        self._check(self.L.efvm_download_state(self.h, C.cast(ptr, C.POINTER(C.c_double)), si, sj, sv))
+
+    def substep(self) -> None:
+        self._check(self.L.efvm_substep(self.h))
+
+    def step(self, n_steps: int, t_stop: float | None = None, history: bool = False):
+        info = abi.EfvmStepInfo()
+        hist = np.zeros((3 * max(n_steps, 1), 6)) if history else None
+        rc = self.L.efvm_step(self.h, int(n_steps), 1 if t_stop is not None else 0,
+                              float(t_stop if t_stop is not None else 0.0),
+                              _dp(hist) if history else None, C.byref(info))
+        self._check(rc)
+        if history:
+            return info, hist[: info.substeps_done]
+        return info
+
+    def run_until(self, t_final: float, max_steps: int = 10_000_000):
+        return self.step(max_steps, t_stop=t_final)
+
+    def cfl(self) -> float:
+        d = C.c_double()
+        self._check(self.L.efvm_cfl(self.h, C.byref(d)))
+        return d.value
+
+    def solver_state(self) -> abi.EfvmSolverState:
+        s = abi.EfvmSolverState()
+        self._check(self.L.efvm_get_solver_state(self.h, C.byref(s)))
+        return s
+
+    def set_solver_state(self, s: abi.EfvmSolverState) -> None:
+        self._check(self.L.efvm_set_solver_state(self.h, C.byref(s)))
+
+    def set_cylinders(self, cyls, freestream) -> None:
+        arr_t = abi.EfvmCylinder * max(len(cyls), 1)
+        ca = arr_t(*[abi.EfvmCylinder(*c) for c in cyls])
+        fs = np.ascontiguousarray(freestream, dtype=np.float64)
+        self._check(self.L.efvm_set_cylinders(self.h, ca, len(cyls), _dp(fs)))
+
+    def marker_force(self) -> np.ndarray:
+        out = np.zeros(6)
+        self._check(self.L.efvm_marker_force(self.h, _dp(out)))
+        return out
+
+    def wall_force(self) -> np.ndarray:
+        out = np.zeros(6)
+        self._check(self.L.efvm_wall_force(self.h, _dp(out)))
+        return out
+
+    def ibm_counts(self):
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self.L.efvm_ibm_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def solid_mask(self) -> np.ndarray:
+        out = np.zeros((self.ny, self.nx), dtype=np.uint8)
+        self._check(self.L.efvm_get_solid_mask(self.h, out.ctypes.data_as(C.POINTER(C.c_uint8))))
+        return out
+
+    def density_error(self, v: abi.EfvmVortex):
+        out = np.zeros(2)
+        self._check(self.L.efvm_density_error(self.h, C.byref(v), _dp(out)))
+        return float(out[0]), float(out[1])
+
+    def init_vortex(self, v: abi.EfvmVortex) -> None:
+        self._check(self.L.efvm_init_vortex(self.h, C.byref(v)))
+
+    def total_mass(self) -> float:
+        d = C.c_double()
+        self._check(self.L.efvm_total_mass(self.h, C.byref(d)))
+        return d.value
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self.L.efvm_get_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        self._check(self.L.efvm_launch_count(self.h, C.byref(n)))
+        return n.value

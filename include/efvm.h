@@ -1,0 +1,260 @@
+/*
+ * efvm.h — C-ABI of the B200 explicit finite-volume step (MUSCL/HLLC fluxes,
+ * viscous terms, SSP-RK3 stage update, CFL dt reduction, ghost-cell IBM fill and
+ * marker-load sum) of dev_field_efvm.
+ *
+ * Every entry point is a plain `extern "C"` function over plain pointers and
+ * sizes.  Every call returns an `int` status (efvm_status); `efvm_last_error`
+ * gives the message of the last failure on a context.  No C++ exception and no
+ * device trap crosses this boundary.
+ *
+ * Ownership: a context owns all of its device memory and one CUDA stream on the
+ * device that was current when it was created.  Host pointers are borrowed only
+ * for the duration of a call.  A context is not thread-safe (use one per
+ * thread); distinct contexts are independent.
+ *
+ * The reference interfaces each entry point replaces are cited as
+ * `path:line` inside the dev_field_efvm source tree (the Rust crates under
+ * `crates/` and the case drivers under `examples/`).
+ */
+#ifndef EFVM_H
+#define EFVM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EFVM_ABI_VERSION 1
+
+/* Status codes.  The reference panics or returns Option; the C-ABI returns a
+ * code instead (crates/cfd_boundary/src/lib.rs:516-518 panics on a half-periodic
+ * axis -> EFVM_ERR_INVALID_ARG here). */
+typedef enum {
+    EFVM_OK = 0,
+    EFVM_ERR_INVALID_ARG = 1,
+    EFVM_ERR_CUDA = 2,
+    EFVM_ERR_NONPHYSICAL = 3, /* rho<=0, p<=0 or a NaN appeared in the state */
+    EFVM_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+    EFVM_ERR_OOM = 5,
+    EFVM_ERR_UNSUPPORTED = 6
+} efvm_status;
+
+/* Boundary sides in FIELD's BoundarySide / PatchId order (XLo..ZHi = 0..5). */
+enum { EFVM_XLO = 0, EFVM_XHI = 1, EFVM_YLO = 2, EFVM_YHI = 3, EFVM_ZLO = 4, EFVM_ZHI = 5 };
+
+/* Stock boundary conditions, crates/cfd_boundary/src/lib.rs:172-362. */
+typedef enum {
+    EFVM_BC_SUPERSONIC_OUTFLOW = 0, /* zero-gradient copy (:173-189), registry default (:375-381) */
+    EFVM_BC_PERIODIC = 1,           /* halo wrap from the opposite slab (:197-216) */
+    EFVM_BC_SLIP_WALL = 2,          /* flip wall-normal momentum (:246-272) */
+    EFVM_BC_NO_SLIP_WALL = 3,       /* flip all momentum (:276-296) */
+    EFVM_BC_SYMMETRY = 4,           /* == slip wall (:299-310) */
+    EFVM_BC_SUPERSONIC_INFLOW = 5,  /* prescribed rho,u,v,w,p; T = p/(rho*287.058) (:220-243) */
+    EFVM_BC_SUBSONIC_INFLOW = 6,    /* prescribed rho,u,v,w,t; p from the interior (:314-337) */
+    EFVM_BC_PRESSURE_OUTLET = 7     /* prescribed p; rho,u from the interior (:341-362) */
+} efvm_bc_kind;
+
+typedef struct {
+    int32_t kind; /* efvm_bc_kind */
+    int32_t reserved;
+    double rho, u, v, w, p, t; /* parameters of the inflow/outlet kinds */
+} efvm_bc;
+
+/* A 2-D uniform mesh (FIELD UniformMeshConfig{nx,ny,nz,ng,bounds_lo,bounds_hi}
+ * with nz == 1 and ng == 2) plus one boundary condition per side
+ * (BoundaryRegistry, crates/cfd_boundary/src/lib.rs:370-449).  The z extent
+ * enters the CFL (crates/cfd_solver/src/lib.rs:659-661) and the marker area. */
+typedef struct {
+    int32_t nx, ny, nz, ng;
+    double lo[3], hi[3];
+    efvm_bc bc[6];
+} efvm_grid;
+
+typedef enum { EFVM_FLUX_RUSANOV = 0, EFVM_FLUX_HLLC = 1, EFVM_FLUX_HLLC_TEXTBOOK = 2 } efvm_flux_scheme;
+typedef enum { EFVM_RECON_FIRST_ORDER = 0, EFVM_RECON_MUSCL = 1 } efvm_reconstruction;
+typedef enum { EFVM_LIMITER_MINMOD = 0, EFVM_LIMITER_MC = 1 } efvm_limiter;
+typedef enum { EFVM_INTEGRATOR_RK3 = 0, EFVM_INTEGRATOR_EULER = 1 } efvm_integrator;
+typedef enum { EFVM_VISC_SUTHERLAND = 0, EFVM_VISC_CONSTANT = 1 } efvm_viscosity;
+/* FP64: everything in double.  FP32_FLUX: reconstruction and face fluxes in
+ * float, stage accumulation, RK combination and marker integral in double. */
+typedef enum { EFVM_PREC_FP64 = 0, EFVM_PREC_FP32_FLUX = 1 } efvm_precision;
+/* How MUSCL treats the periodic seam.  REFERENCE: the halo-ghost side of a seam
+ * face is not reconstructed and has zero slope (crates/cfd_solver/src/lib.rs:
+ * 250-253,323-331), so each side computes its own seam flux.  TRUE_PERIODIC:
+ * the wrapped ghost is reconstructed like an interior cell (conservative). */
+typedef enum { EFVM_SEAM_REFERENCE = 0, EFVM_SEAM_TRUE_PERIODIC = 1 } efvm_seam;
+
+/* Solver, gas, transport and case-system settings.  Mirrors SolverConfig
+ * (crates/cfd_solver/src/lib.rs:39-58), IdealGas (crates/cfd_eos/src/lib.rs:
+ * 27-41), Viscosity (:99-117), the flux/limiter plugins (crates/cfd_solver/src/
+ * lib.rs:764-842), IntegratorPlugin (:877-902) and the case-local systems of the
+ * cylinder and channel drivers. */
+typedef struct {
+    double gamma, r_gas;
+    double cfl;
+    double fixed_dt; /* > 0 overrides the CFL dt (SolverConfig.fixed_dt) */
+    int32_t flux_scheme;    /* efvm_flux_scheme */
+    int32_t reconstruction; /* efvm_reconstruction */
+    int32_t limiter;        /* efvm_limiter */
+    int32_t integrator;     /* efvm_integrator */
+    int32_t viscous;        /* SolverConfig.viscous */
+    int32_t viscosity_model;/* efvm_viscosity */
+    double mu;              /* Viscosity::Constant(mu) */
+    int32_t precision;      /* efvm_precision */
+    int32_t periodic_seam;  /* efvm_seam */
+    /* parabolic velocity inlet overriding the x-lo ghosts,
+     * examples/cylinder_drag_validation/main.rs:151-177 */
+    int32_t parabolic_inflow;
+    int32_t reserved0;
+    double inflow_u_max, inflow_height, inflow_rho;
+    /* downstream sponge after each completed step, main.rs:186-229 */
+    int32_t sponge;
+    int32_t reserved1;
+    double sponge_x_start, sponge_x_end, sponge_sigma;
+    double sponge_u_max, sponge_height, sponge_rho, sponge_p;
+    /* uniform streamwise body force added in PostFlux,
+     * crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118 */
+    double body_force_x;
+} efvm_params;
+
+/* SolverState{dt,time,step,rk_stage} (crates/cfd_solver/src/lib.rs:61-73) and
+ * StepBoundary.completed_full_step (:607-621).  rk_stage: 0,1,2 = First..Third. */
+typedef struct {
+    double dt;
+    double time;
+    uint64_t step;
+    int32_t rk_stage;
+    int32_t completed_full_step;
+} efvm_solver_state;
+
+/* A z-aligned analytic cylinder, crates/cfd_ibm/src/lib.rs:61-87. */
+typedef struct {
+    double cx, cy, radius;
+} efvm_cylinder;
+
+/* The Shu isentropic vortex used as exact solution (crates/cfd_solver/tests/
+ * isentropic_vortex_muscl_convergence.rs:48-64): centre (cx0,cy0) at t=0,
+ * translated by (mean_u,mean_v).  min_image != 0 measures the displacement
+ * with the minimum image on a periodic box of size (len_x,len_y) from lo. */
+typedef struct {
+    double gamma, beta;
+    double cx0, cy0, mean_u, mean_v;
+    double lo_x, lo_y, len_x, len_y;
+    int32_t min_image;
+    int32_t reserved;
+} efvm_vortex;
+
+/* Counters of one efvm_step call. */
+typedef struct {
+    int64_t steps_done;
+    int64_t substeps_done;
+    double time;
+    double dt;
+    int32_t stopped_at_t_stop;
+    int32_t reserved;
+} efvm_step_info;
+
+typedef struct efvm_ctx efvm_ctx;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Replaces App::new + FieldDefaultPlugins + CfdStatePlugin + IdealGasPlugin/
+ * GasPlugin + BoundaryPlugin/StructuredBoundaryPlugin + FluxPlugin/MusclPlugin
+ * + IntegratorPlugin + SolverPlugin + app.prepare()
+ * (crates/cfd_solver/src/lib.rs:691-940, crates/cfd_boundary/src/lib.rs:
+ * 457-533).  Validates the configuration (half-periodic axes, nz != 1, ng != 2
+ * are rejected) and allocates the device state.  The state must then be
+ * uploaded (the reference's init_state_system, crates/cfd_solver/src/lib.rs:
+ * 681-686, is a host closure). */
+int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out);
+int efvm_destroy(efvm_ctx* ctx);
+/* Message of the last failed call on ctx (never NULL). */
+const char* efvm_last_error(const efvm_ctx* ctx);
+int efvm_abi_version(void);
+
+/* ---- state -------------------------------------------------------------- */
+
+/* Copy the interior conserved state in (CfdState.u, crates/cfd_state/src/
+ * lib.rs:180-195).  Element (i,j) component v (0..4 = rho, rho_u, rho_v, rho_w,
+ * rho_e) is read at base[i*stride_i + j*stride_j + v*stride_var], i < nx,
+ * j < ny (strides in doubles).  rho_w is ignored (2-D).  The ghost bands are
+ * filled from the interior before the next substage, as the Halo/Boundary
+ * phases do.  Marks the CFL dt as stale. */
+int efvm_upload_state(efvm_ctx* ctx, const double* base, int64_t stride_i, int64_t stride_j,
+                      int64_t stride_var);
+/* The inverse of efvm_upload_state; writes rho_w = 0. */
+int efvm_download_state(efvm_ctx* ctx, double* base, int64_t stride_i, int64_t stride_j,
+                        int64_t stride_var);
+
+int efvm_get_solver_state(efvm_ctx* ctx, efvm_solver_state* out);
+/* Restores dt/time/step/rk_stage (checkpoint resume, crates/cfd_solver/src/
+ * lib.rs:895-897). */
+int efvm_set_solver_state(efvm_ctx* ctx, const efvm_solver_state* in);
+
+/* ---- stepping ----------------------------------------------------------- */
+
+/* Exactly one app.run(): one RK substage through every phase the reference
+ * runs (Setup: CFL on the first stage + IBM geometry; Halo; Boundary; PreFlux:
+ * IBM mirror; Flux: inviscid + viscous; PostFlux; Update; PostUpdate: sponge;
+ * Output: marker and wall forces).  crates/cfd_solver/src/lib.rs:607-677. */
+int efvm_substep(efvm_ctx* ctx);
+
+/* Run up to n_steps whole RK3 steps from a step boundary on the device,
+ * stopping at the first step boundary where time >= t_stop when stop_at_t is
+ * non-zero (the case drivers' `loop { if t >= T break; 3x app.run() }`,
+ * crates/cfd_solver/tests/isentropic_vortex_muscl_convergence.rs:109-117).
+ * When force_history is not NULL it receives the MarkerForce after every
+ * substage (6 doubles each: pressure xyz, viscous xyz), capacity
+ * 3*n_steps*6 doubles, as examples/cylinder_drag_validation/main.rs:334-340
+ * reads it.  Returns EFVM_ERR_NONPHYSICAL if the state went non-physical. */
+int efvm_step(efvm_ctx* ctx, int64_t n_steps, int32_t stop_at_t, double t_stop,
+              double* force_history, efvm_step_info* info);
+
+/* CFL dt of the current state without stepping (cfl_system,
+ * crates/cfd_solver/src/lib.rs:626-677). */
+int efvm_cfl(efvm_ctx* ctx, double* dt_out);
+
+/* ---- immersed boundary -------------------------------------------------- */
+
+/* CylinderIbmPlugin::with_cylinders + GhostCellIbmPlugin
+ * (crates/cfd_ibm/src/lib.rs:621-680).  freestream = ConsVar (5 doubles) that
+ * seeds the cells that flip solid/fluid. */
+int efvm_set_cylinders(efvm_ctx* ctx, const efvm_cylinder* cylinders, int32_t n,
+                       const double freestream[5]);
+/* MarkerForce{pressure,viscous} of the last Output phase
+ * (crates/cfd_ibm/src/lib.rs:442-480,601-615). */
+int efvm_marker_force(efvm_ctx* ctx, double out[6]);
+/* WallForce{pressure,viscous}, the staircase estimate (crates/cfd_ibm/src/
+ * lib.rs:309-395). */
+int efvm_wall_force(efvm_ctx* ctx, double out[6]);
+/* Number of solid cells and of IBM ghost cells (IbmGhostCells.cells.len()). */
+int efvm_ibm_counts(efvm_ctx* ctx, int64_t* n_solid, int64_t* n_ghost);
+/* The interior SolidMask (crates/cfd_state/src/lib.rs:202-206) as nx*ny bytes,
+ * x fastest (1 = solid). */
+int efvm_get_solid_mask(efvm_ctx* ctx, uint8_t* out);
+
+/* ---- diagnostics -------------------------------------------------------- */
+
+/* Volume-weighted L1 and the max-norm of (rho - rho_exact) over the interior at
+ * the context's current time (crates/cfd_solver/tests/
+ * isentropic_vortex_muscl_convergence.rs:119-138). */
+int efvm_density_error(efvm_ctx* ctx, const efvm_vortex* exact, double out[2]);
+/* Fill the interior with the vortex at t=0 on the device (synthetic inputs). */
+int efvm_init_vortex(efvm_ctx* ctx, const efvm_vortex* v);
+/* Sum of rho*volume over the interior (total mass). */
+int efvm_total_mass(efvm_ctx* ctx, double* out);
+
+/* The CUDA stream the context launches on (a cudaStream_t), so a caller can
+ * time it with its own events. */
+int efvm_get_stream(efvm_ctx* ctx, void** stream);
+/* Number of kernels this context has launched since creation. */
+int efvm_launch_count(efvm_ctx* ctx, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EFVM_H */

@@ -1,0 +1,173 @@
+"""Case definitions shared by the oracle pins, the tests and the bench.
+
+Each builder returns (grid, params, initial interior state (ny, nx, 5), extras)
+for one of the reference's case drivers or one of the benchmark configurations.
+Plain numpy; no device and no oracle code runs here.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+import numpy as np
+
+_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if _REPO not in sys.path:
+    sys.path.insert(0, _REPO)
+
+from dev_field_efvm_b200 import abi  # noqa: E402
+
+R_GAS_AIR = 287.058
+
+
+def prim_to_cons(rho, u, v, p, gamma=1.4):
+    """IdealGas::prim_to_cons (crates/cfd_eos/src/lib.rs:55-59), vectorised."""
+    rho = np.asarray(rho, dtype=np.float64)
+    u = np.broadcast_to(np.asarray(u, dtype=np.float64), rho.shape)
+    v = np.broadcast_to(np.asarray(v, dtype=np.float64), rho.shape)
+    p = np.broadcast_to(np.asarray(p, dtype=np.float64), rho.shape)
+    ke = 0.5 * rho * (u * u + v * v + 0.0 * 0.0)
+    rho_e = p / (gamma - 1.0) + ke
+    return np.stack([rho, rho * u, rho * v, np.zeros_like(rho), rho_e], -1)
+
+
+def centroids(grid: abi.EfvmGrid):
+    """Cell centres lo + ((i) + 0.5) * h of the interior (FIELD UniformMesh)."""
+    hx = (grid.hi[0] - grid.lo[0]) / grid.nx
+    hy = (grid.hi[1] - grid.lo[1]) / grid.ny
+    x = grid.lo[0] + (np.arange(grid.nx, dtype=np.float64) + 0.5) * hx
+    y = grid.lo[1] + (np.arange(grid.ny, dtype=np.float64) + 0.5) * hy
+    return x, y
+
+
+def vortex_state(v: abi.EfvmVortex, t: float, X, Y):
+    """The Shu vortex closure (crates/cfd_solver/tests/isentropic_vortex_muscl_convergence.rs:48-64),
+    vectorised, with the optional minimum-image displacement."""
+    cx = v.cx0 + v.mean_u * t
+    cy = v.cy0 + v.mean_v * t
+    dx = X - cx
+    dy = Y - cy
+    if v.min_image:
+        dx = dx - v.len_x * np.round(dx / v.len_x)
+        dy = dy - v.len_y * np.round(dy / v.len_y)
+    r2 = dx * dx + dy * dy
+    f = np.exp(0.5 * (1.0 - r2))
+    du = -v.beta / (2.0 * math.pi) * dy * f
+    dv = v.beta / (2.0 * math.pi) * dx * f
+    dtemp = -(v.gamma - 1.0) * v.beta * v.beta / (8.0 * v.gamma * math.pi ** 2) * np.exp(1.0 - r2)
+    temp = 1.0 + dtemp
+    rho = temp ** (1.0 / (v.gamma - 1.0))
+    p = rho ** v.gamma
+    return prim_to_cons(rho, v.mean_u + du, v.mean_v + dv, p, v.gamma)
+
+
+def vortex_case(n: int, *, periodic: bool, mean=(0.5, 0.5), beta=5.0, centre=(5.0, 5.0), cfl=0.3,
+                muscl=False, limiter=abi.LIMITER_MINMOD, precision=abi.PREC_FP64, seam=abi.SEAM_REFERENCE,
+                domain=10.0, ny: int | None = None):
+    """The isentropic-vortex cases.  periodic=False is the reference's own gate
+    (crates/cfd_solver/tests/isentropic_vortex_*convergence.rs: zero-gradient x/y,
+    slip z, dz = L/n); periodic=True is the periodic [0,L]^2 benchmark box."""
+    ny = ny or n
+    side = abi.BC_PERIODIC if periodic else abi.BC_SUPERSONIC_OUTFLOW
+    bcs = {abi.XLO: side, abi.XHI: side, abi.YLO: side, abi.YHI: side,
+           abi.ZLO: abi.BC_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+    grid = abi.make_grid(n, ny, lo=(0.0, 0.0, 0.0), hi=(domain, domain * ny / n, domain / n), bcs=bcs)
+    params = abi.make_params(cfl=cfl, reconstruction=abi.RECON_MUSCL if muscl else abi.RECON_FIRST_ORDER,
+                             limiter=limiter, precision=precision, periodic_seam=seam)
+    v = abi.make_vortex(beta=beta, cx0=centre[0], cy0=centre[1], mean_u=mean[0], mean_v=mean[1],
+                        length=(domain, domain * ny / n), min_image=periodic)
+    x, y = centroids(grid)
+    X, Y = np.meshgrid(x, y)
+    u = vortex_state(v, 0.0, X, Y)
+    return grid, params, u, {"vortex": v}
+
+
+def cylinder_case(nx=440, ny=82, *, u_mean=50.0, rho=1.0, p=1.0e5, reynolds=20.0, cfl=0.3, muscl=False,
+                  limiter=abi.LIMITER_MINMOD, sponge_sigma=1.0e4, sponge_x_start=1.4, precision=abi.PREC_FP64,
+                  lz=0.041):
+    """The DFG 2D-1 cylinder (examples/cylinder_drag_validation/main.rs:231-316 with
+    config.toml).  Defaults are the reference's own passing run: 440x82, first-order
+    HLLC, u_mean=50, p=1e5, CFL 0.3, sponge sigma=1e4."""
+    L, H, D, cx, cy = 2.2, 0.41, 0.1, 0.2, 0.2
+    mu = rho * u_mean * D / reynolds
+    u_max = 1.5 * u_mean
+    bcs = {abi.XLO: abi.BC_SUPERSONIC_OUTFLOW,
+           abi.XHI: abi.make_bc(abi.BC_PRESSURE_OUTLET, p=p),
+           abi.YLO: abi.BC_NO_SLIP_WALL, abi.YHI: abi.BC_NO_SLIP_WALL,
+           abi.ZLO: abi.BC_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+    grid = abi.make_grid(nx, ny, lo=(0.0, 0.0, 0.0), hi=(L, H, lz), bcs=bcs)
+    params = abi.make_params(
+        cfl=cfl, viscous=1, viscosity_model=abi.VISC_CONSTANT, mu=mu,
+        reconstruction=abi.RECON_MUSCL if muscl else abi.RECON_FIRST_ORDER, limiter=limiter,
+        precision=precision,
+        parabolic_inflow=1, inflow_u_max=u_max, inflow_height=H, inflow_rho=rho,
+        sponge=1, sponge_x_start=sponge_x_start, sponge_x_end=L, sponge_sigma=sponge_sigma,
+        sponge_u_max=u_max, sponge_height=H, sponge_rho=rho, sponge_p=p)
+    x, y = centroids(grid)
+    X, Y = np.meshgrid(x, y)
+    uy = 4.0 * u_max * Y * (H - Y) / (H * H)
+    u = prim_to_cons(np.full_like(X, rho), uy, 0.0, np.full_like(X, p))
+    freestream = prim_to_cons(np.array(rho), np.array(u_mean), 0.0, np.array(p))
+    q = 0.5 * rho * u_mean * u_mean * D * lz
+    extras = {"cylinders": [(cx, cy, 0.5 * D)], "freestream": freestream.reshape(5), "q": q, "mu": mu,
+              "u_max": u_max}
+    return grid, params, u, extras
+
+
+def cylinder_baseline_case(nx=1100, ny=205, **kw):
+    """The benchmark's cylinder: 1100x205 (D/dx=50), MUSCL, peak inflow 0.3
+    (mean 0.2), freestream Mach 0.1 on the peak speed (a=3, rho=1,
+    p=rho*a^2/gamma), Re=20 on the mean speed, CFL 0.4, sponge rescaled by the
+    convective time (sigma*D/U_mean kept at the reference's 20 -> sigma=40)."""
+    gamma = 1.4
+    a = 3.0
+    p = 1.0 * a * a / gamma
+    args = dict(u_mean=0.2, rho=1.0, p=p, reynolds=20.0, cfl=0.4, muscl=True, sponge_sigma=40.0)
+    args.update(kw)
+    return cylinder_case(nx, ny, **args)
+
+
+def sod_case(n: int, gamma: float = 1.4):
+    """crates/cfd_solver/tests/sod_exact_convergence.rs:200-247."""
+    bcs = {abi.YLO: abi.BC_SLIP_WALL, abi.YHI: abi.BC_SLIP_WALL, abi.ZLO: abi.BC_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+    grid = abi.make_grid(n, 1, hi=(1.0, 0.01, 0.01), bcs=bcs)
+    params = abi.make_params(cfl=0.4, gamma=gamma)
+    x, _ = centroids(grid)
+    left = prim_to_cons(np.array(1.0), np.array(0.0), 0.0, np.array(1.0e5), gamma)
+    right = prim_to_cons(np.array(0.125), np.array(0.0), 0.0, np.array(1.0e4), gamma)
+    u = np.where((x < 0.5)[:, None], left, right)[None, :, :]
+    return grid, params, u, {"x": x}
+
+
+def pulse_case(n: int, cfl=0.45):
+    """examples/periodic_advected_pulse/main.rs:62-118 with its config.toml."""
+    L = 1.0
+    bcs = {abi.XLO: abi.BC_PERIODIC, abi.XHI: abi.BC_PERIODIC, abi.YLO: abi.BC_SLIP_WALL,
+           abi.YHI: abi.BC_SLIP_WALL, abi.ZLO: abi.BC_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+    grid = abi.make_grid(n, 1, hi=(L, L / n, L / n), bcs=bcs)
+    params = abi.make_params(cfl=cfl)
+    x, _ = centroids(grid)
+    u = pulse_state(x, 0.0)[None, :, :]
+    return grid, params, u, {"x": x}
+
+
+def pulse_state(x, t, L=1.0, c0=0.85, sig=0.08, amp=0.2, gamma=1.4, vel=1.0, p=1.0):
+    center = (c0 + vel * t) % L
+    d = x - center
+    d = d - L * np.round(d / L)
+    rho = 1.0 + amp * np.exp(-0.5 * (d / sig) ** 2)
+    return prim_to_cons(rho, np.full_like(rho, vel), 0.0, np.full_like(rho, p), gamma)
+
+
+def poiseuille_case(ny=32, nx=3):
+    """crates/cfd_solver/tests/poiseuille_channel_validation.rs:124-161 (2-D: the
+    reference's nz=1 spanwise cell is the z extent here)."""
+    H, rho0, T0, MU, GX = 1.0, 1.0, 300.0, 10.0, 160.0
+    p0 = rho0 * R_GAS_AIR * T0
+    bcs = {abi.YLO: abi.BC_NO_SLIP_WALL, abi.YHI: abi.BC_NO_SLIP_WALL, abi.ZLO: abi.BC_SLIP_WALL,
+           abi.ZHI: abi.BC_SLIP_WALL}
+    grid = abi.make_grid(nx, ny, hi=(1.0, H, 1.0), bcs=bcs)
+    params = abi.make_params(cfl=0.3, viscous=1, viscosity_model=abi.VISC_CONSTANT, mu=MU, body_force_x=GX)
+    u = prim_to_cons(np.full((ny, nx), rho0), np.zeros((ny, nx)), 0.0, np.full((ny, nx), p0))
+    return grid, params, u, {"H": H, "mu": MU, "gx": GX, "rho": rho0, "t_final": 0.081}

@@ -1,0 +1,210 @@
+"""Known-answer tests of the CPU oracle, ported from the reference's in-crate
+unit tests (the values and tolerances are the reference's own)."""
+import numpy as np
+import pytest
+
+from dev_field_efvm_b200 import abi
+from oracle import pyoracle as po
+from oracle import cases
+
+RUS, HLLC, HLLC_TB = abi.FLUX_RUSANOV, abi.FLUX_HLLC, abi.FLUX_HLLC_TEXTBOOK
+
+
+def p2c(rho, u, v, w, p, t=0.0):
+    return po.prim_to_cons([rho, u, v, w, p, t])
+
+
+# ---- crates/cfd_state/src/lib.rs:213-240 ----------------------------------
+def test_cons_var_velocity_and_kinetic_energy():
+    u = np.array([2.0, 4.0, 6.0, 8.0, 100.0])
+    prim = po.cons_to_prim(u, gamma=1.4, r_gas=287.058)
+    assert list(prim[1:4]) == [2.0, 3.0, 4.0]
+    # pressure = (gamma-1)(E - 0.5*(16+36+64)/2) = 0.4*(100-29)
+    assert abs(po.pressure(u) - 0.4 * (100.0 - 29.0)) < 1e-12
+
+
+# ---- crates/cfd_eos/src/lib.rs:123-150 --------------------------------------
+def test_cons_prim_roundtrip():
+    t = 101325.0 / (1.225 * 287.058)
+    prim = [1.225, 100.0, 0.0, 0.0, 101325.0, t]
+    prim2 = po.cons_to_prim(po.prim_to_cons(prim))
+    assert abs(prim2[0] - 1.225) < 1e-10
+    assert abs(prim2[1] - 100.0) < 1e-10
+    assert abs(prim2[4] - 101325.0) < 1e-6
+    assert abs(prim2[5] - t) < 1e-6
+
+
+def test_sound_speed_air():
+    cons = po.prim_to_cons([1.225, 0.0, 0.0, 0.0, 101325.0, 288.15])
+    assert abs(po.sound_speed(cons) - 340.3) < 1.0
+
+
+def test_sutherland_and_conductivity():
+    mu = po.sutherland(288.15)
+    assert abs(mu - 1.8e-5) < 1e-6
+    k = po.thermal_conductivity(mu, 1.4, 287.058)
+    assert 0.02 < k < 0.03
+
+
+# ---- crates/cfd_riemann/src/lib.rs:658-803 ---------------------------------
+def test_flux_normal_is_rotation_invariant_for_slanted_faces():
+    c, s = 0.6, 0.8
+    rot = lambda v: np.array([c * v[0] - s * v[1], s * v[0] + c * v[1], v[2]])
+    for va, vb in [([30.0, 5.0, -2.0], [10.0, -4.0, 1.0]), ([-80.0, 0.0, 0.0], [120.0, 3.0, 0.0])]:
+        a = p2c(1.0, *va, 100000.0)
+        b = p2c(0.5, *vb, 50000.0)
+        ra, rb = rot(va), rot(vb)
+        a2 = p2c(1.0, *ra, 100000.0)
+        b2 = p2c(0.5, *rb, 50000.0)
+        n = rot([1.0, 0.0, 0.0])
+        for scheme in (RUS, HLLC_TB, HLLC):
+            f = po.flux(scheme, a, b, 0)
+            g = po.flux_normal(scheme, a2, b2, n)
+            fm = rot(f[1:4])
+            tol = 1e-9 * (abs(f[4]) + 1.0)
+            assert abs(g[0] - f[0]) < tol and abs(g[4] - f[4]) < tol
+            assert abs(g[1] - fm[0]) < tol and abs(g[2] - fm[1]) < tol and abs(g[3] - fm[2]) < tol
+
+
+def test_flux_normal_matches_directional_flux():
+    a = p2c(1.0, 30.0, 0.0, 0.0, 100000.0)
+    b = p2c(0.5, 10.0, 0.0, 0.0, 50000.0)
+    fn_px = po.flux_normal(RUS, a, b, [1.0, 0.0, 0.0])
+    f_dir = po.flux(RUS, a, b, 0)
+    assert abs(fn_px[0] - f_dir[0]) < 1e-12 and abs(fn_px[1] - f_dir[1]) < 1e-12
+    fn_mx = po.flux_normal(RUS, a, b, [-1.0, 0.0, 0.0])
+    f_flip = -po.flux(RUS, b, a, 0)
+    assert abs(fn_mx[0] - f_flip[0]) < 1e-12 and abs(fn_mx[4] - f_flip[4]) < 1e-12
+
+
+def test_flux_normal_conservative_between_two_cells():
+    a = p2c(1.0, 50.0, 0.0, 0.0, 100000.0)
+    b = p2c(0.4, -20.0, 0.0, 0.0, 40000.0)
+    fo = po.flux_normal(RUS, a, b, [1.0, 0.0, 0.0])
+    fb = po.flux_normal(RUS, b, a, [-1.0, 0.0, 0.0])
+    assert abs(fo[0] + fb[0]) < 1e-12 and abs(fo[4] + fb[4]) < 1e-12
+
+
+def test_flux_symmetry_rusanov():
+    cons = p2c(1.225, 100.0, 0.0, 0.0, 101325.0)
+    f = po.flux(RUS, cons, cons, 0)
+    fp = po.physical_flux(cons, 0)
+    assert abs(f[0] - fp[0]) < 1e-10 and abs(f[1] - fp[1]) < 1e-6 and abs(f[4] - fp[4]) < 1e-4
+
+
+def test_rusanov_dissipation_finite():
+    left = p2c(1.0, 0.0, 0.0, 0.0, 100000.0)
+    right = p2c(0.125, 0.0, 0.0, 0.0, 10000.0)
+    f = po.flux(RUS, left, right, 0)
+    assert np.all(np.isfinite(f))
+
+
+def test_hllc_uniform_state():
+    cons = p2c(1.225, 100.0, 0.0, 0.0, 101325.0)
+    f = po.flux(HLLC, cons, cons, 0)
+    fp = po.physical_flux(cons, 0)
+    assert abs(f[0] - fp[0]) < 1e-10 and abs(f[1] - fp[1]) < 1e-6
+    assert abs(f[2] - fp[2]) < 1e-10 and abs(f[3] - fp[3]) < 1e-10 and abs(f[4] - fp[4]) < 1e-4
+
+
+def test_hllc_sod_shock_finite():
+    left = p2c(1.0, 0.0, 0.0, 0.0, 100000.0)
+    right = p2c(0.125, 0.0, 0.0, 0.0, 10000.0)
+    f = po.flux(HLLC, left, right, 0)
+    assert np.all(np.isfinite(f)) and f[0] > 0.0
+
+
+def test_hllc_direction_consistency():
+    cx = p2c(1.0, 100.0, 50.0, 25.0, 101325.0)
+    cy = p2c(1.0, 25.0, 100.0, 50.0, 101325.0)
+    fx = po.flux(HLLC, cx, cx, 0)
+    fy = po.flux(HLLC, cy, cy, 1)
+    assert abs(fx[0] - fy[0]) < 1e-10 and abs(fx[1] - fy[2]) < 1e-6
+
+
+# ---- limiters, crates/cfd_solver/src/lib.rs:170-192 ------------------------
+@pytest.mark.parametrize("a,b,mm,mc", [
+    (1.0, 2.0, 1.0, 1.5), (2.0, 1.0, 1.0, 1.5), (-1.0, -3.0, -1.0, -2.0), (1.0, -1.0, 0.0, 0.0),
+    (0.0, 1.0, 0.0, 0.0), (1.0, 10.0, 1.0, 2.0), (-4.0, -0.5, -0.5, -1.0),
+])
+def test_limiters(a, b, mm, mc):
+    assert po.limiter(abi.LIMITER_MINMOD, a, b) == mm
+    assert po.limiter(abi.LIMITER_MC, a, b) == mc
+
+
+# ---- crates/cfd_solver/src/integrate.rs:123-152 ----------------------------
+def test_euler_step_basic():
+    u = np.array([[1.0, 0.0, 0.0, 0.0, 100.0]])
+    rhs = np.array([[0.1, 0.0, 0.0, 0.0, 10.0]])
+    u1, _, nxt, done = po.integrator_substep(abi.INTEGRATOR_EULER, u, u, rhs, 0.5, 0)
+    assert done and nxt == 0
+    assert abs(u1[0, 0] - 1.05) < 1e-15 and abs(u1[0, 4] - 105.0) < 1e-15
+
+
+def test_rk3_constant_rhs_matches_euler_total():
+    u = np.array([[1.0, 0.0, 0.0, 0.0, 100.0]])
+    u0 = u.copy()
+    rhs = np.array([[0.1, 0.0, 0.0, 0.0, 10.0]])
+    stage, done = 0, False
+    cur = u.copy()
+    for _ in range(3):
+        cur, u0, stage, done = po.integrator_substep(abi.INTEGRATOR_RK3, cur, u0, rhs, 0.5, stage)
+    assert done
+    assert abs(cur[0, 0] - (1.0 + 0.5 * 0.1)) < 1e-12
+    assert abs(cur[0, 4] - (100.0 + 0.5 * 10.0)) < 1e-12
+
+
+# ---- crates/cfd_boundary/src/lib.rs:686-717 --------------------------------
+def test_outflow_copies_interior():
+    interior = p2c(1.2, 100.0, 0.0, 0.0, 101325.0)
+    g = po.bc_ghost(abi.make_bc(abi.BC_SUPERSONIC_OUTFLOW), abi.XLO, interior)
+    assert np.array_equal(g, interior)
+
+
+def test_slip_wall_reflects_only_normal_momentum():
+    interior = p2c(1.2, 100.0, 50.0, 25.0, 101325.0)
+    gx = po.bc_ghost(abi.make_bc(abi.BC_SLIP_WALL), abi.XHI, interior)
+    assert abs(gx[1] + interior[1]) < 1e-12
+    assert gx[2] == interior[2] and gx[3] == interior[3] and gx[0] == interior[0]
+    gy = po.bc_ghost(abi.make_bc(abi.BC_SLIP_WALL), abi.YLO, interior)
+    assert abs(gy[2] + interior[2]) < 1e-12 and gy[1] == interior[1]
+
+
+def test_supersonic_inflow_is_prescribed():
+    interior = p2c(0.1, 0.0, 0.0, 0.0, 1000.0)
+    bc = abi.make_bc(abi.BC_SUPERSONIC_INFLOW, rho=1.0, u=500.0, v=0.0, w=0.0, p=2e5)
+    g = po.bc_ghost(bc, abi.XLO, interior)
+    prim = po.cons_to_prim(g)
+    assert abs(prim[0] - 1.0) < 1e-9 and abs(prim[1] - 500.0) < 1e-6 and abs(prim[4] - 2e5) < 1.0
+
+
+def test_no_slip_and_pressure_outlet():
+    interior = p2c(1.2, 100.0, 50.0, 0.0, 101325.0)
+    g = po.bc_ghost(abi.make_bc(abi.BC_NO_SLIP_WALL), abi.YHI, interior)
+    assert g[1] == -interior[1] and g[2] == -interior[2] and g[0] == interior[0] and g[4] == interior[4]
+    g = po.bc_ghost(abi.make_bc(abi.BC_PRESSURE_OUTLET, p=9e4), abi.XHI, interior)
+    prim = po.cons_to_prim(g)
+    assert abs(prim[4] - 9e4) < 1e-6 and abs(prim[1] - 100.0) < 1e-10 and prim[0] == 1.2
+
+
+# ---- periodic halo KAT, crates/cfd_boundary/src/lib.rs:805-828 -------------
+def test_halo_fills_periodic_ghosts_from_the_opposite_slab():
+    g = abi.make_grid(4, 1, hi=(1.0, 1.0, 1.0), bcs={abi.XLO: abi.BC_PERIODIC, abi.XHI: abi.BC_PERIODIC})
+    c = po.OracleCase(g, abi.make_params(fixed_dt=1e-30))
+    u = np.zeros((1, 4, 5))
+    u[0, :, 0] = [10.0, 11.0, 12.0, 13.0]
+    u[0, :, 4] = 1e5
+    c.upload(u)
+    c.substep()  # the Halo phase runs inside the substage; dt ~ 0 keeps the interior
+    raw = c.raw_state()
+    nxr = 8
+    row = 2 * nxr * 1 + 2 * nxr  # raw (k=2, j=2) row start in a (8, 5, 5) raw array
+    k, j = 2, 2
+    base = (k * 5 + j) * nxr
+    assert [raw[base + i, 0] for i in (0, 1, 6, 7)] == [12.0, 13.0, 10.0, 11.0]
+
+
+def test_half_periodic_axis_is_rejected():
+    g = abi.make_grid(8, 1, bcs={abi.XLO: abi.BC_PERIODIC})
+    with pytest.raises(ValueError, match="periodic"):
+        po.OracleCase(g, abi.make_params())
