@@ -1,0 +1,330 @@
+"""Throughput of the B200 explicit finite-volume step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload cylinder|vortex4096]
+
+A step is one SSP-RK3 time step (three substages) of the whole case.  The
+default workload is the cylinder channel with the ghost-cell immersed boundary
+and viscous terms: 1100x205 cells, MUSCL (minmod) + HLLC-Thornber, FP64,
+parabolic inlet, sponge, marker-force Output phase every substage.  The metric
+is cell-updates/s (interior cells advanced by one full RK3 step per second).
+
+`value` is device time with the state resident in HBM and L2 flushed between
+timed steps; `e2e` is the same metric through the C-ABI with host buffers:
+every step uploads the state from pinned host memory, steps, downloads it and
+reads the marker force.  `roofline` relates the stage kernel's algorithmic
+bytes (the RK3 traffic of a cell-update, 256 B, plus the 1 B solid mask per
+stage) to its live CUDA-event duration and the measured HBM copy bandwidth.
+`cpu_baseline` times the CPU oracle (the reference's algorithm restated in
+C++, OpenMP over the host cores) on a bounded sample of the same workload.
+
+Under torchrun (N > 1) every rank advances its own replica of the case (weak
+scaling; one grid does not yet shard across GPUs), timing is the max over
+ranks, and `value` counts the cells of all ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Cell-updates/s on 1 B200: plain FP64 vs chosen form at equal L1 density error"
+UNIT = "cell-updates/s"
+
+
+def workload(name: str):
+    from oracle import cases  # case builders are plain numpy (no oracle code)
+    from dev_field_efvm_b200 import abi
+    if name == "cylinder":
+        grid, params, u, ex = cases.cylinder_baseline_case()
+        desc = {"workload": "cylinder IBM+viscous channel 2.2x0.41, 1100x205 cells (D/dx=50), "
+                            "MUSCL-minmod + HLLC-Thornber, SSP-RK3, CFL 0.4, Re=20, M=0.1, FP64",
+                "nx": grid.nx, "ny": grid.ny}
+        return grid, params, u, ex, desc
+    if name == "vortex4096":
+        grid, params, u, ex = cases.vortex_case(4096, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4)
+        desc = {"workload": "isentropic vortex, periodic [0,10]^2, 4096x4096 cells, MUSCL-minmod + HLLC-Thornber, "
+                            "SSP-RK3, CFL 0.4, FP64", "nx": grid.nx, "ny": grid.ny}
+        return grid, params, u, ex, desc
+    raise SystemExit(f"unknown workload {name}")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """SM clock and throttle reasons of the local GPU, polled through NVML every
+    20 ms while the timed region runs (read-only queries)."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.samples, self.reasons, self.smax = [], set(), None
+        self._stop = threading.Event()
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+        except Exception:
+            self.nv = None
+        return self
+
+    def _poll(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)))
+                mask = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self.nv:
+            self.t.join(timeout=2)
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def cpu_baseline(grid, params, u, ex, target_seconds=12.0):
+    """The CPU oracle (OpenMP, all host threads) on a bounded number of steps."""
+    from oracle import pyoracle
+    c = pyoracle.OracleCase(grid, params, parallel=True)
+    if "cylinders" in ex:
+        c.set_cylinders(ex["cylinders"], ex["freestream"])
+    c.upload(u)
+    c.step(1)  # first step includes the one-off geometry set-up
+    t0 = time.perf_counter()
+    c.step(1)
+    one = time.perf_counter() - t0
+    n = max(1, min(200, int(target_seconds / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    c.step(n)
+    dt = time.perf_counter() - t0
+    cores = pyoracle.lib(True).oracle_num_threads()
+    return {"value": grid.nx * grid.ny * n / dt, "unit": UNIT, "cores": int(cores), "kind": "port",
+            "sample": f"{n} RK3 steps of the same case after 2 untimed steps ({dt:.1f} s)"}
+
+
+def run_reference(args, rank, world, budget_s=90.0):
+    """The reference arm: the CPU oracle of the reference's algorithm on all host
+    threads, same case and metric.  The timed sample is min(K, what fits in
+    about 90 s) whole RK3 steps of the full case, so the arm ends within a few
+    minutes for any K; the rate is cell-updates over that sample's time."""
+    if rank != 0:
+        return
+    grid, params, u, ex, desc = workload(args.workload)
+    from oracle import pyoracle
+    c = pyoracle.OracleCase(grid, params, parallel=True)
+    if "cylinders" in ex:
+        c.set_cylinders(ex["cylinders"], ex["freestream"])
+    c.upload(u)
+    c.step(min(args.warmup, 3))
+    t0 = time.perf_counter()
+    c.step(1)
+    one = time.perf_counter() - t0
+    m = max(1, min(args.steps, int(budget_s / max(one, 1e-9))))
+    t0 = time.perf_counter()
+    c.step(m)
+    dt = time.perf_counter() - t0
+    value = grid.nx * grid.ny * m / dt
+    cores = int(pyoracle.lib(True).oracle_num_threads())
+    sample = f"{m} RK3 steps of the full case ({dt:.1f} s) after {min(args.warmup, 3) + 1} untimed steps"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": m, "warmup": min(args.warmup, 3) + 1, "ms_per_step": 1e3 * dt / m,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": dict(desc, parallelism=f"cpu{cores}"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "vortex4096"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from dev_field_efvm_b200 import abi
+    from dev_field_efvm_b200.device import Context
+
+    grid, params, u, ex, desc = workload(args.workload)
+    cells = grid.nx * grid.ny
+    ctx = Context(grid, params)
+    if "cylinders" in ex:
+        ctx.set_cylinders(ex["cylinders"], ex["freestream"])
+    ctx.upload(u)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    ctx.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    # ---- device-timed steps, L2 flushed between steps --------------------
+    n0 = ctx.launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for a, b in evs:
+                flush.zero_()
+                a.record(stream)
+                ctx.step_async(1)
+                b.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launch_count() - n0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    st = ctx.solver_state()  # synchronising call: reports a non-physical state
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # ---- stage-kernel roofline (live CUDA events per kernel class) --------
+    prof = ctx.profile_steps(max(10, min(args.steps, 50)))
+    n_prof = max(10, min(args.steps, 50))
+    stage_ms_per_launch = prof[0] / (3 * n_prof)
+    mask_bytes = 1 if "cylinders" in ex else 0
+    bytes_per_launch = cells * (256 + 3 * mask_bytes) / 3.0
+    achieved = bytes_per_launch / (stage_ms_per_launch * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(tf):
+        d = json.load(open(tf))
+        if d.get("workload_key") == args.workload:
+            traffic = d.get("bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "kernel": "stage_kernel (fused MUSCL/HLLC/viscous/RK3 substage)",
+                "stage_ms_per_launch": stage_ms_per_launch,
+                "share_of_step": prof[0] / prof[3] if prof[3] > 0 else None}
+
+    # ---- chosen form: FP32 reconstruction/fluxes, FP64 accumulation -------
+    p32 = abi.make_params(**{f: getattr(params, f) for f, _ in abi.EfvmParams._fields_})
+    p32.precision = abi.PREC_FP32_FLUX
+    ctx32 = Context(grid, p32)
+    if "cylinders" in ex:
+        ctx32.set_cylinders(ex["cylinders"], ex["freestream"])
+    ctx32.upload(u)
+    ctx32.step(args.warmup)
+    s32 = torch.cuda.ExternalStream(ctx32.stream())
+    ev32 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s32):
+        for a, b in ev32:
+            flush.zero_()
+            a.record(s32)
+            ctx32.step_async(1)
+            b.record(s32)
+    torch.cuda.synchronize()
+    ms32 = sum(a.elapsed_time(b) for a, b in ev32)
+    value32 = world * cells * args.steps / (ms32 * 1e-3)
+    ctx32.close()
+
+    # ---- end to end through the C-ABI with pinned host buffers -----------
+    host = torch.empty((grid.ny, grid.nx, 5), dtype=torch.float64, pin_memory=True)
+    host.copy_(torch.from_numpy(ctx.download()))
+    ptr = host.data_ptr()
+    n_e2e = max(3, min(args.steps, 50))
+    for _ in range(2):
+        ctx.upload_ptr(ptr, 5, 5 * grid.nx, 1)
+        ctx.step(1)
+        ctx.download_ptr(ptr, 5, 5 * grid.nx, 1)
+        ctx.marker_force()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        ctx.upload_ptr(ptr, 5, 5 * grid.nx, 1)
+        ctx.step(1)
+        ctx.download_ptr(ptr, 5, 5 * grid.nx, 1)
+        ctx.marker_force()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * cells * n_e2e / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(grid, params, u, ex)
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(desc, parallelism=f"replicas{world}" if world > 1 else "single",
+                           l2="flushed between timed steps (256 MB write)",
+                           time=st.time, final_step=int(st.step)),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
+                    "d2h_bytes_per_step": cells * 5 * 8 + 48, "steps": n_e2e},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "chosen_form": {"precision": "fp32 reconstruction+flux, fp64 accumulation", "value": value32,
+                            "unit": UNIT, "ms_per_step": ms32 / args.steps},
+        }
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

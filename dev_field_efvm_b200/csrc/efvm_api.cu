@@ -227,7 +227,6 @@ int build_ibm_lists(efvm_ctx* c) {
     d.zg0 = c->zg0;
     d.zfill = c->zfill;
     d.force_out = c->force_out;
-    d.history = nullptr;
     d.partials = c->force_partials;
     d.counter = c->force_counter;
     return EFVM_OK;
@@ -588,9 +587,13 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
     if (n_steps < 0) return fail(c, EFVM_ERR_INVALID_ARG, "n_steps must be >= 0");
     if (c->params.integrator != EFVM_INTEGRATOR_EULER && c->rk_stage != 0)
         return fail(c, EFVM_ERR_INVALID_ARG, "efvm_step must start at a step boundary (rk_stage == 0)");
-    DevState s_before;
-    int rc = read_state(c, s_before);
-    if (rc) return rc;
+    const bool async = !stop_at_t && !force_history && !info;
+    DevState s_before{};
+    int rc = EFVM_OK;
+    if (!async) {
+        rc = read_state(c, s_before);
+        if (rc) return rc;
+    }
     const int subs = c->params.integrator == EFVM_INTEGRATOR_EULER ? 1 : 3;
     const long long cap = force_history && c->ibm ? (long long)subs * n_steps : 0;
     if (cap > c->history_cap) {
@@ -601,12 +604,12 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
         c->history_cap = cap;
         c->graph_valid = false;
     }
-    c->ibm_desc.history = cap ? c->history : nullptr;
     if (c->graph_with_history != (cap != 0)) c->graph_valid = false;
     c->graph_with_history = cap != 0;
-    sync_control(c, stop_at_t, t_stop, cap);
-    rc = prologue(c);
+    if (!async || c->control_dirty) sync_control(c, stop_at_t, t_stop, cap);
+    rc = prologue(c);  // may rebuild the IBM descriptor (first step after set_cylinders)
     if (rc) return rc;
+    c->ibm_desc.history = cap ? c->history : nullptr;
     if (c->params.integrator == EFVM_INTEGRATOR_EULER) {
         for (int64_t k = 0; k < n_steps; ++k) {
             double* in = c->U[c->euler_cur];
@@ -632,6 +635,7 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
         }
     }
     CUDA_TRY(c, cudaGetLastError());
+    if (async) return EFVM_OK;
     DevState s;
     rc = read_state(c, s);
     if (rc) return rc;
@@ -647,7 +651,7 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
         info->dt = s.dt;
         info->stopped_at_t_stop = (stop_at_t && s.time >= t_stop) ? 1 : 0;
     }
-    c->control_dirty = true;
+    c->control_dirty = stop_at_t != 0 || cap != 0;
     if (s.nonphysical) return fail(c, EFVM_ERR_NONPHYSICAL, "the state went non-physical (rho<=0, p<=0 or NaN)");
     return EFVM_OK;
 }
@@ -779,6 +783,68 @@ int efvm_total_mass(efvm_ctx* c, double* out) {
 int efvm_get_stream(efvm_ctx* c, void** stream) {
     if (!c || !stream) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     *stream = (void*)c->stream;
+    return EFVM_OK;
+}
+
+int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
+    if (!c || !out_ms || n_steps < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid argument");
+    if (c->params.integrator == EFVM_INTEGRATOR_EULER || c->rk_stage != 0)
+        return fail(c, EFVM_ERR_INVALID_ARG, "efvm_profile_steps needs an RK3 context at a step boundary");
+    if (c->control_dirty) sync_control(c, 0, 0.0, 0);
+    int rc = prologue(c);
+    if (rc) return rc;
+    cudaEvent_t ev[8];
+    for (auto& e : ev) CUDA_TRY(c, cudaEventCreate(&e));
+    double acc[4] = {0, 0, 0, 0};
+    Ibm ib = c->ibm_desc;
+    ib.history = nullptr;
+    double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
+    for (int64_t k = 0; k < n_steps; ++k) {
+        CUDA_TRY(c, cudaEventRecord(ev[0], S(c)));
+        c->launches += launch_step_setup(c->ph, c->st, S(c));
+        CUDA_TRY(c, cudaEventRecord(ev[1], S(c)));
+        float ms_stage = 0.f, ms_ibm = 0.f;
+        for (int s = 0; s < 3; ++s) {
+            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s], c->mask, c->st, s, 1, 0, s, S(c));
+            CUDA_TRY(c, cudaEventRecord(ev[2], S(c)));
+            StageArgs a{};
+            a.g = c->g;
+            a.ph = c->ph;
+            a.uin = bufs[s];
+            a.u0 = c->U[0];
+            a.uout = bufs[s + 1];
+            a.mask = c->ibm ? c->mask : nullptr;
+            a.yw = c->yw;
+            a.st = c->st;
+            a.stage = s;
+            a.completes_step = s == 2;
+            a.want_cfl = s == 2 && c->ph.fixed_dt <= 0.0;
+            c->launches += launch_stage(a, 0, 0, S(c));
+            CUDA_TRY(c, cudaEventRecord(ev[3], S(c)));
+            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->mask, c->st, s, 0, 1, s, S(c));
+            CUDA_TRY(c, cudaEventRecord(ev[4], S(c)));
+            CUDA_TRY(c, cudaEventSynchronize(ev[4]));
+            float t_stage = 0.f, t_after = 0.f;
+            cudaEventElapsedTime(&t_stage, ev[2], ev[3]);
+            cudaEventElapsedTime(&t_after, ev[3], ev[4]);
+            float t_before = 0.f;
+            cudaEventElapsedTime(&t_before, s == 0 ? ev[1] : ev[5], ev[2]);
+            ms_stage += t_stage;
+            ms_ibm += t_after + t_before;
+            CUDA_TRY(c, cudaEventRecord(ev[5], S(c)));
+        }
+        CUDA_TRY(c, cudaEventSynchronize(ev[5]));
+        float t_setup = 0.f, t_step = 0.f;
+        cudaEventElapsedTime(&t_setup, ev[0], ev[1]);
+        cudaEventElapsedTime(&t_step, ev[0], ev[5]);
+        acc[0] += ms_stage;
+        acc[1] += ms_ibm;
+        acc[2] += t_setup;
+        acc[3] += t_step;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 4; ++k) out_ms[k] = acc[k];
+    CUDA_TRY(c, cudaGetLastError());
     return EFVM_OK;
 }
 

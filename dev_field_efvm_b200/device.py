@@ -23,6 +23,7 @@ EXPORTS = (
     "efvm_download_state", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
+    "efvm_profile_steps",
 )
 
 
@@ -64,6 +65,7 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_total_mass.argtypes = [vp, dp]
     L.efvm_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.efvm_profile_steps.argtypes = [vp, i64, dp]
     if L.efvm_abi_version() != abi.ABI_VERSION:
         raise ImportError("libefvm_b200.so ABI version mismatch")
     if path is None:
@@ -129,6 +131,16 @@ class Context:
 
     def substep(self) -> None:
         self._check(self.L.efvm_substep(self.h))
+
+    def step_async(self, n_steps: int) -> None:
+        """Enqueue whole steps on the context's stream without waiting."""
+        self._check(self.L.efvm_step(self.h, int(n_steps), 0, 0.0, None, None))
+
+    def profile_steps(self, n_steps: int) -> np.ndarray:
+        """Device ms of [stage kernels, IBM kernels, step set-up, whole steps]."""
+        out = np.zeros(4)
+        self._check(self.L.efvm_profile_steps(self.h, int(n_steps), _dp(out)))
+        return out
 
     def step(self, n_steps: int, t_stop: float | None = None, history: bool = False):
         info = abi.EfvmStepInfo()

@@ -209,7 +209,11 @@ int efvm_substep(efvm_ctx* ctx);
  * When force_history is not NULL it receives the MarkerForce after every
  * substage (6 doubles each: pressure xyz, viscous xyz), capacity
  * 3*n_steps*6 doubles, as examples/cylinder_drag_validation/main.rs:334-340
- * reads it.  Returns EFVM_ERR_NONPHYSICAL if the state went non-physical. */
+ * reads it.  Returns EFVM_ERR_NONPHYSICAL if the state went non-physical.
+ * With stop_at_t == 0, force_history == NULL and info == NULL the call only
+ * enqueues the work on the context's stream and returns without waiting; a
+ * non-physical state is then reported by the next synchronising call
+ * (efvm_get_solver_state, efvm_step with info, a download). */
 int efvm_step(efvm_ctx* ctx, int64_t n_steps, int32_t stop_at_t, double t_stop,
               double* force_history, efvm_step_info* info);
 
@@ -252,6 +256,13 @@ int efvm_total_mass(efvm_ctx* ctx, double* out);
 int efvm_get_stream(efvm_ctx* ctx, void** stream);
 /* Number of kernels this context has launched since creation. */
 int efvm_launch_count(efvm_ctx* ctx, uint64_t* out);
+
+/* Run n_steps whole steps with individually launched kernels and CUDA events
+ * around each kernel class on the context's stream; out_ms[0..3] receives the
+ * summed device time of the stage kernels, the IBM mirror/force kernels, the
+ * per-step set-up kernel, and the whole steps.  Instrumentation for the bench
+ * (the reference has no timers). */
+int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
 
 #ifdef __cplusplus
 }

@@ -241,3 +241,48 @@ def test_t_stop_step_count_matches_oracle():
     di = d.run_until(0.25)
     assert oi.steps_done == di.steps_done and di.stopped_at_t_stop == 1
     assert abs(oi.time - di.time) < 1e-13
+
+
+FIX = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_fixtures.npz"))
+PINS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "oracle_pins.json")))
+
+
+def test_committed_golden_fixtures_on_gpu():
+    grid, params, u, ex = vortex_periodic(32)
+    d = Context(grid, params)
+    d.upload(FIX["vortex32_init"])
+    d.step(5)
+    assert rel_err(d.download(), FIX["vortex32_periodic_muscl_minmod_5steps"]) < TOL_MANY_STEPS
+    grid, params, u, ex = cases.cylinder_case(110, 41, muscl=True)
+    d = Context(grid, params)
+    d.set_cylinders(ex["cylinders"], ex["freestream"])
+    d.upload(FIX["cylinder110x41_init"])
+    info, hist = d.step(3, history=True)
+    assert np.array_equal(d.solid_mask(), FIX["cylinder110x41_mask"])
+    assert rel_err(d.download(), FIX["cylinder110x41_muscl_3steps"]) < TOL_MANY_STEPS
+    ref = FIX["cylinder110x41_muscl_3steps_marker_history"]
+    assert np.max(np.abs(hist - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+def test_reference_cylinder_drag_is_reproduced_on_gpu():
+    """examples/cylinder_drag_validation/config.toml on the GPU: 440x82, first-order
+    HLLC, 44,000 substeps; Cd over the last 10 % must print as the reference's
+    5.6312, agree with the oracle's full run, and sit on a steady plateau."""
+    grid, params, u, ex = cases.cylinder_case()
+    d = Context(grid, params)
+    d.set_cylinders(ex["cylinders"], ex["freestream"])
+    d.upload(u)
+    n = 44000
+    full, rest = divmod(n, 3)
+    info, hist = d.step(full, history=True)
+    fx = list(hist[:, 0] + hist[:, 3])
+    for _ in range(rest):
+        d.substep()
+        f = d.marker_force()
+        fx.append(f[0] + f[3])
+    cd = np.array(fx[int(0.9 * n):]) / ex["q"]
+    pin = PINS["cylinder_dfg_2d1_440x82"]
+    assert f"{cd.mean():.4f}" == f"{pin['published']:.4f}"
+    assert abs(cd.mean() - pin["cd_mean_last_10pct"]) <= 1e-8 * pin["cd_mean_last_10pct"]
+    assert (cd.max() - cd.min()) / abs(cd.mean()) <= 0.02
+    assert abs(cd.mean() - 5.5795) / 5.5795 <= 0.05
