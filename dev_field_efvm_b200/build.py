@@ -23,7 +23,7 @@ HEADERS = ["efvm_internal.h", "efvm_math.cuh", "../../include/efvm.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC,-ffp-contract=off",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
     "-Xptxas", "-v",
 ]
 

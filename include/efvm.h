@@ -26,6 +26,9 @@
 #ifdef __cplusplus
 extern "C" {
 #endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
 
 #define EFVM_ABI_VERSION 1
 
@@ -264,6 +267,9 @@ int efvm_launch_count(efvm_ctx* ctx, uint64_t* out);
  * (the reference has no timers). */
 int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
 
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 #ifdef __cplusplus
 }
 #endif
