@@ -309,6 +309,10 @@ bool bc_supported(int k) { return k >= EFVM_BC_SUPERSONIC_OUTFLOW && k <= EFVM_B
 
 }  // namespace
 
+namespace efvm {
+void set_global_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace efvm
+
 extern "C" {
 
 int efvm_abi_version(void) { return EFVM_ABI_VERSION; }

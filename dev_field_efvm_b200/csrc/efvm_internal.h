@@ -128,6 +128,9 @@ struct StageArgs {
     int want_cfl;
 };
 
+// Sets the message efvm_last_error(NULL) returns (efvm_api.cu).
+void set_global_error(const std::string& msg);
+
 // Host-side launch wrappers (efvm_kernels.cu); each returns the number of
 // kernels it launched.
 int launch_stage(const StageArgs& a, int tile_x, int tile_y, void* stream);

@@ -23,7 +23,7 @@ EXPORTS = (
     "efvm_download_state", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
-    "efvm_profile_steps",
+    "efvm_profile_steps", "efvm_cfl_dt_noalloc",
 )
 
 
@@ -66,6 +66,7 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_profile_steps.argtypes = [vp, i64, dp]
+    L.efvm_cfl_dt_noalloc.argtypes = [vp, vp, vp, vp, i64, C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), vp, vp]
     if L.efvm_abi_version() != abi.ABI_VERSION:
         raise ImportError("libefvm_b200.so ABI version mismatch")
     if path is None:

@@ -267,6 +267,38 @@ int efvm_launch_count(efvm_ctx* ctx, uint64_t* out);
  * (the reference has no timers). */
 int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
 
+/* ---- CFL time step without any allocation -------------------------------- */
+
+/* Rows of scratch that efvm_cfl_dt_noalloc keeps in static device memory. */
+#define EFVM_CFL_NOALLOC_MAX_ROWS 16384
+
+/* The CFL time step (cfl / max wave speed, or fixed_dt) of a state that the
+ * caller keeps in its own device memory, computed without allocating anything.
+ * It has no counterpart in the reference; it evaluates the same wave speed as
+ * efvm_cfl.
+ *
+ * It is for callers that cannot call cudaMalloc or let a library do it: a host
+ * whose device memory is handed out by its own allocator (a framework's memory
+ * pool or a fixed per-process budget) has to supply every buffer itself.  Here
+ * the caller passes the four conserved planes (device pointers to interior cell
+ * (0,0); cell (i,j) at plane[j*pitch + i], pitch in doubles), the grid and
+ * params that define spacing, gas and viscosity, a device pointer that
+ * receives dt, and the stream to run on (NULL = default stream).  The call is
+ * asynchronous on that stream.
+ *
+ * Its only scratch is file-scope device memory of the library: one double per
+ * grid row (EFVM_CFL_NOALLOC_MAX_ROWS rows, 128 KB) and a counter, held on
+ * every GPU that loads the library until the process exits.  Grids with more
+ * rows are rejected with EFVM_ERR_INVALID_ARG (use efvm_cfl).  All calls on a
+ * device share that scratch and it keeps the last call's contents; calls whose
+ * kernels overlap on the GPU race and may return a wrong dt, so order them on
+ * one stream.  The first call on a device looks up the scratch's device
+ * address (once per device, with that device current); make that first call
+ * before any stream capture.  Errors are reported by efvm_last_error(NULL). */
+int efvm_cfl_dt_noalloc(const double* rho, const double* rho_u, const double* rho_v, const double* rho_e,
+                        int64_t pitch, const efvm_grid* grid, const efvm_params* params, double* dt_out,
+                        void* stream);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
