@@ -42,7 +42,7 @@ UNIT = "cell-updates/s"
 
 
 def workload(name: str):
-    from oracle import cases  # case builders are plain numpy (no oracle code)
+    from dev_field_efvm_b200 import cases
     from dev_field_efvm_b200 import abi
     if name == "cylinder":
         grid, params, u, ex = cases.cylinder_baseline_case()

@@ -1,22 +1,17 @@
-"""Case definitions shared by the oracle pins, the tests and the bench.
+"""Case builders: the reference's case drivers and the benchmark workloads.
 
 Each builder returns (grid, params, initial interior state (ny, nx, 5), extras)
-for one of the reference's case drivers or one of the benchmark configurations.
-Plain numpy; no device and no oracle code runs here.
+for one of the reference's drivers (vortex gates, Sod, periodic pulse,
+Poiseuille, DFG cylinder) or a benchmark configuration.  Plain numpy: these
+generate synthetic inputs and exact solutions; nothing here runs a solver.
 """
 from __future__ import annotations
 
 import math
-import os
-import sys
 
 import numpy as np
 
-_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-if _REPO not in sys.path:
-    sys.path.insert(0, _REPO)
-
-from dev_field_efvm_b200 import abi  # noqa: E402
+from . import abi
 
 R_GAS_AIR = 287.058
 

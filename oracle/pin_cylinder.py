@@ -22,7 +22,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(_HERE))
 
-from oracle import cases, pyoracle  # noqa: E402
+from dev_field_efvm_b200 import cases
+from oracle import pyoracle  # noqa: E402
 
 
 def main() -> None:

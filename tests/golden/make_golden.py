@@ -18,7 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from dev_field_efvm_b200 import abi  # noqa: E402
-from oracle import cases, pyoracle  # noqa: E402
+from dev_field_efvm_b200 import cases
+from oracle import pyoracle  # noqa: E402
 
 
 def main():

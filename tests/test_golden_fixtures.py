@@ -4,7 +4,8 @@ import os
 
 import numpy as np
 
-from oracle import cases, pyoracle
+from dev_field_efvm_b200 import cases
+from oracle import pyoracle
 
 FIX = np.load(os.path.join(os.path.dirname(__file__), "golden", "oracle_fixtures.npz"))
 

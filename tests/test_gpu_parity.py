@@ -17,7 +17,7 @@ import pytest
 import exact_riemann as er
 from dev_field_efvm_b200 import abi
 from dev_field_efvm_b200.device import Context, EfvmError
-from oracle import cases
+from dev_field_efvm_b200 import cases
 from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu

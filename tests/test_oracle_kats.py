@@ -5,7 +5,7 @@ import pytest
 
 from dev_field_efvm_b200 import abi
 from oracle import pyoracle as po
-from oracle import cases
+from dev_field_efvm_b200 import cases
 
 RUS, HLLC, HLLC_TB = abi.FLUX_RUSANOV, abi.FLUX_HLLC, abi.FLUX_HLLC_TEXTBOOK
 

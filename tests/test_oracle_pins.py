@@ -13,7 +13,7 @@ import pytest
 
 import exact_riemann as er
 from dev_field_efvm_b200 import abi
-from oracle import cases
+from dev_field_efvm_b200 import cases
 from oracle import pyoracle as po
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_published.json")))

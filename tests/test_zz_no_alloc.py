@@ -17,7 +17,7 @@ import pytest
 
 from dev_field_efvm_b200 import abi, device
 from dev_field_efvm_b200.device import Context
-from oracle import cases
+from dev_field_efvm_b200 import cases
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
