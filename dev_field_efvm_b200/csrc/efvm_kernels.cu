@@ -1,12 +1,12 @@
 // efvm_kernels.cu — sm_100a kernels of the explicit finite-volume step.
 //
-//   stage_kernel   one RK substage over a 2-D tile: MUSCL slopes, L/R face
+//   stage_kernel   one RK substage over strips of 31 columns: MUSCL slopes, L/R face
 //                  states, one numerical flux per face (HLLC-Thornber /
 //                  textbook HLLC / Rusanov), flux divergence, viscous terms,
 //                  solid-cell zeroing, body force, SSP-RK3 (or Euler)
 //                  combination, and on the step's last stage the sponge, the
 //                  boundary-ghost refill of the output and the CFL wave-speed
-//                  max (one atomic per block).
+//                  max (one atomic per warp).
 //   fill_ghosts    Halo + Boundary phases for a freshly uploaded state.
 //   step_setup     per-step dt = cfl / max wave speed, clock/stop bookkeeping.
 //   ibm_kernel     ghost-cell IBM mirror (bilinear image sample) and, after a
@@ -172,31 +172,56 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* t
     }
 }
 
-// Face state of one cell toward +x/+y (sgn = +1) or -x/-y (sgn = -1): centre
-// value, or centre +- half the limited slope (reconstruct_to_face and
-// limited_slope_cons, crates/cfd_solver/src/lib.rs:199-211,273-286).  m/c/p are
-// the previous/own/next cells along the face normal.  The FP32 path takes the
-// differences in FP64 and limits and extrapolates in FP32.
+// A conserved state in the reconstruction precision R, grid frame.
 template <class R>
-__device__ __forceinline__ R recon(double m, double c, double p, int limiter, bool rec, double sgn) {
-    if (!rec) return R(c);
-    if (sizeof(R) == sizeof(double)) {
-        const double s = limit<double>(limiter, p - c, c - m);
-        return R(c + s * sgn * 0.5);
-    } else {
-        const float s = limit<float>(limiter, (float)(p - c), (float)(c - m));
-        return R((float)c + s * (float)sgn * 0.5f);
-    }
+struct V4 {
+    R r, mx, my, E;
+};
+template <class R>
+__device__ __forceinline__ V4<R> toR(const U4& u) {
+    return V4<R>{R(u.r), R(u.mx), R(u.my), R(u.E)};
+}
+__device__ __forceinline__ U4 toU4(const V4<double>& u) { return U4{u.r, u.mx, u.my, u.E}; }
+__device__ __forceinline__ U4 toU4(const V4<float>& u) { return U4{u.r, u.mx, u.my, u.E}; }
+// The state in the frame of an x-face (normal x) or a y-face (normal y).
+template <class R>
+__device__ __forceinline__ Q4<R> xq(const V4<R>& u) {
+    return Q4<R>{u.r, u.mx, u.my, u.E};
+}
+template <class R>
+__device__ __forceinline__ Q4<R> yq(const V4<R>& u) {
+    return Q4<R>{u.r, u.my, u.mx, u.E};
 }
 
-__device__ __forceinline__ U4 shfl_up4(const U4& u, int d) {
-    return U4{__shfl_up_sync(0xffffffffu, u.r, d), __shfl_up_sync(0xffffffffu, u.mx, d),
-              __shfl_up_sync(0xffffffffu, u.my, d), __shfl_up_sync(0xffffffffu, u.E, d)};
+// The two face states c + s/2 (toward the next cell) and c - s/2 (toward the
+// previous one) of a cell, s = lim(p - c, c - m) per conserved variable
+// (limited_slope_cons and reconstruct_to_face, crates/cfd_solver/src/lib.rs:199-211,273-286);
+// m/c/p are the previous/own/next cells along the face normal.  The FP32 path
+// takes the differences in FP32.
+template <class R>
+__device__ __forceinline__ R half_slope(int limiter, R m, R c, R p) {
+    return limit<R>(limiter, p - c, c - m) * R(0.5);
 }
-__device__ __forceinline__ U4 shfl_down4(const U4& u, int d) {
-    return U4{__shfl_down_sync(0xffffffffu, u.r, d), __shfl_down_sync(0xffffffffu, u.mx, d),
-              __shfl_down_sync(0xffffffffu, u.my, d), __shfl_down_sync(0xffffffffu, u.E, d)};
+template <class R>
+__device__ __forceinline__ void slope_faces(int limiter, const V4<R>& m, const V4<R>& c, const V4<R>& p, V4<R>& plus,
+                                            V4<R>& minus) {
+    const R hr = half_slope(limiter, m.r, c.r, p.r), hx = half_slope(limiter, m.mx, c.mx, p.mx);
+    const R hy = half_slope(limiter, m.my, c.my, p.my), he = half_slope(limiter, m.E, c.E, p.E);
+    plus = V4<R>{c.r + hr, c.mx + hx, c.my + hy, c.E + he};
+    minus = V4<R>{c.r - hr, c.mx - hx, c.my - hy, c.E - he};
 }
+
+template <class R>
+__device__ __forceinline__ V4<R> shfl_up_v(const V4<R>& u, int d) {
+    return V4<R>{__shfl_up_sync(0xffffffffu, u.r, d), __shfl_up_sync(0xffffffffu, u.mx, d),
+                 __shfl_up_sync(0xffffffffu, u.my, d), __shfl_up_sync(0xffffffffu, u.E, d)};
+}
+template <class R>
+__device__ __forceinline__ V4<R> shfl_down_v(const V4<R>& u, int d) {
+    return V4<R>{__shfl_down_sync(0xffffffffu, u.r, d), __shfl_down_sync(0xffffffffu, u.mx, d),
+                 __shfl_down_sync(0xffffffffu, u.my, d), __shfl_down_sync(0xffffffffu, u.E, d)};
+}
+
 template <class R>
 __device__ __forceinline__ Q4<R> shfl_up_q(const Q4<R>& u, int d) {
     return Q4<R>{__shfl_up_sync(0xffffffffu, u.r, d), __shfl_up_sync(0xffffffffu, u.mn, d),
@@ -260,100 +285,105 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
     const int jb = blockIdx.y * rows;
     double lam = 0.0;
     if (i0 < g.nx && jb < g.ny) {  // uniform across the warp
+        constexpr bool MUSCL = RECON == EFVM_RECON_MUSCL;
+        constexpr bool FP64 = sizeof(R) == sizeof(double);
         const int je = min(jb + rows, g.ny);
         const int i = i0 + lane;
         const int ic = min(i, g.nx + NG - 1);  // clamped load column (lanes past the grid)
         const bool owner = lane < STRIP && i < g.nx;
-        const bool muscl = RECON == EFVM_RECON_MUSCL;
         const bool true_seam = ph.periodic_seam == EFVM_SEAM_TRUE_PERIODIC;
         const double gm1 = ph.gamma - 1.0;
         const R rg = R(ph.gamma), rgm1 = R(gm1);
         const double* __restrict__ uin = a.uin;
         auto ld = [&](int ii, int jj) { return load4(uin, P, cidx(g, ii, jj)); };
+        const double* __restrict__ colp = uin + cidx(g, ic, 0);  // this lane's column at row 0
+        auto ldrow = [&](int jj) { return toR<R>(load4(colp, P, (long long)jj * g.pitch)); };
 
-        // x-face recon flags of this lane's face (between columns i-1 and i)
-        bool rec_l = muscl, rec_r = muscl;
+        // Reconstruction flags of the faces on the domain edge; every interior
+        // face reconstructs both sides under MUSCL.  x: this lane's face, between
+        // columns i-1 and i.  y: the faces below row 0 and above row ny-1.
+        bool rec_l = MUSCL, rec_r = MUSCL;
         if (i == 0) {
-            rec_l = muscl && ph.periodic_x && true_seam;
-            rec_r = muscl && ph.periodic_x;
+            rec_l = MUSCL && ph.periodic_x && true_seam;
+            rec_r = MUSCL && ph.periodic_x;
         } else if (i == g.nx) {
-            rec_l = muscl && ph.periodic_x;
-            rec_r = muscl && ph.periodic_x && true_seam;
+            rec_l = MUSCL && ph.periodic_x;
+            rec_r = MUSCL && ph.periodic_x && true_seam;
         }
+        const bool seam_rec = MUSCL && ph.periodic_y && true_seam;  // the side across the periodic seam
+        const bool edge_rec = MUSCL && ph.periodic_y;               // the side inside the domain
 
-        // y-face flux (grid frame) between rows j and j+1 at this lane's column
-        auto yflux = [&](int j) -> U4 {
-            bool rec_b = muscl, rec_t = muscl;
-            if (j == -1) {
-                rec_b = muscl && ph.periodic_y && true_seam;
-                rec_t = muscl && ph.periodic_y;
-            } else if (j + 1 == g.ny) {
-                rec_b = muscl && ph.periodic_y;
-                rec_t = muscl && ph.periodic_y && true_seam;
+        // Row window of this lane's column: uc = U(j), un = U(j+1); pc = +y face
+        // state of row j; gb = flux of the y-face below row j (face frame).  Each
+        // row is loaded once and its y-slope limited once.  The loop starts one
+        // row early, where it only forms the face below the first row, so that
+        // every y-face flux comes from the same code: a face on the edge of two
+        // warps' row ranges is computed by both and must agree bit for bit.
+        V4<R> uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
+        if (MUSCL) {
+            V4<R> unused;
+            slope_faces(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
+        }
+        Q4<R> gb;
+        for (int j = jb - 1; j < je; ++j) {
+            const V4<R> un2 = ldrow(j + 2);
+
+            // ---- y-face above row j ----
+            Q4<R> gt;
+            V4<R> pn = un;  // +y face state of row j+1
+            if (MUSCL) {
+                V4<R> mn;
+                slope_faces(ph.limiter, uc, un, un2, pn, mn);
+                const bool lo_edge = j == -1, hi_edge = j + 1 == g.ny;
+                const bool rb = lo_edge ? seam_rec : (hi_edge ? edge_rec : true);
+                const bool rt = lo_edge ? edge_rec : (hi_edge ? seam_rec : true);
+                gt = face_flux<SCHEME, R>(yq(rb ? pc : uc), yq(rt ? mn : un), rg, rgm1);
+            } else {
+                gt = face_flux<SCHEME, R>(yq(uc), yq(un), rg, rgm1);
             }
-            const U4 u0 = ld(ic, j), u1 = ld(ic, j + 1);
-            U4 um = u0, u2 = u1;
-            if (rec_b) um = ld(ic, j - 1);
-            if (rec_t) u2 = ld(ic, j + 2);
-            Q4<R> B, T;
-            B.r = recon<R>(um.r, u0.r, u1.r, ph.limiter, rec_b, 1.0);
-            B.mn = recon<R>(um.my, u0.my, u1.my, ph.limiter, rec_b, 1.0);
-            B.mt = recon<R>(um.mx, u0.mx, u1.mx, ph.limiter, rec_b, 1.0);
-            B.E = recon<R>(um.E, u0.E, u1.E, ph.limiter, rec_b, 1.0);
-            T.r = recon<R>(u0.r, u1.r, u2.r, ph.limiter, rec_t, -1.0);
-            T.mn = recon<R>(u0.my, u1.my, u2.my, ph.limiter, rec_t, -1.0);
-            T.mt = recon<R>(u0.mx, u1.mx, u2.mx, ph.limiter, rec_t, -1.0);
-            T.E = recon<R>(u0.E, u1.E, u2.E, ph.limiter, rec_t, -1.0);
-            const Q4<R> f = face_flux<SCHEME, R>(B, T, rg, rgm1);
-            return U4{(double)f.r, (double)f.mt, (double)f.mn, (double)f.E};
-        };
-
-        U4 gb = yflux(jb - 1);
-        for (int j = jb; j < je; ++j) {
-            const U4 gt = yflux(j);
+            if (j < jb) {  // warp-uniform: the face below the first row only
+                gb = gt;
+                uc = un;
+                un = un2;
+                pc = pn;
+                continue;
+            }
 
             // ---- x-face on the left of column i, row j ----
-            const U4 uc = ld(ic, j);
-            U4 ul = shfl_up4(uc, 1), ur = shfl_down4(uc, 1);
-            U4 ull = ul;  // column i-2 (lane 0 only)
+            V4<R> ul = shfl_up_v(uc, 1), ur = shfl_down_v(uc, 1);
+            V4<R> ull = ul;  // column i-2 (lane 0 only)
             if (lane == 0) {
-                ul = ld(i0 - 1, j);
-                if (muscl) ull = ld(i0 - 2, j);
+                ul = toR<R>(ld(i0 - 1, j));
+                if (MUSCL) ull = toR<R>(ld(i0 - 2, j));
             }
-            if (lane == 31) ur = ld(min(i0 + 32, g.nx + NG - 1), j);
-            Q4<R> Pp, M;  // this column's +x and -x face states
-            Pp.r = recon<R>(ul.r, uc.r, ur.r, ph.limiter, muscl, 1.0);
-            Pp.mn = recon<R>(ul.mx, uc.mx, ur.mx, ph.limiter, muscl, 1.0);
-            Pp.mt = recon<R>(ul.my, uc.my, ur.my, ph.limiter, muscl, 1.0);
-            Pp.E = recon<R>(ul.E, uc.E, ur.E, ph.limiter, muscl, 1.0);
-            M.r = recon<R>(ul.r, uc.r, ur.r, ph.limiter, muscl, -1.0);
-            M.mn = recon<R>(ul.mx, uc.mx, ur.mx, ph.limiter, muscl, -1.0);
-            M.mt = recon<R>(ul.my, uc.my, ur.my, ph.limiter, muscl, -1.0);
-            M.E = recon<R>(ul.E, uc.E, ur.E, ph.limiter, muscl, -1.0);
-            Q4<R> Lp = shfl_up_q(Pp, 1);  // +x state of column i-1
-            if (lane == 0 && muscl) {
-                Lp.r = recon<R>(ull.r, ul.r, uc.r, ph.limiter, true, 1.0);
-                Lp.mn = recon<R>(ull.mx, ul.mx, uc.mx, ph.limiter, true, 1.0);
-                Lp.mt = recon<R>(ull.my, ul.my, uc.my, ph.limiter, true, 1.0);
-                Lp.E = recon<R>(ull.E, ul.E, uc.E, ph.limiter, true, 1.0);
+            if (MUSCL && lane == 31) ur = toR<R>(ld(min(i0 + 32, g.nx + NG - 1), j));
+            Q4<R> fx;
+            if (MUSCL) {
+                V4<R> pp, mm;  // this column's +x and -x face states
+                slope_faces(ph.limiter, ul, uc, ur, pp, mm);
+                V4<R> lp = shfl_up_v(pp, 1);  // +x state of column i-1
+                if (lane == 0) {
+                    V4<R> unused;
+                    slope_faces(ph.limiter, ull, ul, uc, lp, unused);
+                }
+                fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : uc), rg, rgm1);
+            } else {
+                fx = face_flux<SCHEME, R>(xq(ul), xq(uc), rg, rgm1);
             }
-            const Q4<R> Lc{R(ul.r), R(ul.mx), R(ul.my), R(ul.E)};
-            const Q4<R> Rc{R(uc.r), R(uc.mx), R(uc.my), R(uc.E)};
-            const Q4<R> L = rec_l ? Lp : Lc;
-            const Q4<R> Rs = rec_r ? M : Rc;
-            const Q4<R> fx = face_flux<SCHEME, R>(L, Rs, rg, rgm1);
             const Q4<R> fxr = shfl_down_q(fx, 1);  // face on the right of column i
 
             if (owner) {
                 const long long o = cidx(g, i, j);
+                // the cell's state in FP64 (the FP32 path reads it again)
+                const U4 ucd = FP64 ? toU4(uc) : ld(i, j);
                 // Flux divergence in the reference's accumulation order: the face
                 // below (scattered when row j-1 was visited), the face on the
                 // left, then the cell's own +x and +y faces (for_each_face order,
                 // crates/cfd_solver/src/lib.rs:333-337).
                 const double fl[4] = {(double)fx.r, (double)fx.mn, (double)fx.mt, (double)fx.E};
                 const double fr[4] = {(double)fxr.r, (double)fxr.mn, (double)fxr.mt, (double)fxr.E};
-                const double gbv[4] = {gb.r, gb.mx, gb.my, gb.E};
-                const double gtv[4] = {gt.r, gt.mx, gt.my, gt.E};
+                const double gbv[4] = {(double)gb.r, (double)gb.mt, (double)gb.mn, (double)gb.E};
+                const double gtv[4] = {(double)gt.r, (double)gt.mt, (double)gt.mn, (double)gt.E};
                 double rhs[4];
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
@@ -368,9 +398,10 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
                 if (ph.viscous && !solid) {
                     // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D)
                     double us, vs, ts;
-                    prim_uvt(uc, gm1, ph.r_gas, us, vs, ts);
+                    prim_uvt(ucd, gm1, ph.r_gas, us, vs, ts);
                     double nu[4], nv[4], nt[4];  // +x, -x, +y, -y
-                    const U4 nbs[4] = {ur, ul, ld(i, j + 1), ld(i, j - 1)};
+                    const U4 nbs[4] = {FP64 ? toU4(ur) : ld(i + 1, j), FP64 ? toU4(ul) : ld(i - 1, j),
+                                       FP64 ? toU4(un) : ld(i, j + 1), ld(i, j - 1)};
                     const long long no[4] = {o + 1, o - 1, o + g.pitch, o - g.pitch};
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
@@ -395,26 +426,26 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
                 }
                 if (solid) rhs[0] = rhs[1] = rhs[2] = rhs[3] = 0.0;  // zero_solid_rhs, crates/cfd_ibm/src/lib.rs:293-301
                 if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
-                    rhs[1] += uc.r * ph.body_force_x;
-                    rhs[3] += ph.body_force_x * uc.mx;
+                    rhs[1] += ucd.r * ph.body_force_x;
+                    rhs[3] += ph.body_force_x * ucd.mx;
                 }
 
                 // Rk3Integrator / EulerIntegrator::substep, crates/cfd_solver/src/integrate.rs:48-101
                 const double dt = a.st->dt;
-                const double ucv[4] = {uc.r, uc.mx, uc.my, uc.E};
-                double un[4];
+                const double ucv[4] = {ucd.r, ucd.mx, ucd.my, ucd.E};
+                double un_[4];
                 if (a.stage == 1 || a.stage == 2) {
                     const double w0 = a.stage == 1 ? 0.75 : (1.0 / 3.0);
                     const double w1 = a.stage == 1 ? 0.25 : (2.0 / 3.0);
 #pragma unroll
                     for (int v = 0; v < 4; ++v)
-                        un[v] = __dadd_rn(__dmul_rn(w0, a.u0[v * P + o]),
-                                          __dmul_rn(w1, __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt))));
+                        un_[v] = __dadd_rn(__dmul_rn(w0, a.u0[v * P + o]),
+                                           __dmul_rn(w1, __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt))));
                 } else {
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) un[v] = __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt));
+                    for (int v = 0; v < 4; ++v) un_[v] = __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt));
                 }
-                U4 nw{un[0], un[1], un[2], un[3]};
+                U4 nw{un_[0], un_[1], un_[2], un_[3]};
 
                 if (a.completes_step && ph.sponge) {
                     // outlet_sponge_system, examples/cylinder_drag_validation/main.rs:186-229
@@ -438,16 +469,19 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
                 write_ghosts(g, ph, a.uout, i, j, nw);
 
                 // non-physical state flag (rho<=0, p<=0, NaN)
-                const double pn = pressure_d(nw, gm1);
+                const double pn_ = pressure_d(nw, gm1);
                 int bad = 0;
                 if (!(nw.r > 0.0)) bad |= 1;
-                if (!(pn > 0.0)) bad |= 2;
+                if (!(pn_ > 0.0)) bad |= 2;
                 if (nw.r != nw.r || nw.mx != nw.mx || nw.my != nw.my || nw.E != nw.E) bad |= 4;
                 if (bad) atomicOr(&a.st->nonphysical, bad);
 
                 if (a.completes_step && a.want_cfl) lam = fmax(lam, wave_speed(g, ph, nw));
             }
             gb = gt;
+            uc = un;
+            un = un2;
+            pc = pn;
         }
     }
     // wave-speed max for the next step's CFL dt: one atomic per warp
@@ -890,26 +924,29 @@ static int grid_for(long long n, int block) {
     return (int)b;
 }
 
-// Rows per warp: enough warps for a few waves over the 148 SMs, at most 64
-// rows (each strip re-evaluates one y face at its first row).
-static int rows_per_warp(int nx, int ny) {
+// Rows each warp marches.  Small grids take the fewest rows that still fill the
+// resident slots in one wave (the warp's first row also pays for the face below
+// it); large grids take 8, measured fastest at 4096^2: with longer runs the rows
+// that the resident blocks span at once no longer fit in L2 and the halo rows
+// each block re-reads come from HBM.
+static int rows_per_warp(int nx, int ny, int blocks_per_sm) {
     const long long strips = (nx + STRIP - 1) / STRIP;
-    const long long target_warps = 148LL * 16 * 3;
-    long long rows = (strips * ny) / target_warps;
-    if (rows < 4) rows = 4;
-    if (rows > 64) rows = 64;
+    const long long slots = 148LL * blocks_per_sm * WPB;
+    long long rows = (strips * ny + slots - 1) / slots;
+    if (rows < 2) rows = 2;
+    if (rows > 8) rows = 8;
     return (int)rows;
 }
 
 template <int SCHEME, int RECON, class R>
 static void launch_stage_t(const StageArgs& a, cudaStream_t s) {
-    const int rows = rows_per_warp(a.g.nx, a.g.ny);
-    const int strips = (a.g.nx + STRIP - 1) / STRIP;
-    dim3 block(32 * WPB);
-    dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
     // Resident blocks per SM, measured at 4096^2: the FP64 flux is fastest at 96
     // registers/thread (5 blocks of 4 warps), the FP32 flux at 64 (8 blocks).
     constexpr int MINB = sizeof(R) == sizeof(double) ? 5 : 8;
+    const int rows = rows_per_warp(a.g.nx, a.g.ny, MINB);
+    const int strips = (a.g.nx + STRIP - 1) / STRIP;
+    dim3 block(32 * WPB);
+    dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
     stage_kernel<SCHEME, RECON, R, MINB><<<grid, block, 0, s>>>(a, rows);
 }
 
