@@ -513,13 +513,16 @@ __global__ void reset_lam_kernel(DevState* st) {
 // Per-step Setup: dt from the wave-speed max (cfl_system's final lines,
 // crates/cfd_solver/src/lib.rs:671-676) or fixed_dt, and the stop test of the
 // case drivers' `if t >= T_FINAL break`.
-__global__ void step_setup_kernel(Physics ph, DevState* st) {
-    if (!st->active) return;
-    if (st->nonphysical) {
-        st->active = 0;
-        return;
-    }
-    if (st->stop_at_t && st->time >= st->t_stop) {
+// The stop rule of step_setup: a non-physical state or t >= t_stop ends the run.
+__device__ __forceinline__ bool step_stops(const DevState* st) {
+    return st->nonphysical || (st->stop_at_t && st->time >= st->t_stop);
+}
+
+// Per-step set-up (one thread): stop check, dt = cfl / max wave speed (cfl_system,
+// crates/cfd_solver/src/lib.rs:647-669) and the switch of the wave-speed buffer
+// that the step's last stage accumulates into.
+__device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
+    if (step_stops(st)) {
         st->active = 0;
         return;
     }
@@ -534,6 +537,11 @@ __global__ void step_setup_kernel(Physics ph, DevState* st) {
     const int nxt = st->lam_idx ^ 1;
     st->lam[nxt] = 0ull;
     st->lam_idx = nxt;
+}
+
+__global__ void step_setup_kernel(Physics ph, DevState* st) {
+    if (!st->active) return;
+    step_setup(ph, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -648,11 +656,8 @@ __device__ __forceinline__ bool sample_bilinear(const Geometry& g, const Physics
 // Mirror (apply_ibm_ghost_bc, crates/cfd_ibm/src/lib.rs:258-289) of every solid
 // ghost cell, recording its pre-mirror value for the emulated z-ghost of the
 // staircase wall force.  One thread per ghost cell.
-__global__ void ibm_mirror_kernel(Geometry g, Physics ph, Ibm ib, double* q, const uint8_t* __restrict__ mask,
-                                  DevState* st, int stage) {
-    if (!st->active) return;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= ib.n_ghost) return;
+__device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& ph, const Ibm& ib, double* q,
+                                             const uint8_t* __restrict__ mask, int stage, int k) {
     const IbmGhostDev gh = ib.ghosts[k];
     const int j = (int)(gh.cell / g.nx), i = (int)(gh.cell - (long long)j * g.nx);
     const long long o = cidx(g, i, j);
@@ -679,17 +684,15 @@ __global__ void ibm_mirror_kernel(Geometry g, Physics ph, Ibm ib, double* q, con
 // substage history.
 constexpr int FORCE_THREADS = 256;
 
-__global__ void __launch_bounds__(FORCE_THREADS) ibm_forces_kernel(Geometry g, Physics ph, Ibm ib,
-                                                                   const double* __restrict__ q,
-                                                                   const uint8_t* __restrict__ mask, DevState* st,
-                                                                   int stage) {
-    if (!st->active) return;
+__device__ __forceinline__ void forces_block(const Geometry& g, const Physics& ph, const Ibm& ib,
+                                             const double* __restrict__ q, const uint8_t* __restrict__ mask,
+                                             DevState* st, int stage, int blk, int nblk) {
     __shared__ double red[6][FORCE_THREADS];
     __shared__ bool last;
     const int tid = threadIdx.x;
     const double gm1 = ph.gamma - 1.0;
     double f[6] = {0, 0, 0, 0, 0, 0};
-    if (blockIdx.x == 0) {
+    if (blk == 0) {
         for (int m = tid; m < ib.n_markers; m += blockDim.x) {
             const MarkerDev mk = ib.markers[m];
             if (!mk.valid) continue;
@@ -707,7 +710,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) ibm_forces_kernel(Geometry g, P
             }
         }
     } else {
-        const int k = (blockIdx.x - 1) * blockDim.x + tid;
+        const int k = (blk - 1) * blockDim.x + tid;
         if (k < ib.n_ghost) {
             const double dx = g.h[0], dy = g.h[1], dz = g.h[2];
             const double face_area[3] = {dy * dz, dx * dz, dx * dy};
@@ -768,19 +771,19 @@ __global__ void __launch_bounds__(FORCE_THREADS) ibm_forces_kernel(Geometry g, P
         __syncthreads();
     }
     if (tid == 0) {
-        double* part = ib.partials + 6LL * blockIdx.x;
+        double* part = ib.partials + 6LL * blk;
 #pragma unroll
         for (int d = 0; d < 6; ++d) part[d] = red[d][0];
         __threadfence();
         const unsigned int done = atomicAdd(ib.counter, 1u);
-        last = done == gridDim.x - 1;
+        last = done == nblk - 1;
     }
     __syncthreads();
     if (last && tid == 0) {
         __threadfence();
         const volatile double* part = ib.partials;
         double wall[6] = {0, 0, 0, 0, 0, 0};
-        for (int b = 1; b < (int)gridDim.x; ++b)
+        for (int b = 1; b < nblk; ++b)
             for (int d = 0; d < 6; ++d) wall[d] += part[6 * b + d];
         for (int d = 0; d < 6; ++d) {
             ib.force_out[d] = part[d];
@@ -792,6 +795,33 @@ __global__ void __launch_bounds__(FORCE_THREADS) ibm_forces_kernel(Geometry g, P
         }
         *ib.counter = 0u;  // ready for the next launch
     }
+}
+
+// One launch of the IBM work between two stage kernels: `n_force_blocks`
+// blocks integrate the marker and wall forces of the state q that stage
+// `force_stage` wrote, and the remaining blocks mirror the ghost cells of the
+// same q for stage `mirror_stage` (-1: none).  The two parts touch disjoint
+// data: the forces read fluid cells and the stage's z-fill, the mirror reads
+// fluid cells and writes solid cells and the next stage's z-fill.  With
+// `setup`, thread 0 of the first mirror block also does the per-step set-up,
+// and every mirror thread applies its stop rule itself, so a step that ends
+// there leaves the state untouched.
+__global__ void __launch_bounds__(FORCE_THREADS) ibm_kernel(Geometry g, Physics ph, Ibm ib, double* q,
+                                                            const uint8_t* __restrict__ mask, DevState* st,
+                                                            int force_stage, int n_force_blocks, int mirror_stage,
+                                                            int setup) {
+    if (!st->active) return;
+    const int b = blockIdx.x;
+    if (b < n_force_blocks) {  // uniform per block
+        forces_block(g, ph, ib, q, mask, st, force_stage, b, n_force_blocks);
+        return;
+    }
+    if (setup) {
+        if (b == n_force_blocks && threadIdx.x == 0) step_setup(ph, st);
+        if (step_stops(st)) return;
+    }
+    const int k = (b - n_force_blocks) * blockDim.x + threadIdx.x;
+    if (mirror_stage >= 0 && k < ib.n_ghost) mirror_ghost(g, ph, ib, q, mask, mirror_stage, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -1017,19 +1047,14 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
 }
 
 int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, const uint8_t* mask, DevState* st,
-               int stage, int do_mirror, int do_forces, int, void* stream) {
-    cudaStream_t s = (cudaStream_t)stream;
-    int n = 0;
-    if (do_mirror && ib.n_ghost > 0) {
-        ibm_mirror_kernel<<<(ib.n_ghost + 127) / 128, 128, 0, s>>>(g, ph, ib, q, mask, st, stage);
-        ++n;
-    }
-    if (do_forces) {
-        const int blocks = 1 + (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS;
-        ibm_forces_kernel<<<blocks, FORCE_THREADS, 0, s>>>(g, ph, ib, q, mask, st, stage);
-        n += 1;
-    }
-    return n;
+               int force_stage, int mirror_stage, int setup, void* stream) {
+    const int nf = force_stage >= 0 ? 1 + (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS : 0;
+    int nm = mirror_stage >= 0 ? (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS : 0;
+    if (setup && nm < 1) nm = 1;
+    if (nf + nm == 0) return 0;
+    ibm_kernel<<<nf + nm, FORCE_THREADS, 0, (cudaStream_t)stream>>>(g, ph, ib, q, mask, st, force_stage, nf,
+                                                                     mirror_stage, setup);
+    return 1;
 }
 
 int launch_pack(const Geometry& g, const double* src, int64_t si, int64_t sj, int64_t sv, double* q, int to_device,
