@@ -256,7 +256,7 @@ int prologue(efvm_ctx* c) {
     return EFVM_OK;
 }
 
-void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout) {
+void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, bool pdl = true) {
     StageArgs a{};
     a.g = c->g;
     a.ph = c->ph;
@@ -269,29 +269,29 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout) {
     a.stage = stage;
     a.completes_step = (stage == 2 || stage == 3) ? 1 : 0;
     a.want_cfl = a.completes_step && c->ph.fixed_dt <= 0.0;
-    c->launches += launch_stage(a, 0, 0, S(c));
+    c->launches += launch_stage(a, pdl, S(c));
 }
 
 // Launch the kernels of one substage at RK stage `stage` (0..2, or 3 = Euler):
 // [step set-up +] IBM mirror of uin, the stage, the IBM forces of uout.
 void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool with_setup) {
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uin, c->mask, c->st, -1, stage, with_setup, S(c));
-    else if (with_setup) c->launches += launch_step_setup(c->ph, c->st, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uin, c->mask, c->st, -1, stage, with_setup, true, S(c));
+    else if (with_setup) c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     enqueue_stage_kernel(c, stage, uin, uout);
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uout, c->mask, c->st, stage, -1, 0, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uout, c->mask, c->st, stage, -1, 0, true, S(c));
 }
 
 // One whole SSP-RK3 step.  With IBM the forces of a stage and the mirror of the
 // next run in one launch (7 launches a step instead of 10).
 void enqueue_rk3_step(efvm_ctx* c) {
     double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->mask, c->st, -1, 0, 1, S(c));
-    else c->launches += launch_step_setup(c->ph, c->st, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->mask, c->st, -1, 0, 1, true, S(c));
+    else c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     for (int s = 0; s < 3; ++s) {
         enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1]);
         if (c->ibm)
             c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->mask, c->st, s, s < 2 ? s + 1 : -1, 0,
-                                      S(c));
+                                      true, S(c));
     }
 }
 
@@ -821,15 +821,15 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
     double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
     for (int64_t k = 0; k < n_steps; ++k) {
         CUDA_TRY(c, cudaEventRecord(ev[0], S(c)));
-        c->launches += launch_step_setup(c->ph, c->st, S(c));
+        c->launches += launch_step_setup(c->ph, c->st, false, S(c));
         CUDA_TRY(c, cudaEventRecord(ev[1], S(c)));
         float ms_stage = 0.f, ms_ibm = 0.f;
         for (int s = 0; s < 3; ++s) {
-            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s], c->mask, c->st, -1, s, 0, S(c));
+            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s], c->mask, c->st, -1, s, 0, false, S(c));
             CUDA_TRY(c, cudaEventRecord(ev[2], S(c)));
-            enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1]);
+            enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1], false);
             CUDA_TRY(c, cudaEventRecord(ev[3], S(c)));
-            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->mask, c->st, s, -1, 0, S(c));
+            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->mask, c->st, s, -1, 0, false, S(c));
             CUDA_TRY(c, cudaEventRecord(ev[4], S(c)));
             CUDA_TRY(c, cudaEventSynchronize(ev[4]));
             float t_stage = 0.f, t_after = 0.f;

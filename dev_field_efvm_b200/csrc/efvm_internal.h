@@ -133,17 +133,18 @@ void set_global_error(const std::string& msg);
 
 // Host-side launch wrappers (efvm_kernels.cu); each returns the number of
 // kernels it launched.
-int launch_stage(const StageArgs& a, int tile_x, int tile_y, void* stream);
+// `pdl`: launch with programmatic stream serialization (the kernels of a step).
+int launch_stage(const StageArgs& a, bool pdl, void* stream);
 int launch_fill_ghosts(const Geometry& g, const Physics& ph, double* q, void* stream);
 int launch_cfl(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream);
-int launch_step_setup(const Physics& ph, DevState* st, void* stream);
+int launch_step_setup(const Physics& ph, DevState* st, bool pdl, void* stream);
 int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double* stagnant, const double* ambient,
                      double* q, uint8_t* mask, void* stream);
 // IBM work between stage kernels, one launch: the forces of the state q after
 // stage force_stage (-1: none), the ghost mirror of q for stage mirror_stage
 // (-1: none) and, with setup, the per-step set-up before the mirror.
 int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, const uint8_t* mask, DevState* st,
-               int force_stage, int mirror_stage, int setup, void* stream);
+               int force_stage, int mirror_stage, int setup, bool pdl, void* stream);
 int launch_pack(const Geometry& g, const double* host_like, int64_t si, int64_t sj, int64_t sv, double* q,
                  int to_device, void* stream);
 int launch_init_vortex(const Geometry& g, const efvm_vortex& v, double* q, void* stream);

@@ -31,6 +31,16 @@ __device__ __forceinline__ long long cidx(const Geometry& g, int i, int j) {
     return (long long)(YO + j) * g.pitch + (XO + i);
 }
 
+// Programmatic dependent launch.  The kernels of a step are launched with
+// programmatic stream serialization, so a kernel's blocks may be scheduled while
+// its predecessor is still draining.  Each such kernel waits for the predecessor
+// to complete (and its writes to become visible) before it reads anything, then
+// lets its own successor launch.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait_then_release() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Cell centre lo + (i + 0.5) h with one rounding per operation, as the host
 // computes it (no FMA), so geometry tests agree bit for bit.
 __device__ __forceinline__ double centre(double lo, double h, int i) {
@@ -262,6 +272,7 @@ constexpr int WPB = 4;     // warps per block
 // ---------------------------------------------------------------------------
 template <int SCHEME, int RECON, class R, int MINB>
 __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
+    pdl_wait_then_release();
     if (!a.st->active) return;
     const Geometry& g = a.g;
     const Physics& ph = a.ph;
@@ -540,6 +551,7 @@ __device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
 }
 
 __global__ void step_setup_kernel(Physics ph, DevState* st) {
+    pdl_wait_then_release();
     if (!st->active) return;
     step_setup(ph, st);
 }
@@ -810,6 +822,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) ibm_kernel(Geometry g, Physics 
                                                             const uint8_t* __restrict__ mask, DevState* st,
                                                             int force_stage, int n_force_blocks, int mirror_stage,
                                                             int setup) {
+    pdl_wait_then_release();
     if (!st->active) return;
     const int b = blockIdx.x;
     if (b < n_force_blocks) {  // uniform per block
@@ -947,6 +960,23 @@ __global__ void check_state_kernel(Geometry g, Physics ph, const double* __restr
 // ---------------------------------------------------------------------------
 // Host launch wrappers
 // ---------------------------------------------------------------------------
+// Launch with programmatic stream serialization when `pdl` is set (the kernel
+// must begin with pdl_wait_then_release).
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, bool pdl, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 static int grid_for(long long n, int block) {
     long long b = (n + block - 1) / block;
     if (b < 1) b = 1;
@@ -969,7 +999,7 @@ static int rows_per_warp(int nx, int ny, int blocks_per_sm) {
 }
 
 template <int SCHEME, int RECON, class R>
-static void launch_stage_t(const StageArgs& a, cudaStream_t s) {
+static void launch_stage_t(const StageArgs& a, bool pdl, cudaStream_t s) {
     // Resident blocks per SM, measured at 4096^2: the FP64 flux is fastest at 96
     // registers/thread (5 blocks of 4 warps), the FP32 flux at 64 (8 blocks).
     constexpr int MINB = sizeof(R) == sizeof(double) ? 5 : 8;
@@ -977,31 +1007,31 @@ static void launch_stage_t(const StageArgs& a, cudaStream_t s) {
     const int strips = (a.g.nx + STRIP - 1) / STRIP;
     dim3 block(32 * WPB);
     dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
-    stage_kernel<SCHEME, RECON, R, MINB><<<grid, block, 0, s>>>(a, rows);
+    launch_k(stage_kernel<SCHEME, RECON, R, MINB>, grid, block, s, pdl, a, rows);
 }
 
 template <class R>
-static void launch_stage_r(const StageArgs& a, cudaStream_t s) {
+static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
     const bool muscl = a.ph.reconstruction == EFVM_RECON_MUSCL;
     switch (a.ph.flux_scheme) {
         case EFVM_FLUX_RUSANOV:
-            muscl ? launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R>(a, s)
-                  : launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R>(a, s);
+            muscl ? launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R>(a, pdl, s)
+                  : launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
             break;
         case EFVM_FLUX_HLLC_TEXTBOOK:
-            muscl ? launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R>(a, s)
-                  : launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R>(a, s);
+            muscl ? launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R>(a, pdl, s)
+                  : launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
             break;
         default:
-            muscl ? launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R>(a, s)
-                  : launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R>(a, s);
+            muscl ? launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R>(a, pdl, s)
+                  : launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
     }
 }
 
-int launch_stage(const StageArgs& a, int, int, void* stream) {
+int launch_stage(const StageArgs& a, bool pdl, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_r<float>(a, s);
-    else launch_stage_r<double>(a, s);
+    if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_r<float>(a, pdl, s);
+    else launch_stage_r<double>(a, pdl, s);
     return 1;
 }
 
@@ -1019,8 +1049,8 @@ int launch_cfl(const Geometry& g, const Physics& ph, const double* q, DevState* 
     return 2;
 }
 
-int launch_step_setup(const Physics& ph, DevState* st, void* stream) {
-    step_setup_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(ph, st);
+int launch_step_setup(const Physics& ph, DevState* st, bool pdl, void* stream) {
+    launch_k(step_setup_kernel, dim3(1), dim3(1), (cudaStream_t)stream, pdl, ph, st);
     return 1;
 }
 
@@ -1047,13 +1077,13 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
 }
 
 int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, const uint8_t* mask, DevState* st,
-               int force_stage, int mirror_stage, int setup, void* stream) {
+               int force_stage, int mirror_stage, int setup, bool pdl, void* stream) {
     const int nf = force_stage >= 0 ? 1 + (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS : 0;
     int nm = mirror_stage >= 0 ? (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS : 0;
     if (setup && nm < 1) nm = 1;
     if (nf + nm == 0) return 0;
-    ibm_kernel<<<nf + nm, FORCE_THREADS, 0, (cudaStream_t)stream>>>(g, ph, ib, q, mask, st, force_stage, nf,
-                                                                     mirror_stage, setup);
+    launch_k(ibm_kernel, dim3(nf + nm), dim3(FORCE_THREADS), (cudaStream_t)stream, pdl, g, ph, ib, q, mask, st,
+             force_stage, nf, mirror_stage, setup);
     return 1;
 }
 
