@@ -137,6 +137,16 @@ int build_ibm_lists(efvm_ctx* c) {
                                   cudaMemcpyDeviceToHost, S(c)));
     CUDA_TRY(c, cudaStreamSynchronize(S(c)));
     const int ncyl = (int)(c->cyl_host.size() / 3);
+    // the mask is zero outside the interior
+    auto solid = [&](int i, int j) {
+        return i >= 0 && i < g.nx && j >= 0 && j < g.ny && m[(size_t)j * g.nx + i] != 0;
+    };
+    auto corner_bits = [&](int lo_i, int lo_j) {
+        unsigned b = 0;
+        for (int k = 0; k < 4; ++k)
+            if (!solid(lo_i + (k >> 1), lo_j + (k & 1))) b |= 1u << (FLUID_CORNER_SHIFT + k);
+        return b;
+    };
     std::vector<IbmGhostDev> ghosts;
     c->n_solid = 0;
     for (int j = 0; j < g.ny; ++j)
@@ -163,8 +173,13 @@ int build_ibm_lists(efvm_ctx* c) {
             const double push = 2.0 * (-best_signed);
             const double ip[2] = {cc[0] + push * nrm[0], cc[1] + push * nrm[1]};
             IbmGhostDev gh{};
-            gh.cell = (long long)j * g.nx + i;
+            gh.i = i;
+            gh.j = j;
             gh.valid = locate_h(g, ip[0], ip[1], gh.lo_i, gh.lo_j, gh.tx, gh.ty) ? 1 : 0;
+            const int nbi[4] = {i + 1, i - 1, i, i}, nbj[4] = {j, j, j + 1, j - 1};
+            for (int k = 0; k < 4; ++k)
+                if (!solid(nbi[k], nbj[k])) gh.fluid |= 1u << (FLUID_NB_SHIFT + k);
+            if (gh.valid) gh.fluid |= corner_bits(gh.lo_i, gh.lo_j);
             ghosts.push_back(gh);
         }
     // compute_cylinder_markers, crates/cfd_ibm/src/lib.rs:566-598 (n_theta = 64, n_z = 1)
@@ -189,6 +204,7 @@ int build_ibm_lists(efvm_ctx* c) {
             const double px = cx + r * nx, py = cy + r * ny;
             const double sx = px + offset * nx, sy = py + offset * ny;
             mk.valid = locate_h(g, sx, sy, mk.lo_i, mk.lo_j, mk.tx, mk.ty) ? 1 : 0;
+            if (mk.valid) mk.fluid = corner_bits(mk.lo_i, mk.lo_j);
             markers.push_back(mk);
         }
     }
@@ -204,7 +220,7 @@ int build_ibm_lists(efvm_ctx* c) {
     CUDA_TRY(c, cudaMalloc(&c->markers_dev, nm * sizeof(MarkerDev)));
     if (c->force_partials) cudaFree(c->force_partials);
     c->force_partials = nullptr;
-    const size_t nblocks = 1 + (ghosts.size() + 255) / 256;
+    const size_t nblocks = 1 + (ghosts.size() + IBM_THREADS - 1) / IBM_THREADS;
     CUDA_TRY(c, cudaMalloc(&c->force_partials, nblocks * 6 * sizeof(double)));
     CUDA_TRY(c, cudaMalloc(&c->zg0, ng * 4 * sizeof(double)));
     CUDA_TRY(c, cudaMalloc(&c->zfill, 3 * ng * 4 * sizeof(double)));
@@ -275,22 +291,22 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
 // Launch the kernels of one substage at RK stage `stage` (0..2, or 3 = Euler):
 // [step set-up +] IBM mirror of uin, the stage, the IBM forces of uout.
 void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool with_setup) {
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uin, c->mask, c->st, -1, stage, with_setup, true, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uin, c->st, -1, stage, with_setup, true, S(c));
     else if (with_setup) c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     enqueue_stage_kernel(c, stage, uin, uout);
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uout, c->mask, c->st, stage, -1, 0, true, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uout, c->st, stage, -1, 0, true, S(c));
 }
 
 // One whole SSP-RK3 step.  With IBM the forces of a stage and the mirror of the
 // next run in one launch (7 launches a step instead of 10).
 void enqueue_rk3_step(efvm_ctx* c) {
     double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->mask, c->st, -1, 0, 1, true, S(c));
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->st, -1, 0, 1, true, S(c));
     else c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     for (int s = 0; s < 3; ++s) {
         enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1]);
         if (c->ibm)
-            c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->mask, c->st, s, s < 2 ? s + 1 : -1, 0,
+            c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, s, s < 2 ? s + 1 : -1, 0,
                                       true, S(c));
     }
 }
@@ -825,11 +841,11 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
         CUDA_TRY(c, cudaEventRecord(ev[1], S(c)));
         float ms_stage = 0.f, ms_ibm = 0.f;
         for (int s = 0; s < 3; ++s) {
-            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s], c->mask, c->st, -1, s, 0, false, S(c));
+            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s], c->st, -1, s, 0, false, S(c));
             CUDA_TRY(c, cudaEventRecord(ev[2], S(c)));
             enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1], false);
             CUDA_TRY(c, cudaEventRecord(ev[3], S(c)));
-            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->mask, c->st, s, -1, 0, false, S(c));
+            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->st, s, -1, 0, false, S(c));
             CUDA_TRY(c, cudaEventRecord(ev[4], S(c)));
             CUDA_TRY(c, cudaEventSynchronize(ev[4]));
             float t_stage = 0.f, t_after = 0.f;

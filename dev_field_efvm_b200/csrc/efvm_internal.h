@@ -74,13 +74,20 @@ struct Physics {
     double cfl_visc_sum;  // 1/dx^2 + 1/dy^2 + 1/dz^2
 };
 
+// Bits of IbmGhostDev::fluid / MarkerDev::fluid.  The solid mask changes only
+// with the geometry, so which neighbours and bilinear corners are fluid is
+// fixed when the lists are built.
+constexpr unsigned FLUID_NB_SHIFT = 0;      // +x, -x, +y, -y face neighbour (ghosts only)
+constexpr unsigned FLUID_CORNER_SHIFT = 4;  // bilinear corner k = 2*di + dj
+constexpr int IBM_THREADS = 128;            // threads per block of the IBM kernel
+
 // One solid cell that the IBM mirror refills every substage (IbmGhostCells).
 struct IbmGhostDev {
-    long long cell;          // interior linear index j*nx + i
+    int i, j;                // interior cell
     int lo_i, lo_j;          // low corner of the bilinear block (interior indices, may be -1 / n)
     double tx, ty;           // bilinear fractions
     int valid;               // locate() succeeded
-    int pad;
+    unsigned fluid;          // FLUID_* bits
 };
 
 // One surface marker (IbmMarker) with its sample point already located.
@@ -91,7 +98,7 @@ struct MarkerDev {
     int lo_i, lo_j;
     double tx, ty;
     int valid;
-    int pad;
+    unsigned fluid;          // FLUID_CORNER bits
 };
 
 struct Ibm {
@@ -143,7 +150,7 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
 // IBM work between stage kernels, one launch: the forces of the state q after
 // stage force_stage (-1: none), the ghost mirror of q for stage mirror_stage
 // (-1: none) and, with setup, the per-step set-up before the mirror.
-int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, const uint8_t* mask, DevState* st,
+int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, DevState* st,
                int force_stage, int mirror_stage, int setup, bool pdl, void* stream);
 int launch_pack(const Geometry& g, const double* host_like, int64_t si, int64_t sj, int64_t sv, double* q,
                  int to_device, void* stream);

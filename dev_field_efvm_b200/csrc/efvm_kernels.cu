@@ -631,33 +631,36 @@ __global__ void geometry_kernel(Geometry g, const double* __restrict__ cyl, int 
 
 // sample_trilinear restricted to the z = centre plane (the z weight is exactly
 // 1 on the cell layer and 0 on the ghost layers), crates/cfd_ibm/src/lib.rs:106-149.
+// Solid corners (clear FLUID_CORNER bits) are skipped.  The four corner states
+// are loaded before any of them is used so that the loads overlap.
 __device__ __forceinline__ bool sample_bilinear(const Geometry& g, const Physics& ph, const double* q,
-                                                const uint8_t* mask, int lo_i, int lo_j, double tx, double ty,
+                                                unsigned fluid, int lo_i, int lo_j, double tx, double ty,
                                                 double out[5]) {
     const double gm1 = ph.gamma - 1.0;
+    U4 cu[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cu[k] = load4(q, g.plane, cidx(g, lo_i + (k >> 1), lo_j + (k & 1)));
     double acc[5] = {0, 0, 0, 0, 0};  // rho, u, v, p, t
     double total = 0.0;
-    for (int di = 0; di < 2; ++di) {
-        const double wx = di == 0 ? 1.0 - tx : tx;
-        for (int dj = 0; dj < 2; ++dj) {
-            const double wy = dj == 0 ? 1.0 - ty : ty;
-            const long long o = cidx(g, lo_i + di, lo_j + dj);
-            if (mask[o]) continue;
-            const U4 u = load4(q, g.plane, o);
-            if (!isfinite(u.r) || u.r <= 0.0) continue;
-            const double w = wx * wy;
-            const double inv = 1.0 / u.r;
-            const double vu = u.mx * inv, vv = u.my * inv;
-            const double ke = 0.5 * u.r * (vu * vu + vv * vv);
-            const double p = gm1 * (u.E - ke);
-            const double t = p * inv / ph.r_gas;
-            acc[0] += w * u.r;
-            acc[1] += w * vu;
-            acc[2] += w * vv;
-            acc[3] += w * p;
-            acc[4] += w * t;
-            total += w;
-        }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {  // (di, dj) = (0,0), (0,1), (1,0), (1,1)
+        const double wx = (k >> 1) == 0 ? 1.0 - tx : tx;
+        const double wy = (k & 1) == 0 ? 1.0 - ty : ty;
+        const U4 u = cu[k];
+        if (!((fluid >> (FLUID_CORNER_SHIFT + k)) & 1u)) continue;
+        if (!isfinite(u.r) || u.r <= 0.0) continue;
+        const double w = wx * wy;
+        const double inv = 1.0 / u.r;
+        const double vu = u.mx * inv, vv = u.my * inv;
+        const double ke = 0.5 * u.r * (vu * vu + vv * vv);
+        const double p = gm1 * (u.E - ke);
+        const double t = p * inv / ph.r_gas;
+        acc[0] += w * u.r;
+        acc[1] += w * vu;
+        acc[2] += w * vv;
+        acc[3] += w * p;
+        acc[4] += w * t;
+        total += w;
     }
     if (total < 1e-12) return false;
     const double inv = 1.0 / total;
@@ -669,20 +672,19 @@ __device__ __forceinline__ bool sample_bilinear(const Geometry& g, const Physics
 // ghost cell, recording its pre-mirror value for the emulated z-ghost of the
 // staircase wall force.  One thread per ghost cell.
 __device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& ph, const Ibm& ib, double* q,
-                                             const uint8_t* __restrict__ mask, int stage, int k) {
+                                             int stage, int k) {
     const IbmGhostDev gh = ib.ghosts[k];
-    const int j = (int)(gh.cell / g.nx), i = (int)(gh.cell - (long long)j * g.nx);
-    const long long o = cidx(g, i, j);
+    const long long o = cidx(g, gh.i, gh.j);
     const U4 pre = load4(q, g.plane, o);
+    double img[5];
+    const bool ok = gh.valid && sample_bilinear(g, ph, q, gh.fluid, gh.lo_i, gh.lo_j, gh.tx, gh.ty, img);
     double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
     zf[0] = pre.r; zf[1] = pre.mx; zf[2] = pre.my; zf[3] = pre.E;
     if (stage == 0 || stage == 3) {
         double* z0 = ib.zg0 + 4LL * k;
         z0[0] = pre.r; z0[1] = pre.mx; z0[2] = pre.my; z0[3] = pre.E;
     }
-    if (!gh.valid) return;
-    double img[5];
-    if (!sample_bilinear(g, ph, q, mask, gh.lo_i, gh.lo_j, gh.tx, gh.ty, img)) return;
+    if (!ok) return;
     // u_ghost = 2 u_wall - u_image with u_wall = 0; rho, p, T from the image
     const U4 m = prim_to_cons(img[0], 2.0 * 0.0 - img[1], 2.0 * 0.0 - img[2], img[3], ph.gamma - 1.0);
     store4(q, g.plane, o, m);
@@ -690,18 +692,16 @@ __device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& p
 
 // Output phase: MarkerForce (compute_marker_loadings, crates/cfd_ibm/src/
 // lib.rs:442-480) in block 0 and WallForce (compute_wall_forces, :309-362) over
-// blocks 1..: each block reduces its share in a fixed order and writes 6
-// partial sums; the last block to finish adds the partials in block order
-// (deterministic), publishes both forces and appends the marker force to the
-// substage history.
-constexpr int FORCE_THREADS = 256;
-
+// blocks 1..: each block reduces its share in a fixed order (warp shuffle
+// trees, then the warps in order) and writes 6 partial sums; the last block to
+// finish adds the wall partials in a fixed order (deterministic), publishes
+// both forces and appends the marker force to the substage history.
 __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& ph, const Ibm& ib,
-                                             const double* __restrict__ q, const uint8_t* __restrict__ mask,
-                                             DevState* st, int stage, int blk, int nblk) {
-    __shared__ double red[6][FORCE_THREADS];
+                                             const double* __restrict__ q, DevState* st, int stage, int blk,
+                                             int nblk) {
+    __shared__ double red[IBM_THREADS / 32][6];
     __shared__ bool last;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const double gm1 = ph.gamma - 1.0;
     double f[6] = {0, 0, 0, 0, 0, 0};
     if (blk == 0) {
@@ -709,7 +709,7 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
             const MarkerDev mk = ib.markers[m];
             if (!mk.valid) continue;
             double img[5];
-            if (!sample_bilinear(g, ph, q, mask, mk.lo_i, mk.lo_j, mk.tx, mk.ty, img)) continue;
+            if (!sample_bilinear(g, ph, q, mk.fluid, mk.lo_i, mk.lo_j, mk.tx, mk.ty, img)) continue;
             if (!(isfinite(img[3]) && isfinite(img[4]) && isfinite(img[1]) && isfinite(img[2]))) continue;
             const double usd[3] = {img[1] - mk.wall_velocity[0], img[2] - mk.wall_velocity[1], 0.0 - mk.wall_velocity[2]};
             const double udotn = usd[0] * mk.normal[0] + usd[1] * mk.normal[1] + usd[2] * mk.normal[2];
@@ -724,41 +724,38 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
     } else {
         const int k = (blk - 1) * blockDim.x + tid;
         if (k < ib.n_ghost) {
+            const IbmGhostDev gh = ib.ghosts[k];
+            const int i = gh.i, j = gh.j;
             const double dx = g.h[0], dy = g.h[1], dz = g.h[2];
             const double face_area[3] = {dy * dz, dx * dz, dx * dy};
             const double dn[3] = {dx, dy, dz};
             const double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
             const double* z0 = ib.zg0 + 4LL * k;
-            const long long cell = ib.ghosts[k].cell;
-            const int j = (int)(cell / g.nx), i = (int)(cell - (long long)j * g.nx);
-            // the six face neighbours of compute_wall_forces: +x, -x, +y, -y, then the
-            // two z-ghost layers of the 2-D mesh (never solid; their state is the
-            // slip-wall copy of this cell, RK-advanced with a zero rhs)
+            // all neighbour states first (in bounds: the ring of boundary ghosts)
+            U4 nbu[6];
+            nbu[0] = load4(q, g.plane, cidx(g, i + 1, j));
+            nbu[1] = load4(q, g.plane, cidx(g, i - 1, j));
+            nbu[2] = load4(q, g.plane, cidx(g, i, j + 1));
+            nbu[3] = load4(q, g.plane, cidx(g, i, j - 1));
+            {
+                // the two z-ghost layers of the 2-D mesh (never solid; their state is
+                // the slip-wall copy of this cell, RK-advanced with a zero rhs)
+                double zv[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (stage == 1) zv[c] = 0.75 * z0[c] + 0.25 * (zf[c] + 0.0);
+                    else if (stage == 2) zv[c] = (1.0 / 3.0) * z0[c] + (2.0 / 3.0) * (zf[c] + 0.0);
+                    else zv[c] = zf[c] + 0.0;
+                }
+                nbu[4] = nbu[5] = U4{zv[0], zv[1], zv[2], zv[3]};
+            }
+            // the six face neighbours of compute_wall_forces: +x, -x, +y, -y, +z, -z
 #pragma unroll
             for (int nb = 0; nb < 6; ++nb) {
-                U4 u;
-                int dim;
-                double sign;
-                if (nb < 4) {
-                    const int ni = i + (nb == 0 ? 1 : (nb == 1 ? -1 : 0));
-                    const int nj = j + (nb == 2 ? 1 : (nb == 3 ? -1 : 0));
-                    const long long o = cidx(g, ni, nj);
-                    if (mask[o]) continue;
-                    u = load4(q, g.plane, o);
-                    dim = nb < 2 ? 0 : 1;
-                    sign = (nb & 1) ? -1.0 : 1.0;
-                } else {
-                    double zv[4];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        if (stage == 1) zv[c] = 0.75 * z0[c] + 0.25 * (zf[c] + 0.0);
-                        else if (stage == 2) zv[c] = (1.0 / 3.0) * z0[c] + (2.0 / 3.0) * (zf[c] + 0.0);
-                        else zv[c] = zf[c] + 0.0;
-                    }
-                    u = U4{zv[0], zv[1], zv[2], zv[3]};
-                    dim = 2;
-                    sign = nb == 4 ? 1.0 : -1.0;
-                }
+                if (nb < 4 && !((gh.fluid >> (FLUID_NB_SHIFT + nb)) & 1u)) continue;
+                const U4 u = nbu[nb];
+                const int dim = nb >> 1;
+                const double sign = (nb & 1) ? -1.0 : 1.0;
                 const double p = pressure_d(u, gm1);
                 f[dim] -= p * sign * face_area[dim];
                 const double inv = 1.0 / u.r;
@@ -774,38 +771,46 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
         }
     }
 #pragma unroll
-    for (int d = 0; d < 6; ++d) red[d][tid] = f[d];
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (tid < s)
+    for (int d = 0; d < 6; ++d)
+        for (int o = 16; o > 0; o >>= 1) f[d] += __shfl_down_sync(0xffffffffu, f[d], o);
+    if (lane == 0)
 #pragma unroll
-            for (int d = 0; d < 6; ++d) red[d][tid] += red[d][tid + s];
-        __syncthreads();
-    }
+        for (int d = 0; d < 6; ++d) red[warp][d] = f[d];
+    __syncthreads();
     if (tid == 0) {
         double* part = ib.partials + 6LL * blk;
 #pragma unroll
-        for (int d = 0; d < 6; ++d) part[d] = red[d][0];
+        for (int d = 0; d < 6; ++d) {
+            double v = red[0][d];
+            for (int w = 1; w < IBM_THREADS / 32; ++w) v += red[w][d];
+            part[d] = v;
+        }
         __threadfence();
         const unsigned int done = atomicAdd(ib.counter, 1u);
-        last = done == nblk - 1;
+        last = done == (unsigned)nblk - 1;
     }
     __syncthreads();
-    if (last && tid == 0) {
+    if (last && warp == 0) {
         __threadfence();
         const volatile double* part = ib.partials;
         double wall[6] = {0, 0, 0, 0, 0, 0};
-        for (int b = 1; b < nblk; ++b)
+        for (int b = 1 + lane; b < nblk; b += 32)
+#pragma unroll
             for (int d = 0; d < 6; ++d) wall[d] += part[6 * b + d];
-        for (int d = 0; d < 6; ++d) {
-            ib.force_out[d] = part[d];
-            ib.force_out[6 + d] = wall[d];
+#pragma unroll
+        for (int d = 0; d < 6; ++d)
+            for (int o = 16; o > 0; o >>= 1) wall[d] += __shfl_down_sync(0xffffffffu, wall[d], o);
+        if (lane == 0) {
+            for (int d = 0; d < 6; ++d) {
+                ib.force_out[d] = part[d];
+                ib.force_out[6 + d] = wall[d];
+            }
+            if (ib.history && st->hist_pos < st->hist_cap) {
+                for (int d = 0; d < 6; ++d) ib.history[6 * st->hist_pos + d] = part[d];
+                st->hist_pos += 1;
+            }
+            *ib.counter = 0u;  // ready for the next launch
         }
-        if (ib.history && st->hist_pos < st->hist_cap) {
-            for (int d = 0; d < 6; ++d) ib.history[6 * st->hist_pos + d] = part[d];
-            st->hist_pos += 1;
-        }
-        *ib.counter = 0u;  // ready for the next launch
     }
 }
 
@@ -818,15 +823,14 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
 // `setup`, thread 0 of the first mirror block also does the per-step set-up,
 // and every mirror thread applies its stop rule itself, so a step that ends
 // there leaves the state untouched.
-__global__ void __launch_bounds__(FORCE_THREADS) ibm_kernel(Geometry g, Physics ph, Ibm ib, double* q,
-                                                            const uint8_t* __restrict__ mask, DevState* st,
-                                                            int force_stage, int n_force_blocks, int mirror_stage,
-                                                            int setup) {
+__global__ void __launch_bounds__(IBM_THREADS) ibm_kernel(Geometry g, Physics ph, Ibm ib, double* q, DevState* st,
+                                                          int force_stage, int n_force_blocks, int mirror_stage,
+                                                          int setup) {
     pdl_wait_then_release();
     if (!st->active) return;
     const int b = blockIdx.x;
     if (b < n_force_blocks) {  // uniform per block
-        forces_block(g, ph, ib, q, mask, st, force_stage, b, n_force_blocks);
+        forces_block(g, ph, ib, q, st, force_stage, b, n_force_blocks);
         return;
     }
     if (setup) {
@@ -834,7 +838,7 @@ __global__ void __launch_bounds__(FORCE_THREADS) ibm_kernel(Geometry g, Physics 
         if (step_stops(st)) return;
     }
     const int k = (b - n_force_blocks) * blockDim.x + threadIdx.x;
-    if (mirror_stage >= 0 && k < ib.n_ghost) mirror_ghost(g, ph, ib, q, mask, mirror_stage, k);
+    if (mirror_stage >= 0 && k < ib.n_ghost) mirror_ghost(g, ph, ib, q, mirror_stage, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -1076,14 +1080,14 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
     return 1;
 }
 
-int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, const uint8_t* mask, DevState* st,
+int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, DevState* st,
                int force_stage, int mirror_stage, int setup, bool pdl, void* stream) {
-    const int nf = force_stage >= 0 ? 1 + (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS : 0;
-    int nm = mirror_stage >= 0 ? (ib.n_ghost + FORCE_THREADS - 1) / FORCE_THREADS : 0;
+    const int nf = force_stage >= 0 ? 1 + (ib.n_ghost + IBM_THREADS - 1) / IBM_THREADS : 0;
+    int nm = mirror_stage >= 0 ? (ib.n_ghost + IBM_THREADS - 1) / IBM_THREADS : 0;
     if (setup && nm < 1) nm = 1;
     if (nf + nm == 0) return 0;
-    launch_k(ibm_kernel, dim3(nf + nm), dim3(FORCE_THREADS), (cudaStream_t)stream, pdl, g, ph, ib, q, mask, st,
-             force_stage, nf, mirror_stage, setup);
+    launch_k(ibm_kernel, dim3(nf + nm), dim3(IBM_THREADS), (cudaStream_t)stream, pdl, g, ph, ib, q, st, force_stage,
+             nf, mirror_stage, setup);
     return 1;
 }
 
