@@ -166,3 +166,20 @@ def poiseuille_case(ny=32, nx=3):
     params = abi.make_params(cfl=0.3, viscous=1, viscosity_model=abi.VISC_CONSTANT, mu=MU, body_force_x=GX)
     u = prim_to_cons(np.full((ny, nx), rho0), np.zeros((ny, nx)), 0.0, np.full((ny, nx), p0))
     return grid, params, u, {"H": H, "mu": MU, "gx": GX, "rho": rho0, "t_final": 0.081}
+
+
+def restart_pulse_case():
+    """The restart test's pulse (crates/cfd_solver/tests/restart.rs:17-55): a
+    density and pressure bump moving at 30 m/s through a 24-cell slip-walled box
+    of air, first-order HLLC (Thornber), SSP-RK3, CFL 0.4, so both the fields
+    and dt change every step."""
+    n = 24
+    bcs = {side: abi.BC_SLIP_WALL for side in (abi.XLO, abi.XHI, abi.YLO, abi.YHI, abi.ZLO, abi.ZHI)}
+    grid = abi.make_grid(n, 1, hi=(1.0, 0.05, 0.05), bcs=bcs)
+    params = abi.make_params(cfl=0.4)
+    x, _ = centroids(grid)
+    bump = np.exp(-(((x - 0.4) / 0.08) ** 2))
+    rho = 1.0 + 0.5 * bump
+    p = 1e5 * (1.0 + 0.8 * bump)
+    u = prim_to_cons(rho, np.full_like(rho, 30.0), 0.0, p)[None, :, :]
+    return grid, params, u, {"x": x}

@@ -62,14 +62,25 @@ __device__ __forceinline__ void store4(double* q, long long plane, long long o, 
     q[3 * plane + o] = u.E;
 }
 
+// The helpers below (pressure, prim_to_cons, the boundary ghosts, the wave
+// speed) are evaluated in more than one kernel on the same state: the stage
+// epilogue refills ghosts and takes the CFL maximum, and the stand-alone ghost
+// fill and CFL pass do the same after an upload.  A restart must see identical
+// values from both, so these round every operation explicitly (no FMA
+// contraction, whose choice may differ between inlined copies).
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a, b); }
+
+// IdealGas::pressure, crates/cfd_eos/src/lib.rs:61-64 (w = 0)
 __device__ __forceinline__ double pressure_d(const U4& u, double gm1) {
-    return gm1 * (u.E - 0.5 * (u.mx * u.mx + u.my * u.my) / u.r);
+    return mul_(gm1, sub_(u.E, mul_(0.5, add_(mul_(u.mx, u.mx), mul_(u.my, u.my))) / u.r));
 }
 
 // IdealGas::prim_to_cons (2-D, w = 0), crates/cfd_eos/src/lib.rs:55-59
 __device__ __forceinline__ U4 prim_to_cons(double rho, double u, double v, double p, double gm1) {
-    const double ke = 0.5 * rho * (u * u + v * v);
-    return U4{rho, rho * u, rho * v, p / gm1 + ke};
+    const double ke = mul_(mul_(0.5, rho), add_(mul_(u, u), mul_(v, v)));
+    return U4{rho, mul_(rho, u), mul_(rho, v), add_(p / gm1, ke)};
 }
 
 // Viscosity::mu, crates/cfd_eos/src/lib.rs:108-117 (Sutherland :75-80)
@@ -87,26 +98,26 @@ __device__ __forceinline__ U4 bc_ghost(const DevBC& bc, int side, const U4& in, 
         case EFVM_BC_SYMMETRY: {
             const double n0 = side < 2 ? (side == 1 ? 1.0 : -1.0) : 0.0;
             const double n1 = side >= 2 ? (side == 3 ? 1.0 : -1.0) : 0.0;
-            const double mn = in.mx * n0 + in.my * n1;
+            const double mn = add_(mul_(in.mx, n0), mul_(in.my, n1));
             U4 g = in;
-            g.mx = in.mx - 2.0 * mn * n0;
-            g.my = in.my - 2.0 * mn * n1;
+            g.mx = sub_(in.mx, mul_(mul_(2.0, mn), n0));
+            g.my = sub_(in.my, mul_(mul_(2.0, mn), n1));
             return g;
         }
         case EFVM_BC_NO_SLIP_WALL:
             return U4{in.r, -in.mx, -in.my, in.E};
         case EFVM_BC_SUPERSONIC_INFLOW: {
-            const double ke = 0.5 * bc.rho * (bc.u * bc.u + bc.v * bc.v + bc.w * bc.w);
-            return U4{bc.rho, bc.rho * bc.u, bc.rho * bc.v, bc.p / gm1 + ke};
+            const double ke = mul_(mul_(0.5, bc.rho), add_(add_(mul_(bc.u, bc.u), mul_(bc.v, bc.v)), mul_(bc.w, bc.w)));
+            return U4{bc.rho, mul_(bc.rho, bc.u), mul_(bc.rho, bc.v), add_(bc.p / gm1, ke)};
         }
         case EFVM_BC_SUBSONIC_INFLOW: {
             const double p_in = pressure_d(in, gm1);
-            const double ke = 0.5 * bc.rho * (bc.u * bc.u + bc.v * bc.v + bc.w * bc.w);
-            return U4{bc.rho, bc.rho * bc.u, bc.rho * bc.v, p_in / gm1 + ke};
+            const double ke = mul_(mul_(0.5, bc.rho), add_(add_(mul_(bc.u, bc.u), mul_(bc.v, bc.v)), mul_(bc.w, bc.w)));
+            return U4{bc.rho, mul_(bc.rho, bc.u), mul_(bc.rho, bc.v), add_(p_in / gm1, ke)};
         }
         case EFVM_BC_PRESSURE_OUTLET: {
             const double inv = 1.0 / in.r;
-            const double u = in.mx * inv, v = in.my * inv;
+            const double u = mul_(in.mx, inv), v = mul_(in.my, inv);
             return prim_to_cons(in.r, u, v, bc.p, gm1);
         }
         default:
@@ -131,7 +142,7 @@ __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& p
                 // parabolic_inflow_system, examples/cylinder_drag_validation/main.rs:151-177
                 const double y = centre(g.lo[1], g.h[1], j);
                 const double um = ph.inflow_u_max, hh = ph.inflow_height, rho = ph.inflow_rho;
-                const double uy = 4.0 * um * y * (hh - y) / (hh * hh);
+                const double uy = mul_(mul_(mul_(4.0, um), y), sub_(hh, y)) / mul_(hh, hh);
                 const double p_in = pressure_d(u, gm1);
                 const U4 c = prim_to_cons(rho, uy, 0.0, p_in, gm1);
                 store4(q, P, cidx(g, -1, j), c);
@@ -154,16 +165,16 @@ __device__ __forceinline__ double wave_speed(const Geometry& g, const Physics& p
     if (!(u.r > 0.0)) return 0.0;
     const double gm1 = ph.gamma - 1.0;
     const double inv = 1.0 / u.r;
-    const double vx = u.mx * inv, vy = u.my * inv;
+    const double vx = mul_(u.mx, inv), vy = mul_(u.my, inv);
     const double p = pressure_d(u, gm1);
-    const double a = sqrt(ph.gamma * p / u.r);
-    double lam = (fabs(vx) + a) / g.h[0] + (fabs(vy) + a) / g.h[1] + (0.0 + a) / g.h[2];
+    const double a = sqrt(mul_(ph.gamma, p) / u.r);
+    double lam = add_(add_(add_(fabs(vx), a) / g.h[0], add_(fabs(vy), a) / g.h[1]), add_(0.0, a) / g.h[2]);
     if (ph.viscous) {
-        const double ke = 0.5 * u.r * (vx * vx + vy * vy);
-        const double pp = gm1 * (u.E - ke);
-        const double t = pp * inv / ph.r_gas;
+        const double ke = mul_(mul_(0.5, u.r), add_(mul_(vx, vx), mul_(vy, vy)));
+        const double pp = mul_(gm1, sub_(u.E, ke));
+        const double t = mul_(pp, inv) / ph.r_gas;
         const double nu = viscosity(ph, t) / u.r;
-        lam += 2.0 * nu * ph.cfl_visc_sum;
+        lam = add_(lam, mul_(mul_(2.0, nu), ph.cfl_visc_sum));
     }
     return lam;
 }
@@ -590,7 +601,7 @@ __global__ void fill_ghosts_x_kernel(Geometry g, Physics ph, double* q) {
         if (ph.parabolic_inflow) {
             const double y = centre(g.lo[1], g.h[1], j);
             const double um = ph.inflow_u_max, hh = ph.inflow_height, rho = ph.inflow_rho;
-            const double uy = 4.0 * um * y * (hh - y) / (hh * hh);
+            const double uy = mul_(mul_(mul_(4.0, um), y), sub_(hh, y)) / mul_(hh, hh);
             const U4 c = prim_to_cons(rho, uy, 0.0, pressure_d(u0, gm1), gm1);
             store4(q, P, cidx(g, -1, j), c);
             store4(q, P, cidx(g, -2, j), c);

@@ -84,23 +84,27 @@ struct CflArgs {
 
 // Same wave speed as the context path's CFL (cfl_system's per-cell lambda with
 // the z term of the 2-D mesh and the optional viscous spectral radius).
+// Every operation is rounded explicitly (no FMA contraction), as in the
+// context path, so the two agree bit for bit.
 __device__ double cell_lambda(const CflArgs& a, double r, double mx, double my, double E) {
     if (!(r > 0.0)) return 0.0;
     const double gm1 = a.gamma - 1.0;
     const double inv = 1.0 / r;
-    const double vx = mx * inv, vy = my * inv;
-    const double p = gm1 * (E - 0.5 * (mx * mx + my * my) / r);
-    const double c = sqrt(a.gamma * p / r);
-    double lam = (fabs(vx) + c) / a.dx + (fabs(vy) + c) / a.dy + (0.0 + c) / a.dz;
+    const double vx = __dmul_rn(mx, inv), vy = __dmul_rn(my, inv);
+    const double m2 = __dadd_rn(__dmul_rn(mx, mx), __dmul_rn(my, my));
+    const double p = __dmul_rn(gm1, __dsub_rn(E, __dmul_rn(0.5, m2) / r));
+    const double c = sqrt(__dmul_rn(a.gamma, p) / r);
+    double lam = __dadd_rn(__dadd_rn(__dadd_rn(fabs(vx), c) / a.dx, __dadd_rn(fabs(vy), c) / a.dy),
+                           __dadd_rn(0.0, c) / a.dz);
     if (a.viscous) {
-        const double ke = 0.5 * r * (vx * vx + vy * vy);
-        const double t = gm1 * (E - ke) * inv / a.r_gas;
+        const double ke = __dmul_rn(__dmul_rn(0.5, r), __dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)));
+        const double t = __dmul_rn(__dmul_rn(gm1, __dsub_rn(E, ke)), inv) / a.r_gas;
         double mu = a.mu;
         if (a.visc_model == EFVM_VISC_SUTHERLAND) {
             const double MU_REF = 1.827e-5, T_REF = 291.15, S = 120.0;
             mu = MU_REF * pow(t / T_REF, 1.5) * (T_REF + S) / (t + S);
         }
-        lam += 2.0 * (mu / r) * a.visc_sum;
+        lam = __dadd_rn(lam, __dmul_rn(__dmul_rn(2.0, mu / r), a.visc_sum));
     }
     return lam;
 }

@@ -186,6 +186,14 @@ class Context:
         self._check(self.L.efvm_wall_force(self.h, _dp(out)))
         return out
 
+    def apply_geometry(self) -> None:
+        """Apply cylinders set since the last step to the current state now: the
+        solid mask, the stagnant re-seed of cells that turn solid and the IBM
+        lists (the Setup phase of the next substage would do the same).  A
+        restore calls it before loading its fields, so that they are not
+        re-seeded afterwards."""
+        self.ibm_counts()
+
     def ibm_counts(self):
         a, b = C.c_int64(), C.c_int64()
         self._check(self.L.efvm_ibm_counts(self.h, C.byref(a), C.byref(b)))

@@ -1184,6 +1184,19 @@ int oracle_set_cylinders(void* hp, const efvm_cylinder* c, int32_t n, const doub
     return EFVM_OK;
 }
 
+// The Setup-phase geometry systems alone (refresh_cylinder_mask,
+// compute_cylinder_ghosts, compute_cylinder_markers; crates/cfd_ibm/src/lib.rs:155-254,566-598),
+// as a freshly prepared App runs them before a restore overwrites its fields.
+int oracle_apply_geometry(void* hp) {
+    Case& cs = ((OracleHandle*)hp)->cs;
+    if (cs.ibm) {
+        cs.refresh_cylinder_mask();
+        cs.compute_cylinder_ghosts();
+        cs.compute_cylinder_markers();
+    }
+    return EFVM_OK;
+}
+
 int oracle_marker_force(void* hp, double out[6]) {
     Case& cs = ((OracleHandle*)hp)->cs;
     for (int d = 0; d < 6; ++d) out[d] = cs.marker_force[d];

@@ -60,6 +60,7 @@ def lib(parallel: bool = False) -> C.CDLL:
     L.oracle_marker_force.argtypes = [vp, dp]
     L.oracle_wall_force.argtypes = [vp, dp]
     L.oracle_ibm_counts.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
+    L.oracle_apply_geometry.argtypes = [vp]
     L.oracle_get_mask.argtypes = [vp, C.POINTER(C.c_uint8)]
     L.oracle_flux.argtypes = [C.c_int, C.c_double, C.c_double, dp, dp, C.c_int, dp]
     L.oracle_flux_normal.argtypes = [C.c_int, C.c_double, C.c_double, dp, dp, dp, dp]
@@ -177,6 +178,9 @@ class OracleCase:
         out = np.zeros(6)
         self.L.oracle_wall_force(self.h, _dp(out))
         return out
+
+    def apply_geometry(self) -> None:
+        self.L.oracle_apply_geometry(self.h)
 
     def ibm_counts(self):
         a, b = C.c_int64(), C.c_int64()

@@ -1,0 +1,63 @@
+"""The benchmark configurations run to their full horizons on the GPU.
+
+* Small periodic vortex: 128^2, MUSCL-minmod + HLLC (Thornber) + SSP-RK3,
+  CFL 0.4, to t >= 10.  Step count and density L1 against the oracle's own run
+  of the same case (tests/golden/oracle_pins.json, from oracle/pin_vortex128.py).
+* Cylinder at D/dx = 50: 1100x205, MUSCL, viscous (Re 20), Mach 0.1, run to the
+  plateau (t = 6.3, 12.6 D/U_mean, about 5e4 steps).  The drag coefficient over
+  the last 10 % of substages must meet the reference's own gate: within 5 % of
+  the DFG 2D-1 value 5.5795 with a peak-to-peak spread of at most 2 %
+  (examples/cylinder_drag_validation/main.rs:318-415).  The oracle would need
+  hours for this horizon; its per-cell parity with the GPU on the same case is
+  covered over a few steps in test_gpu_parity.py.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from dev_field_efvm_b200 import cases
+from dev_field_efvm_b200.device import Context
+
+pytestmark = pytest.mark.gpu
+
+PINS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "oracle_pins.json")))
+DFG_CD = 5.5795
+
+
+def test_vortex128_periodic_to_t10_matches_oracle_run():
+    pin = PINS["vortex128_periodic_muscl_minmod_t10"]
+    grid, params, u, ex = cases.vortex_case(128, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4)
+    d = Context(grid, params)
+    d.upload(u)
+    d.run_until(pin["t_final"])
+    s = d.solver_state()
+    assert s.step == pin["steps"]
+    # 2082 steps whose dt differ from the oracle's by ulps (FMA contraction in the
+    # kernels): the clock agrees to 1e-10 and the error norms to 1e-8 relative
+    assert abs(s.time - pin["time"]) <= 1e-10 * pin["time"]
+    l1, linf = d.density_error(ex["vortex"])
+    print(f"vortex128 t={s.time:.6f} steps={s.step} L1={l1:.6e} Linf={linf:.6e} (oracle L1 {pin['l1']:.6e})")
+    assert abs(l1 - pin["l1"]) <= 1e-8 * pin["l1"]
+    assert abs(linf - pin["linf"]) <= 1e-8 * pin["linf"]
+
+
+def test_cylinder_1100x205_plateau_drag_meets_reference_gate():
+    grid, params, u, ex = cases.cylinder_baseline_case()
+    d = Context(grid, params)
+    d.set_cylinders(ex["cylinders"], ex["freestream"])
+    d.upload(u)
+    t_final = 6.3
+    info, hist = d.step(200_000, t_stop=t_final, history=True)
+    assert info.stopped_at_t_stop
+    cd = (hist[:, 0] + hist[:, 3]) / ex["q"]
+    tail = cd[int(0.9 * len(cd)):]
+    mean = float(tail.mean())
+    ptp = float((tail.max() - tail.min()) / abs(mean))
+    print(f"cylinder 1100x205 t={info.time:.4f} steps={info.steps_done} Cd={mean:.5f} ptp={ptp:.2e} "
+          f"dev from DFG={abs(mean - DFG_CD) / DFG_CD:.3%}")
+    assert abs(mean - DFG_CD) / DFG_CD <= 0.05
+    assert ptp <= 0.02
