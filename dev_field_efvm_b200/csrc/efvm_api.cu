@@ -338,6 +338,7 @@ int read_state(efvm_ctx* c, DevState& s) {
 }
 
 bool bc_supported(int k) { return k >= EFVM_BC_SUPERSONIC_OUTFLOW && k <= EFVM_BC_PRESSURE_OUTLET; }
+bool has_halo(const efvm_ctx* c) { return c->ph.halo_ylo || c->ph.halo_yhi; }
 
 }  // namespace
 
@@ -354,7 +355,11 @@ const char* efvm_last_error(const efvm_ctx* ctx) {
     return g_last_error.c_str();
 }
 
-int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out) {
+// efvm_create / efvm_create_slab: a context for global rows [row0, row0 + rows)
+// of `grid`; `slab` marks the y sides that face another slab or the periodic
+// wrap as halo sides.
+static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t row0, int32_t rows, bool slab,
+                       efvm_ctx** out) {
     if (!grid || !params || !out) return fail(nullptr, EFVM_ERR_INVALID_ARG, "null argument");
     *out = nullptr;
     const efvm_grid& gr = *grid;
@@ -385,6 +390,8 @@ int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out
         return fail(nullptr, EFVM_ERR_INVALID_ARG, "enum field out of range");
     if (p.sponge && !(p.sponge_x_end > p.sponge_x_start))
         return fail(nullptr, EFVM_ERR_INVALID_ARG, "sponge_x_end must exceed sponge_x_start");
+    if (slab && (row0 < 0 || rows < 2 || (int64_t)row0 + rows > gr.ny))
+        return fail(nullptr, EFVM_ERR_INVALID_ARG, "a slab needs rows >= 2 inside the grid: 0 <= row0, row0 + rows <= ny");
 
     efvm_ctx* c = new efvm_ctx();
     c->grid = gr;
@@ -392,7 +399,8 @@ int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out
     cudaGetDevice(&c->device);
     Geometry& g = c->g;
     g.nx = gr.nx;
-    g.ny = gr.ny;
+    g.ny = rows;
+    g.j_off = row0;
     g.pitch = ((XO + gr.nx + NG) + 7) / 8 * 8;
     g.plane = ((long long)(gr.ny + 2 * YO) * g.pitch + 31) / 32 * 32;
     const int n[3] = {gr.nx, gr.ny, gr.nz};
@@ -420,6 +428,15 @@ int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out
     ph.periodic_seam = p.periodic_seam;
     ph.periodic_x = gr.bc[EFVM_XLO].kind == EFVM_BC_PERIODIC;
     ph.periodic_y = gr.bc[EFVM_YLO].kind == EFVM_BC_PERIODIC;
+    if (slab) {
+        // the periodic wrap of y, like the edges between slabs, goes through halos
+        const bool per_y = ph.periodic_y != 0;
+        ph.halo_ylo = row0 > 0 || per_y;
+        ph.halo_yhi = row0 + rows < gr.ny || per_y;
+        ph.seam_ylo = per_y && row0 == 0;
+        ph.seam_yhi = per_y && row0 + rows == gr.ny;
+        ph.periodic_y = 0;
+    }
     for (int s = 0; s < 4; ++s) {
         ph.bc[s].kind = gr.bc[s].kind;
         ph.bc[s].rho = gr.bc[s].rho;
@@ -472,8 +489,9 @@ int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out
     // crates/cfd_solver/src/lib.rs:484-493
     std::vector<double> yw(3 * (size_t)g.ny);
     for (int j = 0; j < g.ny; ++j) {
-        const double hm = centre_h(g.lo[1], g.h[1], j) - centre_h(g.lo[1], g.h[1], j - 1);
-        const double hp = centre_h(g.lo[1], g.h[1], j + 1) - centre_h(g.lo[1], g.h[1], j);
+        const int jg = j + g.j_off;
+        const double hm = centre_h(g.lo[1], g.h[1], jg) - centre_h(g.lo[1], g.h[1], jg - 1);
+        const double hp = centre_h(g.lo[1], g.h[1], jg + 1) - centre_h(g.lo[1], g.h[1], jg);
         yw[j] = 1.0 / hm;
         yw[g.ny + j] = 1.0 / hp;
         yw[2 * g.ny + j] = 2.0 / (hm + hp);
@@ -497,6 +515,15 @@ int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out
     if (e != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e)));
     *out = c;
     return EFVM_OK;
+}
+
+int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out) {
+    return create_impl(grid, params, 0, grid ? grid->ny : 0, false, out);
+}
+
+int efvm_create_slab(const efvm_grid* grid, const efvm_params* params, int32_t row0, int32_t rows,
+                     efvm_ctx** out) {
+    return create_impl(grid, params, row0, rows, true, out);
 }
 
 int efvm_destroy(efvm_ctx* c) {
@@ -596,6 +623,51 @@ int efvm_set_solver_state(efvm_ctx* c, const efvm_solver_state* in) {
     return EFVM_OK;
 }
 
+int efvm_prepare(efvm_ctx* c) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (c->control_dirty) sync_control(c, 0, 0.0, 0);
+    int rc = prologue(c);
+    if (rc) return rc;
+    CUDA_TRY(c, cudaGetLastError());
+    return EFVM_OK;
+}
+
+static int halo_rows(efvm_ctx* c, int32_t side, double* buf, int unpack) {
+    if (!c || !buf) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (side != EFVM_YLO && side != EFVM_YHI) return fail(c, EFVM_ERR_INVALID_ARG, "side must be EFVM_YLO or EFVM_YHI");
+    if (c->g.ny < 2) return fail(c, EFVM_ERR_INVALID_ARG, "halo rows need ny >= 2");
+    if (unpack && !(side == EFVM_YLO ? c->ph.halo_ylo : c->ph.halo_yhi))
+        return fail(c, EFVM_ERR_INVALID_ARG, "efvm_halo_unpack: that side does not face another slab");
+    int j0;
+    if (unpack) j0 = side == EFVM_YLO ? -2 : c->g.ny;
+    else j0 = side == EFVM_YLO ? 0 : c->g.ny - 2;
+    c->launches += launch_halo_rows(c->g, cur_buf(c), buf, j0, unpack, S(c));
+    CUDA_TRY(c, cudaGetLastError());
+    return EFVM_OK;
+}
+
+int efvm_halo_pack(efvm_ctx* c, int32_t side, double* dev_buf) { return halo_rows(c, side, dev_buf, 0); }
+
+int efvm_halo_unpack(efvm_ctx* c, int32_t side, const double* dev_buf) {
+    return halo_rows(c, side, const_cast<double*>(dev_buf), 1);
+}
+
+int efvm_wave_speed_slot(efvm_ctx* c, uint64_t** dev_slot) {
+    if (!c || !dev_slot) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    DevState s;
+    int rc = read_state(c, s);
+    if (rc) return rc;
+    if (!s.ext_lam) {
+        s.ext_lam = 1;
+        s.lam_ext = 0ull;
+        CUDA_TRY(c, cudaMemcpyAsync(c->st, &s, sizeof(DevState), cudaMemcpyHostToDevice, S(c)));
+        CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+        c->lam_stale = true;  // the next prologue measures the current state into the slot
+    }
+    *dev_slot = reinterpret_cast<uint64_t*>(&c->st->lam_ext);
+    return EFVM_OK;
+}
+
 int efvm_substep(efvm_ctx* c) {
     if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     if (c->control_dirty) sync_control(c, 0, 0.0, 0);
@@ -621,6 +693,8 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
               efvm_step_info* info) {
     if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     if (n_steps < 0) return fail(c, EFVM_ERR_INVALID_ARG, "n_steps must be >= 0");
+    if (has_halo(c))
+        return fail(c, EFVM_ERR_UNSUPPORTED, "a slab advances by efvm_substep with a halo exchange per stage");
     if (c->params.integrator != EFVM_INTEGRATOR_EULER && c->rk_stage != 0)
         return fail(c, EFVM_ERR_INVALID_ARG, "efvm_step must start at a step boundary (rk_stage == 0)");
     const bool async = !stop_at_t && !force_history && !info;
@@ -703,7 +777,7 @@ int efvm_cfl(efvm_ctx* c, double* dt_out) {
     int rc = read_state(c, s);
     if (rc) return rc;
     double lam;
-    std::memcpy(&lam, &s.lam[s.lam_idx], sizeof(double));
+    std::memcpy(&lam, s.ext_lam ? &s.lam_ext : &s.lam[s.lam_idx], sizeof(double));
     *dt_out = lam > 0.0 ? c->ph.cfl / lam : std::numeric_limits<double>::infinity();
     if (c->rk_stage == 0) c->lam_stale = false;
     else c->lam_stale = true;
@@ -717,6 +791,7 @@ int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const d
         c->graph_valid = false;
         return EFVM_OK;
     }
+    if (has_halo(c)) return fail(c, EFVM_ERR_UNSUPPORTED, "IBM cylinders are not supported on a slab");
     c->cyl_host.clear();
     for (int b = 0; b < n; ++b) {
         if (!(cyl[b].radius > 0.0)) return fail(c, EFVM_ERR_INVALID_ARG, "cylinder radius must be > 0");

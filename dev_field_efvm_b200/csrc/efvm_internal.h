@@ -36,6 +36,9 @@ struct DevState {
     double t_stop;
     long long hist_pos;      // next MarkerForce history slot
     long long hist_cap;
+    unsigned long long lam_ext;  // external wave-speed slot (slabs), see efvm_wave_speed_slot
+    int ext_lam;             // 1: accumulate into / read from lam_ext
+    int pad_;
 };
 
 // Boundary side description resolved for the device.
@@ -53,6 +56,8 @@ struct Geometry {
     double h[3];          // spacing dx, dy, dz
     double inv_x, inv_y;  // face area / cell volume for x and y faces
     double cell_volume;
+    int j_off;            // global index of row 0 (slabs; 0 otherwise)
+    int pad_;
 };
 
 struct Physics {
@@ -63,6 +68,10 @@ struct Physics {
     double mu;
     int precision, periodic_seam;
     int periodic_x, periodic_y;
+    // Slabs (efvm_create_slab): a y side whose ghosts come from a neighbouring
+    // slab, and whether that side is the global periodic seam.
+    int halo_ylo, halo_yhi;
+    int seam_ylo, seam_yhi;
     DevBC bc[4];  // XLO, XHI, YLO, YHI
     int parabolic_inflow;
     double inflow_u_max, inflow_height, inflow_rho;
@@ -159,6 +168,9 @@ int launch_density_error(const Geometry& g, const efvm_vortex& v, const double* 
                           double* partial, int nblocks, void* stream);
 int launch_total_mass(const Geometry& g, const double* q, double* partial, int nblocks, void* stream);
 int launch_check_state(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream);
+// Rows j0, j0+1 (all four variables, interior columns) to buf (unpack = 0) or
+// from buf (unpack = 1); buf is [variable][row][i], 8*nx doubles.
+int launch_halo_rows(const Geometry& g, double* q, double* buf, int j0, int unpack, void* stream);
 int launch_set_control(DevState* st, int active, int stop_at_t, double t_stop, long long hist_cap, void* stream);
 
 }  // namespace efvm

@@ -140,7 +140,7 @@ __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& p
             store4(q, P, cidx(g, -1, j), bc_ghost(ph.bc[0], 0, u, gm1));
             if (ph.parabolic_inflow) {
                 // parabolic_inflow_system, examples/cylinder_drag_validation/main.rs:151-177
-                const double y = centre(g.lo[1], g.h[1], j);
+                const double y = centre(g.lo[1], g.h[1], j + g.j_off);
                 const double um = ph.inflow_u_max, hh = ph.inflow_height, rho = ph.inflow_rho;
                 const double uy = mul_(mul_(mul_(4.0, um), y), sub_(hh, y)) / mul_(hh, hh);
                 const double p_in = pressure_d(u, gm1);
@@ -155,9 +155,16 @@ __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& p
         if (j >= g.ny - NG) store4(q, P, cidx(g, i, j - g.ny), u);
         if (j < NG) store4(q, P, cidx(g, i, j + g.ny), u);
     } else {
-        if (j == 0) store4(q, P, cidx(g, i, -1), bc_ghost(ph.bc[2], 2, u, gm1));
-        if (j == g.ny - 1) store4(q, P, cidx(g, i, g.ny), bc_ghost(ph.bc[3], 3, u, gm1));
+        // a side that faces another slab is filled by the caller's halo exchange
+        if (j == 0 && !ph.halo_ylo) store4(q, P, cidx(g, i, -1), bc_ghost(ph.bc[2], 2, u, gm1));
+        if (j == g.ny - 1 && !ph.halo_yhi) store4(q, P, cidx(g, i, g.ny), bc_ghost(ph.bc[3], 3, u, gm1));
     }
+}
+
+// The wave-speed accumulator of the current step: the context's own double
+// buffer, or the external slot that slabs max-reduce across GPUs.
+__device__ __forceinline__ unsigned long long* lam_slot(DevState* st) {
+    return st->ext_lam ? &st->lam_ext : &st->lam[st->lam_idx];
 }
 
 // Local max wave speed of cfl_system, crates/cfd_solver/src/lib.rs:647-669.
@@ -332,8 +339,9 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
             rec_l = MUSCL && ph.periodic_x;
             rec_r = MUSCL && ph.periodic_x && true_seam;
         }
-        const bool seam_rec = MUSCL && ph.periodic_y && true_seam;  // the side across the periodic seam
-        const bool edge_rec = MUSCL && ph.periodic_y;               // the side inside the domain
+        const bool y_periodic = ph.periodic_y || ph.seam_ylo || ph.seam_yhi;
+        const bool seam_rec = MUSCL && y_periodic && true_seam;  // the side across the periodic seam
+        const bool edge_rec = MUSCL && y_periodic;               // the side inside the domain
 
         // Row window of this lane's column: uc = U(j), un = U(j+1); pc = +y face
         // state of row j; gb = flux of the y-face below row j (face frame).  Each
@@ -356,7 +364,9 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
             if (MUSCL) {
                 V4<R> mn;
                 slope_faces(ph.limiter, uc, un, un2, pn, mn);
-                const bool lo_edge = j == -1, hi_edge = j + 1 == g.ny;
+                // faces on the domain's y edges; an edge between slabs is an interior face
+                const bool lo_edge = j == -1 && (!ph.halo_ylo || ph.seam_ylo);
+                const bool hi_edge = j + 1 == g.ny && (!ph.halo_yhi || ph.seam_yhi);
                 const bool rb = lo_edge ? seam_rec : (hi_edge ? edge_rec : true);
                 const bool rt = lo_edge ? edge_rec : (hi_edge ? seam_rec : true);
                 gt = face_flux<SCHEME, R>(yq(rb ? pc : uc), yq(rt ? mn : un), rg, rgm1);
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
                     // outlet_sponge_system, examples/cylinder_drag_validation/main.rs:186-229
                     const double cx = centre(g.lo[0], g.h[0], i);
                     if (cx >= ph.sponge_x_start) {
-                        const double cy = centre(g.lo[1], g.h[1], j);
+                        const double cy = centre(g.lo[1], g.h[1], j + g.j_off);
                         const double inv_w = 1.0 / (ph.sponge_x_end - ph.sponge_x_start);
                         const double s = fmin(fmax((cx - ph.sponge_x_start) * inv_w, 0.0), 1.0);
                         const double f = fmin(ph.sponge_sigma * s * s * dt, 1.0);
@@ -510,7 +520,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
     if (a.completes_step && a.want_cfl) {
         for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
         if (lane == 0 && lam > 0.0 && lam == lam)
-            atomicMax(&a.st->lam[a.st->lam_idx], (unsigned long long)__double_as_longlong(lam));
+            atomicMax(lam_slot(a.st), (unsigned long long)__double_as_longlong(lam));
     }
 }
 
@@ -525,11 +535,11 @@ __global__ void cfl_kernel(Geometry g, Physics ph, const double* __restrict__ q,
         const U4 u = load4(q, g.plane, cidx(g, i, j));
         lam = fmax(lam, wave_speed(g, ph, u));
     }
-    block_max_atomic(lam, &st->lam[st->lam_idx]);
+    block_max_atomic(lam, lam_slot(st));
 }
 
 __global__ void reset_lam_kernel(DevState* st) {
-    st->lam[st->lam_idx] = 0ull;
+    *lam_slot(st) = 0ull;
 }
 
 // Per-step Setup: dt from the wave-speed max (cfl_system's final lines,
@@ -552,10 +562,14 @@ __device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
     if (ph.fixed_dt > 0.0) {
         dt = ph.fixed_dt;
     } else {
-        const double lam = __longlong_as_double((long long)st->lam[st->lam_idx]);
+        const double lam = __longlong_as_double((long long)*lam_slot(st));
         dt = lam > 0.0 ? ph.cfl / lam : INFINITY;
     }
     st->dt = dt;
+    if (st->ext_lam) {  // the slot starts this step's accumulation from zero
+        st->lam_ext = 0ull;
+        return;
+    }
     const int nxt = st->lam_idx ^ 1;
     st->lam[nxt] = 0ull;
     st->lam_idx = nxt;
@@ -581,8 +595,9 @@ __global__ void fill_ghosts_y_kernel(Geometry g, Physics ph, double* q) {
             store4(q, P, cidx(g, i, g.ny + k), load4(q, P, cidx(g, i, k)));
         }
     } else {
-        store4(q, P, cidx(g, i, -1), bc_ghost(ph.bc[2], 2, load4(q, P, cidx(g, i, 0)), gm1));
-        store4(q, P, cidx(g, i, g.ny), bc_ghost(ph.bc[3], 3, load4(q, P, cidx(g, i, g.ny - 1)), gm1));
+        if (!ph.halo_ylo) store4(q, P, cidx(g, i, -1), bc_ghost(ph.bc[2], 2, load4(q, P, cidx(g, i, 0)), gm1));
+        if (!ph.halo_yhi)
+            store4(q, P, cidx(g, i, g.ny), bc_ghost(ph.bc[3], 3, load4(q, P, cidx(g, i, g.ny - 1)), gm1));
     }
 }
 __global__ void fill_ghosts_x_kernel(Geometry g, Physics ph, double* q) {
@@ -599,7 +614,7 @@ __global__ void fill_ghosts_x_kernel(Geometry g, Physics ph, double* q) {
         const U4 u0 = load4(q, P, cidx(g, 0, j));
         store4(q, P, cidx(g, -1, j), bc_ghost(ph.bc[0], 0, u0, gm1));
         if (ph.parabolic_inflow) {
-            const double y = centre(g.lo[1], g.h[1], j);
+            const double y = centre(g.lo[1], g.h[1], j + g.j_off);
             const double um = ph.inflow_u_max, hh = ph.inflow_height, rho = ph.inflow_rho;
             const double uy = mul_(mul_(mul_(4.0, um), y), sub_(hh, y)) / mul_(hh, hh);
             const U4 c = prim_to_cons(rho, uy, 0.0, pressure_d(u0, gm1), gm1);
@@ -621,7 +636,7 @@ __global__ void geometry_kernel(Geometry g, const double* __restrict__ cyl, int 
     const long long n = (long long)g.nx * g.ny;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
-        const double cx = centre(g.lo[0], g.h[0], i), cy = centre(g.lo[1], g.h[1], j);
+        const double cx = centre(g.lo[0], g.h[0], i), cy = centre(g.lo[1], g.h[1], j + g.j_off);
         bool inside = false;
         for (int b = 0; b < ncyl && !inside; ++b) {
             const double dx = __dsub_rn(cx, cyl[3 * b]), dy = __dsub_rn(cy, cyl[3 * b + 1]);
@@ -906,7 +921,7 @@ __global__ void init_vortex_kernel(Geometry g, efvm_vortex v, double* q) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
         U4 c;
-        vortex_rho(v, 0.0, centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j), &c);
+        vortex_rho(v, 0.0, centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j + g.j_off), &c);
         store4(q, g.plane, cidx(g, i, j), c);
     }
 }
@@ -920,7 +935,7 @@ __global__ void density_error_kernel(Geometry g, efvm_vortex v, const double* __
     const long long n = (long long)g.nx * g.ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(k / g.nx), i = (int)(k - (long long)j * g.nx);
-        const double ex = vortex_rho(v, t, centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j), nullptr);
+        const double ex = vortex_rho(v, t, centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j + g.j_off), nullptr);
         const double e = fabs(q[cidx(g, i, j)] - ex);
         a += e;
         m = fmax(m, e);
@@ -1066,6 +1081,24 @@ int launch_cfl(const Geometry& g, const Physics& ph, const double* q, DevState* 
 
 int launch_step_setup(const Physics& ph, DevState* st, bool pdl, void* stream) {
     launch_k(step_setup_kernel, dim3(1), dim3(1), (cudaStream_t)stream, pdl, ph, st);
+    return 1;
+}
+
+// Two rows of one y side to/from a contiguous buffer [variable][row][i].
+// unpack == 0: interior rows j0, j0+1 -> buf; unpack == 1: buf -> rows j0, j0+1.
+__global__ void halo_rows_kernel(Geometry g, double* q, double* buf, int j0, int unpack) {
+    const int n = 4 * 2 * g.nx;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int v = t / (2 * g.nx), r = (t / g.nx) % 2, i = t % g.nx;
+        const long long o = (long long)v * g.plane + cidx(g, i, j0 + r);
+        if (unpack) q[o] = buf[t];
+        else buf[t] = q[o];
+    }
+}
+
+int launch_halo_rows(const Geometry& g, double* q, double* buf, int j0, int unpack, void* stream) {
+    const int n = 4 * 2 * g.nx;
+    halo_rows_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(g, q, buf, j0, unpack);
     return 1;
 }
 

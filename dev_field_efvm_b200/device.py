@@ -23,7 +23,8 @@ EXPORTS = (
     "efvm_download_state", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
-    "efvm_profile_steps", "efvm_cfl_dt_noalloc",
+    "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
+    "efvm_wave_speed_slot", "efvm_cfl_dt_noalloc",
 )
 
 
@@ -66,6 +67,11 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_profile_steps.argtypes = [vp, i64, dp]
+    L.efvm_create_slab.argtypes = [C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), i32, i32, C.POINTER(vp)]
+    L.efvm_prepare.argtypes = [vp]
+    L.efvm_halo_pack.argtypes = [vp, i32, vp]
+    L.efvm_halo_unpack.argtypes = [vp, i32, vp]
+    L.efvm_wave_speed_slot.argtypes = [vp, C.POINTER(vp)]
     L.efvm_cfl_dt_noalloc.argtypes = [vp, vp, vp, vp, i64, C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), vp, vp]
     if L.efvm_abi_version() != abi.ABI_VERSION:
         raise ImportError("libefvm_b200.so ABI version mismatch")
@@ -81,12 +87,17 @@ def _dp(a: np.ndarray):
 class Context:
     """One case on the GPU: an efvm_ctx and its device state."""
 
-    def __init__(self, grid: abi.EfvmGrid, params: abi.EfvmParams):
+    def __init__(self, grid: abi.EfvmGrid, params: abi.EfvmParams, rows: tuple[int, int] | None = None):
+        """rows = (row0, n): a slab of global rows [row0, row0 + n) (efvm_create_slab)."""
         self.L = load()
         self.grid, self.params = grid, params
-        self.nx, self.ny = grid.nx, grid.ny
+        self.nx = grid.nx
+        self.row0, self.ny = (0, grid.ny) if rows is None else (int(rows[0]), int(rows[1]))
         h = C.c_void_p()
-        rc = self.L.efvm_create(C.byref(grid), C.byref(params), C.byref(h))
+        if rows is None:
+            rc = self.L.efvm_create(C.byref(grid), C.byref(params), C.byref(h))
+        else:
+            rc = self.L.efvm_create_slab(C.byref(grid), C.byref(params), self.row0, self.ny, C.byref(h))
         if rc != abi.OK:
             raise EfvmError(rc, self.L.efvm_last_error(None).decode())
         self.h = h
@@ -132,6 +143,22 @@ class Context:
 
     def substep(self) -> None:
         self._check(self.L.efvm_substep(self.h))
+
+    # ---- slabs (efvm_create_slab) ----
+    def prepare(self) -> None:
+        self._check(self.L.efvm_prepare(self.h))
+
+    def halo_pack(self, side: int, dev_ptr: int) -> None:
+        self._check(self.L.efvm_halo_pack(self.h, side, C.c_void_p(dev_ptr)))
+
+    def halo_unpack(self, side: int, dev_ptr: int) -> None:
+        self._check(self.L.efvm_halo_unpack(self.h, side, C.c_void_p(dev_ptr)))
+
+    def wave_speed_slot(self) -> int:
+        """Device address of the external wave-speed slot (a uint64)."""
+        p = C.c_void_p()
+        self._check(self.L.efvm_wave_speed_slot(self.h, C.byref(p)))
+        return int(p.value)
 
     def step_async(self, n_steps: int) -> None:
         """Enqueue whole steps on the context's stream without waiting."""

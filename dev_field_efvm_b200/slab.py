@@ -1,0 +1,252 @@
+"""One grid split into row slabs over several GPUs (one process per GPU).
+
+field_core decomposes a mesh over MPI ranks; every substage each rank fills
+the ghosts on its rank edges from its neighbours (halo_exchange_forward_all)
+and the solver takes the smallest dt over ranks (all_reduce_min_f64).  Here a
+grid of ny rows is split into contiguous row slabs, one device context per
+slab (efvm_create_slab), and every RK stage exchanges the two rows next to each
+slab edge with the neighbouring slab; once per step the largest wave speed is
+max-reduced over slabs (the same dt as the minimum of the per-slab dt).  The
+periodic wrap of a periodic y axis is one more slab edge, between the last
+slab and the first.
+
+The data path per stage is two rows of four FP64 planes per neighbour
+(8 * nx doubles each way), so the exchange is small next to a stage's compute;
+it runs on the context's stream and needs no host round trip.
+
+Transports:
+  * DistTransport: torch.distributed point-to-point send/recv and all_reduce
+    (NCCL with device tensors across GPUs; gloo with CPU tensors in the CPU tests).
+  * LocalTransport: all slabs in one process, copied on the device
+    (several slabs on one GPU, used to check the split on a single GPU).
+
+An engine is one slab's compute: the device Context (DeviceSlab) or any object
+with the same five methods (prepare, pack, unpack, substep, slot).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import torch
+
+from . import abi
+
+YLO, YHI = abi.YLO, abi.YHI
+# tags of the two directions, for transports that match messages by tag
+TAG_UP, TAG_DOWN = 11, 12
+
+
+def split_rows(ny: int, parts: int) -> list[tuple[int, int]]:
+    """Contiguous (row0, rows) slabs, sizes differing by at most one, each >= 2."""
+    if parts < 1 or ny < 2 * parts:
+        raise ValueError(f"cannot split {ny} rows into {parts} slabs of at least 2 rows")
+    base, extra = divmod(ny, parts)
+    out, r = [], 0
+    for k in range(parts):
+        n = base + (1 if k < extra else 0)
+        out.append((r, n))
+        r += n
+    return out
+
+
+@dataclass
+class Neighbours:
+    lower: int | None  # slab below (rows with smaller j), or None at a wall
+    upper: int | None
+
+
+def neighbours(rank: int, world: int, periodic_y: bool) -> Neighbours:
+    lo = rank - 1 if rank > 0 else (world - 1 if periodic_y else None)
+    hi = rank + 1 if rank < world - 1 else (0 if periodic_y else None)
+    return Neighbours(lo, hi)
+
+
+class DeviceSlab:
+    """The device engine of one slab: a Context made with efvm_create_slab."""
+
+    def __init__(self, grid: abi.EfvmGrid, params: abi.EfvmParams, row0: int, rows: int):
+        from .device import Context
+
+        self.ctx = Context(grid, params, rows=(row0, rows))
+        self.nx, self.ny = grid.nx, rows
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.ExternalStream(self.ctx.stream())
+        ptr = self.ctx.wave_speed_slot()
+        # a zero-copy int64 view of the slot (non-negative doubles' bits order like the values)
+        self._slot = torch.as_tensor(_CudaWord(ptr), device=self.device)
+
+    def new_buffer(self) -> torch.Tensor:
+        return torch.empty(8 * self.nx, dtype=torch.float64, device=self.device)
+
+    def prepare(self) -> None:
+        self.ctx.prepare()
+
+    def pack(self, side: int, buf: torch.Tensor) -> None:
+        self.ctx.halo_pack(side, buf.data_ptr())
+
+    def unpack(self, side: int, buf: torch.Tensor) -> None:
+        self.ctx.halo_unpack(side, buf.data_ptr())
+
+    def substep(self) -> None:
+        self.ctx.substep()
+
+    def slot(self) -> torch.Tensor:
+        return self._slot
+
+    def synchronize(self) -> None:
+        self.stream.synchronize()
+
+
+class _CudaWord:
+    """__cuda_array_interface__ of one int64 at a device address."""
+
+    def __init__(self, ptr: int):
+        self.__cuda_array_interface__ = {"shape": (1,), "typestr": "<i8", "data": (ptr, False), "version": 3}
+
+
+class DistTransport:
+    """Halo rows and the wave-speed maximum over torch.distributed.
+
+    Every rank posts the same pattern: sends to the upper then the lower
+    neighbour, receives from the lower then the upper one, so that with two
+    slabs on a periodic axis (the same peer above and below) the messages pair
+    up in order; tags make the pairing explicit for transports that use them."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+
+    def exchange(self, nb: Neighbours, send_lo, send_hi, recv_lo, recv_hi) -> None:
+        dist = self.dist
+        ops = []
+        if nb.upper is not None and nb.upper != self.rank:
+            ops.append(dist.P2POp(dist.isend, send_hi, nb.upper, self.group, TAG_UP))
+        if nb.lower is not None and nb.lower != self.rank:
+            ops.append(dist.P2POp(dist.isend, send_lo, nb.lower, self.group, TAG_DOWN))
+        if nb.lower is not None and nb.lower != self.rank:
+            ops.append(dist.P2POp(dist.irecv, recv_lo, nb.lower, self.group, TAG_UP))
+        if nb.upper is not None and nb.upper != self.rank:
+            ops.append(dist.P2POp(dist.irecv, recv_hi, nb.upper, self.group, TAG_DOWN))
+        if nb.lower == self.rank:  # one slab on a periodic axis: the wrap is local
+            recv_lo.copy_(send_hi)
+        if nb.upper == self.rank:
+            recv_hi.copy_(send_lo)
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+
+    def max_reduce(self, word: torch.Tensor) -> None:
+        if self.world > 1:
+            self.dist.all_reduce(word, op=self.dist.ReduceOp.MAX, group=self.group)
+
+
+class SlabRank:
+    """This process's slab of the grid, stepped in lockstep with the others."""
+
+    def __init__(self, engine, nb: Neighbours, transport):
+        self.e, self.nb, self.t = engine, nb, transport
+        mk = getattr(engine, "new_buffer")
+        self.send = {YLO: mk(), YHI: mk()}
+        self.recv = {YLO: mk(), YHI: mk()}
+        self.stream = getattr(engine, "stream", None)
+
+    def _ctx(self):
+        if self.stream is not None:
+            return torch.cuda.stream(self.stream)
+        return _Null()
+
+    def exchange(self) -> None:
+        """Fill both halo sides of the next substep's input from the neighbours."""
+        e, nb = self.e, self.nb
+        if nb.lower is not None:
+            e.pack(YLO, self.send[YLO])
+        if nb.upper is not None:
+            e.pack(YHI, self.send[YHI])
+        with self._ctx():
+            self.t.exchange(nb, self.send[YLO], self.send[YHI], self.recv[YLO], self.recv[YHI])
+        if nb.lower is not None:
+            e.unpack(YLO, self.recv[YLO])
+        if nb.upper is not None:
+            e.unpack(YHI, self.recv[YHI])
+
+    def step(self, n_steps: int) -> None:
+        """n whole SSP-RK3 steps (every rank calls this with the same n)."""
+        for _ in range(n_steps):
+            self.e.prepare()
+            with self._ctx():
+                self.t.max_reduce(self.e.slot())
+            for _s in range(3):
+                self.exchange()
+                self.e.substep()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+class LocalTransport:
+    """Every slab in this process: the exchange and the reduction are device
+    copies between the slabs' buffers, ordered by synchronising the slabs'
+    streams (a single-GPU stand-in for the multi-GPU transport)."""
+
+    def __init__(self, engines, periodic_y: bool):
+        self.engines = engines
+        self.world = len(engines)
+        self.nbs = [neighbours(k, self.world, periodic_y) for k in range(self.world)]
+        mk = [e.new_buffer for e in engines]
+        self.send = [{YLO: mk[k](), YHI: mk[k]()} for k in range(self.world)]
+        self.recv = [{YLO: mk[k](), YHI: mk[k]()} for k in range(self.world)]
+
+    def _sync(self):
+        for e in self.engines:
+            if hasattr(e, "synchronize"):
+                e.synchronize()
+
+    def exchange(self) -> None:
+        for k, e in enumerate(self.engines):
+            if self.nbs[k].lower is not None:
+                e.pack(YLO, self.send[k][YLO])
+            if self.nbs[k].upper is not None:
+                e.pack(YHI, self.send[k][YHI])
+        self._sync()
+        for k in range(self.world):
+            nb = self.nbs[k]
+            if nb.lower is not None:
+                self.recv[k][YLO].copy_(self.send[nb.lower][YHI])
+            if nb.upper is not None:
+                self.recv[k][YHI].copy_(self.send[nb.upper][YLO])
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+        for k, e in enumerate(self.engines):
+            if self.nbs[k].lower is not None:
+                e.unpack(YLO, self.recv[k][YLO])
+            if self.nbs[k].upper is not None:
+                e.unpack(YHI, self.recv[k][YHI])
+
+    def reduce(self) -> None:
+        self._sync()
+        words = [e.slot() for e in self.engines]
+        m = torch.stack([w.clone() for w in words]).max(dim=0).values
+        for w in words:
+            w.copy_(m)
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+
+    def step(self, n_steps: int) -> None:
+        for _ in range(n_steps):
+            for e in self.engines:
+                e.prepare()
+            self.reduce()
+            for _s in range(3):
+                self.exchange()
+                for e in self.engines:
+                    e.substep()
+        self._sync()

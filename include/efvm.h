@@ -267,6 +267,54 @@ int efvm_launch_count(efvm_ctx* ctx, uint64_t* out);
  * (the reference has no timers). */
 int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
 
+/* ---- slabs of one grid on several GPUs ------------------------------------ */
+
+/* A grid split into row slabs runs one context per slab (one process per GPU).
+ * field_core decomposes a mesh over MPI ranks and fills rank-edge ghosts with
+ * halo_exchange_forward_all, and the solver min-reduces dt over ranks
+ * (all_reduce_min_f64); a slab does the same with two calls per neighbour per
+ * RK stage and one reduction per step, which the caller carries over its own
+ * transport (NCCL, or copies between contexts on one GPU):
+ *
+ *   efvm_prepare(ctx);  max-reduce *slot over slabs;
+ *   for s in 0..2 { efvm_halo_pack(ctx, YLO/YHI, send); exchange with the two
+ *                   neighbours; efvm_halo_unpack(ctx, YLO/YHI, recv);
+ *                   efvm_substep(ctx); }
+ *   (efvm_prepare does work only after an upload or a solver-state change)
+ *
+ * Faces between slabs are interior faces, so results do not depend on the
+ * split (field_core leaves the halo side of a rank edge unreconstructed under
+ * MUSCL, crates/cfd_solver/src/lib.rs:323-331; here only the global periodic
+ * seam keeps the efvm_seam rule).  IBM cylinders and efvm_step are not
+ * supported on slabs (EFVM_ERR_UNSUPPORTED). */
+
+/* A context for global rows [row0, row0 + rows) of `grid` (rows >= 2).  Cell
+ * coordinates, spacing and boundary conditions are the global grid's; a y side
+ * that faces another slab, or the periodic wrap of a periodic y axis, takes its
+ * two ghost rows from efvm_halo_unpack.  Upload/download cover the slab's rows. */
+int efvm_create_slab(const efvm_grid* grid, const efvm_params* params, int32_t row0, int32_t rows,
+                     efvm_ctx** out);
+/* Run now what the next substep would run first: the stand-alone CFL pass after
+ * an upload (into the wave speed slot when one is enabled), pending cylinder
+ * geometry, and the boundary-ghost fill of non-HALO sides. */
+int efvm_prepare(efvm_ctx* ctx);
+/* Copy the two interior rows next to y side `side` (EFVM_YLO: rows 0,1;
+ * EFVM_YHI: rows ny-2, ny-1) of the next substep's input into dev_buf, a device
+ * buffer of 8*nx doubles laid out [variable rho, rho_u, rho_v, rho_e][row, in
+ * increasing j][i].  Asynchronous on the context's stream. */
+int efvm_halo_pack(efvm_ctx* ctx, int32_t side, double* dev_buf);
+/* Write such a buffer, packed by the neighbour on that side, into the two ghost
+ * rows of side `side` (EFVM_YLO: rows -2,-1; EFVM_YHI: rows ny, ny+1) of the next
+ * substep's input.  The side must take its ghosts from a neighbour.  Asynchronous. */
+int efvm_halo_unpack(efvm_ctx* ctx, int32_t side, const double* dev_buf);
+/* Switch the context to an external wave-speed slot and return its device
+ * address: an unsigned 64-bit word holding the bits of the largest wave speed
+ * (a non-negative double, so its bits order like the value).  The last stage of
+ * each step (and the CFL pass after an upload) max-accumulates into it; the
+ * next step's set-up reads it, takes dt = cfl / slot, and clears it.  Between
+ * the two the caller max-reduces the word across slabs (an integer max). */
+int efvm_wave_speed_slot(efvm_ctx* ctx, uint64_t** dev_slot);
+
 /* ---- CFL time step without any allocation -------------------------------- */
 
 /* Rows of scratch that efvm_cfl_dt_noalloc keeps in static device memory. */
