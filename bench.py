@@ -19,8 +19,9 @@ stage) to its live CUDA-event duration and the measured HBM copy bandwidth.
 C++, OpenMP over the host cores) on a bounded sample of the same workload.
 
 Under torchrun (N > 1) every rank advances its own replica of the case (weak
-scaling; one grid does not yet shard across GPUs), timing is the max over
-ranks, and `value` counts the cells of all ranks.
+scaling: the cylinder's immersed body is not split over row slabs, see
+dev_field_efvm_b200/slab.py), timing is the max over ranks, and `value` counts
+the cells of all ranks.
 """
 from __future__ import annotations
 
@@ -41,7 +42,7 @@ METRIC = "Cell-updates/s on 1 B200: plain FP64 vs chosen form at equal L1 densit
 UNIT = "cell-updates/s"
 
 
-def workload(name: str):
+def workload(name: str, size: int | None = None):
     from dev_field_efvm_b200 import cases
     from dev_field_efvm_b200 import abi
     if name == "cylinder":
@@ -51,8 +52,9 @@ def workload(name: str):
                 "nx": grid.nx, "ny": grid.ny}
         return grid, params, u, ex, desc
     if name == "vortex4096":
-        grid, params, u, ex = cases.vortex_case(4096, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4)
-        desc = {"workload": "isentropic vortex, periodic [0,10]^2, 4096x4096 cells, MUSCL-minmod + HLLC-Thornber, "
+        n = size or 4096
+        grid, params, u, ex = cases.vortex_case(n, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4)
+        desc = {"workload": f"isentropic vortex, periodic [0,10]^2, {n}x{n} cells, MUSCL-minmod + HLLC-Thornber, "
                             "SSP-RK3, CFL 0.4, FP64", "nx": grid.nx, "ny": grid.ny}
         return grid, params, u, ex, desc
     raise SystemExit(f"unknown workload {name}")
@@ -139,7 +141,7 @@ def run_reference(args, rank, world, budget_s=90.0):
     minutes for any K; the rate is cell-updates over that sample's time."""
     if rank != 0:
         return
-    grid, params, u, ex, desc = workload(args.workload)
+    grid, params, u, ex, desc = workload(args.workload, args.size)
     from oracle import pyoracle
     c = pyoracle.OracleCase(grid, params, parallel=True)
     if "cylinders" in ex:
@@ -173,6 +175,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cylinder", choices=["cylinder", "vortex4096"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=None,
+                    help="vortex workload only: a smaller n x n grid of the same case (for profiler captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -195,7 +199,7 @@ def main():
     from dev_field_efvm_b200 import abi
     from dev_field_efvm_b200.device import Context
 
-    grid, params, u, ex, desc = workload(args.workload)
+    grid, params, u, ex, desc = workload(args.workload, args.size)
     cells = grid.nx * grid.ny
     ctx = Context(grid, params)
     if "cylinders" in ex:
@@ -241,9 +245,9 @@ def main():
     traffic = None
     tf = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
     if os.path.exists(tf):
-        d = json.load(open(tf))
-        if d.get("workload_key") == args.workload:
-            traffic = d.get("bytes_per_launch")
+        entry = json.load(open(tf)).get(args.workload) if args.size is None else None
+        if entry:
+            traffic = entry.get("bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind,
                 "kernel": "stage_kernel (fused MUSCL/HLLC/viscous/RK3 substage)",
