@@ -167,13 +167,112 @@ def run_reference(args, rank, world, budget_s=90.0):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rank, world, local):
+    """512 independent cases in one batch (n log-uniform in [32, 512]; half
+    periodic vortices to t = 1, half four-quadrant Riemann problems to t = 0.05;
+    MUSCL-minmod + HLLC-Thornber, FP32 fluxes with FP64 accumulation).  `value`
+    is the batch's total cell-updates over its device time (CUDA events on the
+    batch stream around the whole run, host polling gaps included); the
+    sequential leg runs the same cases one context after another and gives the
+    per-case completion percentiles it is compared with.  Each rank runs its own
+    batch (weak scaling)."""
+    import torch
+    torch.cuda.set_device(local)
+    from dev_field_efvm_b200 import cases
+    from dev_field_efvm_b200.device import Batch, Context
+
+    grids, params, states, t_stop, kinds = cases.batch_cases()
+    cells = np.array([g.nx * g.ny for g in grids], dtype=np.float64)
+    warm = Batch(grids, params)
+    for k, u in enumerate(states):
+        warm.upload(k, u)
+    warm.run(t_stop, max_steps=args.warmup)
+    warm.close()
+
+    b = Batch(grids, params)
+    for k, u in enumerate(states):
+        b.upload(k, u)
+    stream = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = b.launch_count()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        res = b.run(t_stop)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = b.launch_count() - n0
+    steps = np.array([r.steps for r in res], dtype=np.float64)
+    work = float((cells * steps).sum())
+    value = work / (ms * 1e-3)
+    comp = np.array([r.completion_ms for r in res])
+
+    # end to end: host states in, the whole batch run, host states out
+    t0 = time.perf_counter()
+    b2 = Batch(grids, params)
+    for k, u in enumerate(states):
+        b2.upload(k, u)
+    b2.run(t_stop)
+    for k in range(len(grids)):
+        b2.download(k)
+    e2e_s = time.perf_counter() - t0
+    b2.close()
+    h2d = int(sum(u.size for u in states) * 8)
+
+    # sequential: one context per case, one after another (shortest first)
+    order = np.argsort(cells * steps)
+    seq_done = np.zeros(len(grids))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in order:
+        c = Context(grids[k], params)
+        c.upload(states[k])
+        c.run_until(float(t_stop[k]))
+        seq_done[k] = (time.perf_counter() - t0) * 1e3
+        c.close()
+    seq_s = time.perf_counter() - t0
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        achieved = value * 256.0 / 1e9
+        line = {
+            "metric": "total cell-updates/s of a 512-case batch on 1 B200", "value": world * value, "unit": UNIT,
+            "n_gpus": world, "steps": int(steps.max()), "warmup": args.warmup, "ms_per_step": ms / steps.max(),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32-flux/f64-state",
+            "data": "synthetic",
+            "config": {"workload": "512 cases, n log-uniform in [32,512] (23.4 M cells): 256 periodic vortices to "
+                                   "t=1, 256 four-quadrant Riemann problems to t=0.05; MUSCL-minmod + HLLC-Thornber, "
+                                   "SSP-RK3, CFL 0.4, FP32 fluxes + FP64 state",
+                       "cases": len(grids), "cells": int(cells.sum()), "cell_updates": work,
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (2.2 GB of state)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": peak_kind,
+                         "kernel": "whole batch run (256 algorithmic B per cell-update over the run's device time)"},
+            "cpu_baseline": None,
+            "e2e": {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": h2d, "note": "one 'step' here is the whole batch run"},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "batch": {"completion_ms_p50": float(np.percentile(comp, 50)),
+                      "completion_ms_p99": float(np.percentile(comp, 99)),
+                      "batch_ms": ms,
+                      "sequential_completion_ms_p50": float(np.percentile(seq_done, 50)),
+                      "sequential_completion_ms_p99": float(np.percentile(seq_done, 99)),
+                      "sequential_s": seq_s, "sequential_value": work / seq_s,
+                      "all_finished": bool(all(r.finished for r in res))},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=8000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "vortex4096"])
+    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "vortex4096", "batch512"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--size", type=int, default=None,
                     help="vortex workload only: a smaller n x n grid of the same case (for profiler captures)")
@@ -185,7 +284,14 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
+        if args.workload == "batch512":
+            print(json.dumps({"impl": "reference", "unavailable": "the batch workload has no reference arm here; "
+                              "run the default workload"}), flush=True)
+            return
         run_reference(args, rank, world)
+        return
+    if args.workload == "batch512":
+        run_batch(args, rank, world, local)
         return
 
     import torch

@@ -102,6 +102,16 @@ class EfvmParams(C.Structure):
     ]
 
 
+class EfvmBatchCaseResult(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int64),
+        ("time", C.c_double),
+        ("completion_ms", C.c_double),
+        ("nonphysical", C.c_int32),
+        ("finished", C.c_int32),
+    ]
+
+
 class EfvmSolverState(C.Structure):
     _fields_ = [
         ("dt", C.c_double),

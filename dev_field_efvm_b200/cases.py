@@ -207,3 +207,50 @@ def moments(u: np.ndarray, x: np.ndarray, cell_volume: float) -> np.ndarray:
     """[sum rho V, sum rho^2 V, sum rho x V] (tests/periodic_mpi.rs:83-96)."""
     rho = u[..., 0]
     return np.array([np.sum(rho * cell_volume), np.sum(rho * rho * cell_volume), np.sum(rho * x * cell_volume)])
+
+
+def riemann4_state(x, y, split, states, gamma=1.4):
+    """Four constant quadrants around split = (xs, ys); states[q] = (rho, u, v, p)
+    for q = 0: x<xs,y<ys; 1: x>=xs,y<ys; 2: x<xs,y>=ys; 3: x>=xs,y>=ys."""
+    X, Y = np.meshgrid(x, y)
+    q = (X >= split[0]).astype(int) + 2 * (Y >= split[1]).astype(int)
+    st = np.asarray(states, dtype=np.float64)
+    return prim_to_cons(st[q, 0], st[q, 1], st[q, 2], st[q, 3], gamma)
+
+
+def batch_cases(n_cases=512, seed=2024, n_min=32, n_max=512, t_vortex=1.0, t_riemann=0.05,
+                precision=abi.PREC_FP32_FLUX):
+    """The batching workload: n_cases square grids with n log-uniform in
+    [n_min, n_max]; even cases are isentropic vortices on the periodic [0,10]^2
+    box (beta ~ U[1,5], centre ~ U[3,7]^2, mean flow (1,1)), odd cases
+    four-quadrant Riemann problems on [0,1]^2 with zero-gradient (transmissive)
+    boundaries (rho, p ~ U[0.1,2], u, v ~ U[-1,1], split point ~ U[0.3,0.7]^2).
+    All share MUSCL-minmod + HLLC-Thornber, SSP-RK3, CFL 0.4 and `precision`;
+    dz = L/n.  Returns (grids, params, states, t_stop, kinds)."""
+    rng = np.random.default_rng(seed)
+    params = abi.make_params(cfl=0.4, reconstruction=abi.RECON_MUSCL, limiter=abi.LIMITER_MINMOD, precision=precision)
+    grids, states, t_stop, kinds = [], [], [], []
+    out = abi.BC_SUPERSONIC_OUTFLOW
+    for k in range(n_cases):
+        n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        if k % 2 == 0:
+            beta = float(rng.uniform(1.0, 5.0))
+            centre = (float(rng.uniform(3.0, 7.0)), float(rng.uniform(3.0, 7.0)))
+            grid, _, u, _ = vortex_case(n, periodic=True, muscl=True, mean=(1.0, 1.0), beta=beta, centre=centre)
+            grids.append(grid)
+            states.append(u)
+            t_stop.append(t_vortex)
+            kinds.append("vortex")
+        else:
+            bcs = {abi.XLO: out, abi.XHI: out, abi.YLO: out, abi.YHI: out,
+                   abi.ZLO: abi.BC_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+            grid = abi.make_grid(n, n, hi=(1.0, 1.0, 1.0 / n), bcs=bcs)
+            split = (float(rng.uniform(0.3, 0.7)), float(rng.uniform(0.3, 0.7)))
+            quads = [(rng.uniform(0.1, 2.0), rng.uniform(-1.0, 1.0), rng.uniform(-1.0, 1.0), rng.uniform(0.1, 2.0))
+                     for _ in range(4)]
+            x, y = centroids(grid)
+            grids.append(grid)
+            states.append(riemann4_state(x, y, split, quads))
+            t_stop.append(t_riemann)
+            kinds.append("riemann")
+    return grids, params, states, np.array(t_stop), kinds

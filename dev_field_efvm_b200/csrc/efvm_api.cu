@@ -346,63 +346,50 @@ namespace efvm {
 void set_global_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace efvm
 
-extern "C" {
+namespace efvm {
 
-int efvm_abi_version(void) { return EFVM_ABI_VERSION; }
-
-const char* efvm_last_error(const efvm_ctx* ctx) {
-    if (ctx) return ctx->err.c_str();
-    return g_last_error.c_str();
-}
-
-// efvm_create / efvm_create_slab: a context for global rows [row0, row0 + rows)
-// of `grid`; `slab` marks the y sides that face another slab or the periodic
-// wrap as halo sides.
-static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t row0, int32_t rows, bool slab,
-                       efvm_ctx** out) {
-    if (!grid || !params || !out) return fail(nullptr, EFVM_ERR_INVALID_ARG, "null argument");
-    *out = nullptr;
-    const efvm_grid& gr = *grid;
-    if (gr.nz != 1) return fail(nullptr, EFVM_ERR_UNSUPPORTED, "only 2-D meshes (nz == 1) are supported");
-    if (gr.ng != 2) return fail(nullptr, EFVM_ERR_UNSUPPORTED, "only ng == 2 ghost layers are supported");
-    if (gr.nx < 2 || gr.ny < 1) return fail(nullptr, EFVM_ERR_INVALID_ARG, "nx must be >= 2 and ny >= 1");
+int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bool slab, Geometry& g, Physics& ph,
+               std::string& err) {
+    auto bad = [&](int code, const std::string& m) {
+        err = m;
+        return code;
+    };
+    if (gr.nz != 1) return bad(EFVM_ERR_UNSUPPORTED, "only 2-D meshes (nz == 1) are supported");
+    if (gr.ng != 2) return bad(EFVM_ERR_UNSUPPORTED, "only ng == 2 ghost layers are supported");
+    if (gr.nx < 2 || gr.ny < 1) return bad(EFVM_ERR_INVALID_ARG, "nx must be >= 2 and ny >= 1");
     for (int a = 0; a < 3; ++a)
-        if (!(gr.hi[a] > gr.lo[a])) return fail(nullptr, EFVM_ERR_INVALID_ARG, "bounds_hi must exceed bounds_lo");
+        if (!(gr.hi[a] > gr.lo[a])) return bad(EFVM_ERR_INVALID_ARG, "bounds_hi must exceed bounds_lo");
     for (int a = 0; a < 3; ++a) {
         const bool lo_p = gr.bc[2 * a].kind == EFVM_BC_PERIODIC, hi_p = gr.bc[2 * a + 1].kind == EFVM_BC_PERIODIC;
         if (lo_p != hi_p)
-            return fail(nullptr, EFVM_ERR_INVALID_ARG,
+            return bad(EFVM_ERR_INVALID_ARG,
                         "invalid periodic boundary configuration: periodic boundary on axis " + std::to_string(a) +
                             " requires both sides");
     }
     for (int s = 0; s < 6; ++s)
-        if (!bc_supported(gr.bc[s].kind)) return fail(nullptr, EFVM_ERR_INVALID_ARG, "unknown boundary kind");
+        if (!bc_supported(gr.bc[s].kind)) return bad(EFVM_ERR_INVALID_ARG, "unknown boundary kind");
     if ((gr.bc[EFVM_XLO].kind == EFVM_BC_PERIODIC && gr.nx < 2) || (gr.bc[EFVM_YLO].kind == EFVM_BC_PERIODIC && gr.ny < 2))
-        return fail(nullptr, EFVM_ERR_INVALID_ARG, "a periodic axis needs at least 2 cells (two ghost layers wrap)");
+        return bad(EFVM_ERR_INVALID_ARG, "a periodic axis needs at least 2 cells (two ghost layers wrap)");
     if (gr.bc[EFVM_ZLO].kind == EFVM_BC_PERIODIC)
-        return fail(nullptr, EFVM_ERR_UNSUPPORTED, "a periodic z axis has no meaning on a 2-D mesh");
-    const efvm_params& p = *params;
-    if (!(p.gamma > 1.0) || !(p.r_gas > 0.0)) return fail(nullptr, EFVM_ERR_INVALID_ARG, "gamma must exceed 1, r_gas > 0");
-    if (!(p.cfl > 0.0) && !(p.fixed_dt > 0.0)) return fail(nullptr, EFVM_ERR_INVALID_ARG, "cfl or fixed_dt must be > 0");
+        return bad(EFVM_ERR_UNSUPPORTED, "a periodic z axis has no meaning on a 2-D mesh");
+    if (!(p.gamma > 1.0) || !(p.r_gas > 0.0)) return bad(EFVM_ERR_INVALID_ARG, "gamma must exceed 1, r_gas > 0");
+    if (!(p.cfl > 0.0) && !(p.fixed_dt > 0.0)) return bad(EFVM_ERR_INVALID_ARG, "cfl or fixed_dt must be > 0");
     if (p.flux_scheme < 0 || p.flux_scheme > 2 || p.reconstruction < 0 || p.reconstruction > 1 || p.limiter < 0 ||
         p.limiter > 1 || p.integrator < 0 || p.integrator > 1 || p.precision < 0 || p.precision > 1 ||
         p.periodic_seam < 0 || p.periodic_seam > 1 || p.viscosity_model < 0 || p.viscosity_model > 1)
-        return fail(nullptr, EFVM_ERR_INVALID_ARG, "enum field out of range");
+        return bad(EFVM_ERR_INVALID_ARG, "enum field out of range");
     if (p.sponge && !(p.sponge_x_end > p.sponge_x_start))
-        return fail(nullptr, EFVM_ERR_INVALID_ARG, "sponge_x_end must exceed sponge_x_start");
+        return bad(EFVM_ERR_INVALID_ARG, "sponge_x_end must exceed sponge_x_start");
     if (slab && (row0 < 0 || rows < 2 || (int64_t)row0 + rows > gr.ny))
-        return fail(nullptr, EFVM_ERR_INVALID_ARG, "a slab needs rows >= 2 inside the grid: 0 <= row0, row0 + rows <= ny");
+        return bad(EFVM_ERR_INVALID_ARG, "a slab needs rows >= 2 inside the grid: 0 <= row0, row0 + rows <= ny");
 
-    efvm_ctx* c = new efvm_ctx();
-    c->grid = gr;
-    c->params = p;
-    cudaGetDevice(&c->device);
-    Geometry& g = c->g;
+    g = Geometry{};
+    ph = Physics{};
     g.nx = gr.nx;
     g.ny = rows;
     g.j_off = row0;
     g.pitch = ((XO + gr.nx + NG) + 7) / 8 * 8;
-    g.plane = ((long long)(gr.ny + 2 * YO) * g.pitch + 31) / 32 * 32;
+    g.plane = ((long long)(rows + 2 * YO) * g.pitch + 31) / 32 * 32;
     const int n[3] = {gr.nx, gr.ny, gr.nz};
     for (int a = 0; a < 3; ++a) {
         g.lo[a] = gr.lo[a];
@@ -412,7 +399,6 @@ static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t
     g.cell_volume = g.h[0] * g.h[1] * g.h[2];
     g.inv_x = (g.h[1] * g.h[2]) / g.cell_volume;
     g.inv_y = (g.h[0] * g.h[2]) / g.cell_volume;
-    Physics& ph = c->ph;
     ph.gamma = p.gamma;
     ph.r_gas = p.r_gas;
     ph.cfl = p.cfl;
@@ -462,7 +448,53 @@ static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t
     ph.dx_inv2 = 1.0 / (g.h[0] * g.h[0]);
     ph.cp = p.gamma * p.r_gas / (p.gamma - 1.0);
     ph.cfl_visc_sum = 1.0 / (g.h[0] * g.h[0]) + 1.0 / (g.h[1] * g.h[1]) + 1.0 / (g.h[2] * g.h[2]);
+    return EFVM_OK;
+}
 
+// viscous_system's pre-inverted y weights from centroid distances (global row
+// indices), crates/cfd_solver/src/lib.rs:484-493: y_im, y_ip, y_is per row.
+std::vector<double> viscous_y_weights(const Geometry& g) {
+    std::vector<double> yw(3 * (size_t)g.ny);
+    for (int j = 0; j < g.ny; ++j) {
+        const int jg = j + g.j_off;
+        const double hm = centre_h(g.lo[1], g.h[1], jg) - centre_h(g.lo[1], g.h[1], jg - 1);
+        const double hp = centre_h(g.lo[1], g.h[1], jg + 1) - centre_h(g.lo[1], g.h[1], jg);
+        yw[j] = 1.0 / hm;
+        yw[g.ny + j] = 1.0 / hp;
+        yw[2 * g.ny + j] = 2.0 / (hm + hp);
+    }
+    return yw;
+}
+
+}  // namespace efvm
+
+extern "C" {
+
+int efvm_abi_version(void) { return EFVM_ABI_VERSION; }
+
+const char* efvm_last_error(const efvm_ctx* ctx) {
+    if (ctx) return ctx->err.c_str();
+    return g_last_error.c_str();
+}
+
+// efvm_create / efvm_create_slab: a context for global rows [row0, row0 + rows)
+// of `grid`; `slab` marks the y sides that face another slab or the periodic
+// wrap as halo sides.
+static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t row0, int32_t rows, bool slab,
+                       efvm_ctx** out) {
+    if (!grid || !params || !out) return fail(nullptr, EFVM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    Geometry g;
+    Physics ph;
+    std::string err;
+    const int rc = setup_case(*grid, *params, row0, rows, slab, g, ph, err);
+    if (rc) return fail(nullptr, rc, err);
+    efvm_ctx* c = new efvm_ctx();
+    c->grid = *grid;
+    c->params = *params;
+    cudaGetDevice(&c->device);
+    c->g = g;
+    c->ph = ph;
     auto cleanup_fail = [&](int code) {
         efvm_destroy(c);
         return code;
@@ -485,17 +517,7 @@ static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t
     e = cudaMalloc(&c->mask, (size_t)g.plane);
     if (e != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc mask"));
     cudaMemsetAsync(c->mask, 0, (size_t)g.plane, c->stream);
-    // viscous_system's pre-inverted y weights from centroid distances,
-    // crates/cfd_solver/src/lib.rs:484-493
-    std::vector<double> yw(3 * (size_t)g.ny);
-    for (int j = 0; j < g.ny; ++j) {
-        const int jg = j + g.j_off;
-        const double hm = centre_h(g.lo[1], g.h[1], jg) - centre_h(g.lo[1], g.h[1], jg - 1);
-        const double hp = centre_h(g.lo[1], g.h[1], jg + 1) - centre_h(g.lo[1], g.h[1], jg);
-        yw[j] = 1.0 / hm;
-        yw[g.ny + j] = 1.0 / hp;
-        yw[2 * g.ny + j] = 2.0 / (hm + hp);
-    }
+    const std::vector<double> yw = viscous_y_weights(g);
     if (cudaMalloc(&c->yw, yw.size() * sizeof(double)) != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
     cudaMemcpyAsync(c->yw, yw.data(), yw.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (cudaMalloc(&c->st, sizeof(DevState)) != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));

@@ -12,6 +12,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/efvm.h"
 
@@ -39,6 +40,7 @@ struct DevState {
     unsigned long long lam_ext;  // external wave-speed slot (slabs), see efvm_wave_speed_slot
     int ext_lam;             // 1: accumulate into / read from lam_ext
     int pad_;
+    unsigned long long done_ns;  // device global timer when the set-up stopped the run
 };
 
 // Boundary side description resolved for the device.
@@ -143,6 +145,45 @@ struct StageArgs {
     int completes_step;               // sponge + CFL + clock in the epilogue
     int want_cfl;
 };
+
+// ---- batches of independent cases (efvm_batch.cu) --------------------------
+// One case of a batch, as the batch kernels read it.
+struct BatchCase {
+    Geometry g;
+    Physics ph;             // the shared settings with this case's boundaries and spacing
+    int rows;               // rows per warp of this case's tiles
+    int pad;
+    double* U[3];
+    const double* yw;
+    DevState* st;
+};
+
+// One stage over the tiles of every active case: tile (case, strip, row block)
+// is one warp's share of that case's stage.
+struct BatchStageArgs {
+    Physics ph;             // the shared settings (scheme, precision, gas, CFL)
+    const BatchCase* __restrict__ cases;
+    const int4* tiles;
+    int stage, completes_step, want_cfl;
+    int in_buf, out_buf;    // U[in_buf] -> U[out_buf]; U[0] is u^n
+};
+
+// Stage-kernel tiling of one case: strips of columns, and rows per warp for a
+// case that runs alone (fp32: the FP32-flux form).
+int stage_strips(int nx);
+int stage_rows(int nx, int ny, bool fp32);
+int launch_batch_stage(const BatchStageArgs& b, int n_tiles, bool pdl, void* stream);
+// Per-step set-up of every case (one thread each).
+int launch_batch_setup(const Physics& ph, const BatchCase* cases, int n_cases, bool pdl, void* stream);
+// Write the device global timer (ns) to *out.
+int launch_clock(unsigned long long* out, void* stream);
+
+// Validation and the device description of one case (efvm_api.cu): global rows
+// [row0, row0 + rows) of `gr`, halo sides when `slab`.  Returns a status and
+// sets `err` on failure.
+int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bool slab, Geometry& g, Physics& ph,
+               std::string& err);
+std::vector<double> viscous_y_weights(const Geometry& g);
 
 // Sets the message efvm_last_error(NULL) returns (efvm_api.cu).
 void set_global_error(const std::string& msg);

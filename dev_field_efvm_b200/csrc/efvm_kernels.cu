@@ -288,15 +288,14 @@ constexpr int WPB = 4;     // warps per block
 // on a step's last stage, the sponge, refills the boundary ghosts of the output
 // and takes the wave-speed max for the next step's CFL dt.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, class R, int MINB>
-__global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
-    pdl_wait_then_release();
+template <int SCHEME, int RECON, class R, class A>
+__device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
     if (!a.st->active) return;
     const Geometry& g = a.g;
     const Physics& ph = a.ph;
     const long long P = g.plane;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+    const int lane = threadIdx.x & 31;
+    if (strip == 0 && by == 0 && lane == 0) {
         // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
         // (no other thread reads time/step/rk_stage during this kernel)
         DevState* st = a.st;
@@ -310,8 +309,8 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
             st->completed = 0;
         }
     }
-    const int i0 = (blockIdx.x * WPB + warp) * STRIP;
-    const int jb = blockIdx.y * rows;
+    const int i0 = strip * STRIP;
+    const int jb = by * rows;
     double lam = 0.0;
     if (i0 < g.nx && jb < g.ny) {  // uniform across the warp
         constexpr bool MUSCL = RECON == EFVM_RECON_MUSCL;
@@ -524,6 +523,44 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
     }
 }
 
+template <int SCHEME, int RECON, class R, int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
+    pdl_wait_then_release();
+    stage_strip<SCHEME, RECON, R>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5), blockIdx.y);
+}
+
+// The stage arguments of one batch case, with its geometry and physics in the
+// case table in global memory.
+struct BatchView {
+    const Geometry& g;
+    const Physics& ph;
+    const double* __restrict__ uin;
+    const double* u0;
+    double* uout;
+    const uint8_t* __restrict__ mask;
+    const double* __restrict__ yw;
+    DevState* st;
+    int stage, completes_step, want_cfl;
+};
+
+// The same stage over a batch of independent cases, one warp per tile: warp w
+// of block b runs tiles[b * WPB + w] = (case, strip, row block) of that case,
+// with the case's geometry, boundary conditions, buffers and clock.  Warps are
+// the unit so that small cases waste no lanes of a block.
+template <int SCHEME, int RECON, class R, int MINB>
+__global__ void __launch_bounds__(32 * WPB, MINB) batch_stage_kernel(BatchStageArgs b, int n_tiles) {
+    pdl_wait_then_release();
+    const int tile = blockIdx.x * WPB + (threadIdx.x >> 5);
+    if (tile >= n_tiles) return;  // uniform per warp; the kernel has no block barrier
+    const int4 t = b.tiles[tile];
+    const BatchCase& c = b.cases[t.x];
+    // the case's geometry and physics are read in place from the case table
+    const BatchView v{c.g, c.ph, c.U[b.in_buf], c.U[0], c.U[b.out_buf], nullptr, c.yw, c.st,
+                      b.stage, b.completes_step, b.want_cfl};
+    stage_strip<SCHEME, RECON, R>(v, c.rows, t.y, t.z);
+}
+
+
 // ---------------------------------------------------------------------------
 // CFL wave-speed max over the interior of one state (standalone pass)
 // ---------------------------------------------------------------------------
@@ -553,9 +590,16 @@ __device__ __forceinline__ bool step_stops(const DevState* st) {
 // Per-step set-up (one thread): stop check, dt = cfl / max wave speed (cfl_system,
 // crates/cfd_solver/src/lib.rs:647-669) and the switch of the wave-speed buffer
 // that the step's last stage accumulates into.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
     if (step_stops(st)) {
         st->active = 0;
+        st->done_ns = global_ns();
         return;
     }
     double dt;
@@ -580,6 +624,16 @@ __global__ void step_setup_kernel(Physics ph, DevState* st) {
     if (!st->active) return;
     step_setup(ph, st);
 }
+
+__global__ void batch_setup_kernel(Physics ph, const BatchCase* cases, int n) {
+    pdl_wait_then_release();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    DevState* st = cases[k].st;
+    if (st->active) step_setup(ph, st);
+}
+
+__global__ void clock_kernel(unsigned long long* out) { *out = global_ns(); }
 
 // ---------------------------------------------------------------------------
 // Halo + Boundary for a whole state (after upload / geometry changes)
@@ -1062,6 +1116,54 @@ int launch_stage(const StageArgs& a, bool pdl, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_r<float>(a, pdl, s);
     else launch_stage_r<double>(a, pdl, s);
+    return 1;
+}
+
+int stage_strips(int nx) { return (nx + STRIP - 1) / STRIP; }
+
+int stage_rows(int nx, int ny, bool fp32) { return rows_per_warp(nx, ny, fp32 ? 8 : 5); }
+
+template <int SCHEME, int RECON, class R>
+static void launch_batch_t(const BatchStageArgs& b, int n_tiles, bool pdl, cudaStream_t s) {
+    constexpr int MINB = sizeof(R) == sizeof(double) ? 5 : 8;
+    launch_k(batch_stage_kernel<SCHEME, RECON, R, MINB>, dim3((n_tiles + WPB - 1) / WPB), dim3(32 * WPB), s, pdl, b,
+             n_tiles);
+}
+
+template <class R>
+static void launch_batch_r(const BatchStageArgs& b, int n_tiles, bool pdl, cudaStream_t s) {
+    const bool muscl = b.ph.reconstruction == EFVM_RECON_MUSCL;
+    switch (b.ph.flux_scheme) {
+        case EFVM_FLUX_RUSANOV:
+            muscl ? launch_batch_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R>(b, n_tiles, pdl, s)
+                  : launch_batch_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R>(b, n_tiles, pdl, s);
+            break;
+        case EFVM_FLUX_HLLC_TEXTBOOK:
+            muscl ? launch_batch_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R>(b, n_tiles, pdl, s)
+                  : launch_batch_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R>(b, n_tiles, pdl, s);
+            break;
+        default:
+            muscl ? launch_batch_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R>(b, n_tiles, pdl, s)
+                  : launch_batch_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R>(b, n_tiles, pdl, s);
+    }
+}
+
+int launch_batch_stage(const BatchStageArgs& b, int n_tiles, bool pdl, void* stream) {
+    if (n_tiles <= 0) return 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b.ph.precision == EFVM_PREC_FP32_FLUX) launch_batch_r<float>(b, n_tiles, pdl, s);
+    else launch_batch_r<double>(b, n_tiles, pdl, s);
+    return 1;
+}
+
+int launch_batch_setup(const Physics& ph, const BatchCase* cases, int n_cases, bool pdl, void* stream) {
+    launch_k(batch_setup_kernel, dim3((n_cases + 127) / 128), dim3(128), (cudaStream_t)stream, pdl, ph, cases,
+             n_cases);
+    return 1;
+}
+
+int launch_clock(unsigned long long* out, void* stream) {
+    clock_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(out);
     return 1;
 }
 

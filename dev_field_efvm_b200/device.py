@@ -24,7 +24,9 @@ EXPORTS = (
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
-    "efvm_wave_speed_slot", "efvm_cfl_dt_noalloc",
+    "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
+    "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
+    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_cfl_dt_noalloc",
 )
 
 
@@ -72,6 +74,16 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_halo_pack.argtypes = [vp, i32, vp]
     L.efvm_halo_unpack.argtypes = [vp, i32, vp]
     L.efvm_wave_speed_slot.argtypes = [vp, C.POINTER(vp)]
+    L.efvm_batch_create.argtypes = [C.POINTER(abi.EfvmGrid), i32, C.POINTER(abi.EfvmParams), C.POINTER(vp)]
+    L.efvm_batch_destroy.argtypes = [vp]
+    L.efvm_batch_last_error.restype = C.c_char_p
+    L.efvm_batch_last_error.argtypes = [vp]
+    L.efvm_batch_upload_state.argtypes = [vp, i32, dp, i64, i64, i64]
+    L.efvm_batch_download_state.argtypes = [vp, i32, dp, i64, i64, i64]
+    L.efvm_batch_get_solver_state.argtypes = [vp, i32, C.POINTER(abi.EfvmSolverState)]
+    L.efvm_batch_run.argtypes = [vp, dp, i64, i64, C.POINTER(abi.EfvmBatchCaseResult)]
+    L.efvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.efvm_batch_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_cfl_dt_noalloc.argtypes = [vp, vp, vp, vp, i64, C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), vp, vp]
     if L.efvm_abi_version() != abi.ABI_VERSION:
         raise ImportError("libefvm_b200.so ABI version mismatch")
@@ -253,3 +265,68 @@ class Context:
         n = C.c_uint64()
         self._check(self.L.efvm_launch_count(self.h, C.byref(n)))
         return n.value
+
+
+class Batch:
+    """Many independent cases advanced together (efvm_batch_*)."""
+
+    def __init__(self, grids, params: abi.EfvmParams):
+        self.L = load()
+        self.n = len(grids)
+        self.shapes = [(g.ny, g.nx) for g in grids]
+        arr = (abi.EfvmGrid * self.n)(*grids)
+        h = C.c_void_p()
+        rc = self.L.efvm_batch_create(arr, self.n, C.byref(params), C.byref(h))
+        if rc != abi.OK:
+            raise EfvmError(rc, self.L.efvm_batch_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != abi.OK:
+            raise EfvmError(rc, self.L.efvm_batch_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.efvm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, k: int, u: np.ndarray) -> None:
+        ny, nx = self.shapes[k]
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        assert u.shape == (ny, nx, 5), u.shape
+        self._check(self.L.efvm_batch_upload_state(self.h, k, _dp(u), 5, 5 * nx, 1))
+
+    def download(self, k: int) -> np.ndarray:
+        ny, nx = self.shapes[k]
+        out = np.zeros((ny, nx, 5))
+        self._check(self.L.efvm_batch_download_state(self.h, k, _dp(out), 5, 5 * nx, 1))
+        return out
+
+    def solver_state(self, k: int) -> abi.EfvmSolverState:
+        s = abi.EfvmSolverState()
+        self._check(self.L.efvm_batch_get_solver_state(self.h, k, C.byref(s)))
+        return s
+
+    def run(self, t_stop, max_steps: int = 10_000_000, chunk: int = 16):
+        """Advance every case to its t_stop; returns per-case results."""
+        t = np.ascontiguousarray(np.broadcast_to(np.asarray(t_stop, dtype=np.float64), (self.n,)))
+        res = (abi.EfvmBatchCaseResult * self.n)()
+        self._check(self.L.efvm_batch_run(self.h, _dp(t), max_steps, chunk, res))
+        return list(res)
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        self._check(self.L.efvm_batch_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        self._check(self.L.efvm_batch_get_stream(self.h, C.byref(p)))
+        return int(p.value or 0)
+

@@ -315,6 +315,47 @@ int efvm_halo_unpack(efvm_ctx* ctx, int32_t side, const double* dev_buf);
  * the two the caller max-reduces the word across slabs (an integer max). */
 int efvm_wave_speed_slot(efvm_ctx* ctx, uint64_t** dev_slot);
 
+/* ---- batches of independent cases ---------------------------------------- */
+
+/* A batch advances many independent cases (an ensemble or a parameter sweep;
+ * the reference runs one App per case) together: per RK3 step one set-up
+ * launch for all cases and one launch per stage over the strips of every
+ * running case, each case with its own grid, boundary conditions, CFL dt,
+ * clock and stop time.  All cases share one efvm_params (RK3 only); IBM
+ * cylinders are not supported in a batch. */
+typedef struct efvm_batch efvm_batch;
+
+typedef struct {
+    int64_t steps;         /* whole steps this run took */
+    double time;           /* the case's clock at the end */
+    double completion_ms;  /* device time from the start of the run to the set-up that stopped the case;
+                              -1 if it did not stop */
+    int32_t nonphysical;   /* non-physical state flags (as efvm_get_solver_state reports) */
+    int32_t finished;      /* 1 if the case reached its stop time */
+} efvm_batch_case_result;
+
+/* n_cases grids (each as for efvm_create) sharing `params`. */
+int efvm_batch_create(const efvm_grid* grids, int32_t n_cases, const efvm_params* params, efvm_batch** out);
+int efvm_batch_destroy(efvm_batch* batch);
+/* Message of the last failed batch call (batch may be NULL). */
+const char* efvm_batch_last_error(const efvm_batch* batch);
+/* State of case `k`, strided as for efvm_upload_state / efvm_download_state. */
+int efvm_batch_upload_state(efvm_batch* batch, int32_t k, const double* base, int64_t stride_i, int64_t stride_j,
+                            int64_t stride_var);
+int efvm_batch_download_state(efvm_batch* batch, int32_t k, double* base, int64_t stride_i, int64_t stride_j,
+                              int64_t stride_var);
+int efvm_batch_get_solver_state(efvm_batch* batch, int32_t k, efvm_solver_state* out);
+/* Advance every case by whole RK3 steps until its clock reaches t_stop[k] (the
+ * time loop of examples/*: while t < t_final, three app.run() per step) or
+ * max_steps steps have run.  Finished cases leave the launch table every
+ * `chunk` steps (<= 0: 16).  results (may be NULL) receives one entry per case.
+ * Returns EFVM_ERR_NONPHYSICAL if any case went non-physical. */
+int efvm_batch_run(efvm_batch* batch, const double* t_stop, int64_t max_steps, int64_t chunk,
+                   efvm_batch_case_result* results);
+int efvm_batch_launch_count(efvm_batch* batch, uint64_t* out);
+/* The CUDA stream the batch launches on (a cudaStream_t). */
+int efvm_batch_get_stream(efvm_batch* batch, void** stream);
+
 /* ---- CFL time step without any allocation -------------------------------- */
 
 /* Rows of scratch that efvm_cfl_dt_noalloc keeps in static device memory. */

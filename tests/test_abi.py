@@ -43,16 +43,18 @@ def test_struct_layouts_match_the_header(tmp_path):
     probe = tmp_path / "probe.c"
     probe.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "efvm.h"\n'
-        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
+        "int main(void){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
         "sizeof(efvm_bc),sizeof(efvm_grid),sizeof(efvm_params),sizeof(efvm_solver_state),"
         "sizeof(efvm_cylinder),sizeof(efvm_vortex),sizeof(efvm_step_info),"
-        "offsetof(efvm_params,body_force_x),offsetof(efvm_grid,bc));return 0;}\n")
+        "offsetof(efvm_params,body_force_x),offsetof(efvm_grid,bc),"
+        "sizeof(efvm_batch_case_result),offsetof(efvm_batch_case_result,finished));return 0;}\n")
     exe = tmp_path / "probe"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(probe), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     want = [C.sizeof(abi.EfvmBC), C.sizeof(abi.EfvmGrid), C.sizeof(abi.EfvmParams), C.sizeof(abi.EfvmSolverState),
             C.sizeof(abi.EfvmCylinder), C.sizeof(abi.EfvmVortex), C.sizeof(abi.EfvmStepInfo),
-            abi.EfvmParams.body_force_x.offset, abi.EfvmGrid.bc.offset]
+            abi.EfvmParams.body_force_x.offset, abi.EfvmGrid.bc.offset,
+            C.sizeof(abi.EfvmBatchCaseResult), abi.EfvmBatchCaseResult.finished.offset]
     assert got == want
 
 

@@ -1,0 +1,83 @@
+"""Batches of independent cases (efvm_batch_*) against the same cases run one
+context at a time: same step counts and clocks, and the same states (the batch
+stage kernel runs the single-case strip code over a table of tiles)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from dev_field_efvm_b200 import abi, cases
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def small_batch(precision):
+    return cases.batch_cases(n_cases=8, seed=7, n_min=32, n_max=128, t_vortex=0.5, t_riemann=0.03,
+                             precision=precision)
+
+
+@pytest.mark.parametrize("precision,tol", [(abi.PREC_FP64, 1e-12), (abi.PREC_FP32_FLUX, 1e-12)])
+def test_batch_matches_single_contexts(precision, tol):
+    from dev_field_efvm_b200.device import Batch, Context
+
+    grids, params, states, t_stop, kinds = small_batch(precision)
+    b = Batch(grids, params)
+    for k, u in enumerate(states):
+        b.upload(k, u)
+    res = b.run(t_stop, chunk=4)
+    exact = 0
+    for k, (g, u) in enumerate(zip(grids, states)):
+        c = Context(g, params)
+        c.upload(u)
+        c.run_until(float(t_stop[k]))
+        s = c.solver_state()
+        assert res[k].finished == 1 and res[k].nonphysical == 0
+        assert res[k].steps == s.step, (k, kinds[k], res[k].steps, s.step)
+        assert abs(res[k].time - s.time) <= 1e-12 * s.time
+        ub, uc = b.download(k), c.download()
+        exact += int(np.array_equal(ub, uc))
+        assert rel(ub, uc) <= tol, (k, kinds[k], rel(ub, uc))
+        c.close()
+    print(f"{exact} of {len(grids)} cases bit-identical to their single-context runs")
+
+
+def test_chunking_does_not_change_results_and_completion_is_ordered():
+    from dev_field_efvm_b200.device import Batch
+
+    grids, params, states, t_stop, kinds = small_batch(abi.PREC_FP32_FLUX)
+    out = []
+    for chunk in (1, 1000):
+        b = Batch(grids, params)
+        for k, u in enumerate(states):
+            b.upload(k, u)
+        res = b.run(t_stop, chunk=chunk)
+        out.append(([b.download(k) for k in range(len(grids))], res))
+        b.close()
+    (ua, ra), (ub, rb) = out
+    for k in range(len(grids)):
+        assert np.array_equal(ua[k], ub[k])
+        assert ra[k].steps == rb[k].steps
+    # with chunk 1 the table shrinks as cases finish; completion follows step count
+    order = np.argsort([r.steps for r in ra])
+    comp = np.array([ra[k].completion_ms for k in order])
+    assert np.all(comp > 0) and np.all(np.diff(comp) >= -1e-3)
+
+
+def test_batch_reports_nonphysical_case():
+    from dev_field_efvm_b200.device import Batch, EfvmError
+
+    grids, params, states, t_stop, kinds = small_batch(abi.PREC_FP64)
+    bad = states[1].copy()
+    bad[3, 3, 0] = -1.0
+    b = Batch(grids, params)
+    for k, u in enumerate(states):
+        b.upload(k, bad if k == 1 else u)
+    with pytest.raises(EfvmError) as e:
+        b.run(t_stop)
+    assert e.value.code == abi.ERR_NONPHYSICAL
+    s = b.solver_state(0)
+    assert s.time >= t_stop[0]  # the other cases ran to their stop time
