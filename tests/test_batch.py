@@ -20,8 +20,12 @@ def small_batch(precision):
                              precision=precision)
 
 
-@pytest.mark.parametrize("precision,tol", [(abi.PREC_FP64, 1e-12), (abi.PREC_FP32_FLUX, 1e-12)])
-def test_batch_matches_single_contexts(precision, tol):
+# FP64: the batch kernel reproduces the single-case kernel to 1e-12 (in practice
+# bit for bit).  FP32 fluxes: the two kernels are separate compilations of the
+# same code, whose FP32 rounding (multiply-add contraction) may differ; the
+# difference stays at FP32 level (state 1e-5, clock 1e-6 relative).
+@pytest.mark.parametrize("precision,tol,ttol", [(abi.PREC_FP64, 1e-12, 1e-12), (abi.PREC_FP32_FLUX, 1e-5, 1e-6)])
+def test_batch_matches_single_contexts(precision, tol, ttol):
     from dev_field_efvm_b200.device import Batch, Context
 
     grids, params, states, t_stop, kinds = small_batch(precision)
@@ -37,7 +41,7 @@ def test_batch_matches_single_contexts(precision, tol):
         s = c.solver_state()
         assert res[k].finished == 1 and res[k].nonphysical == 0
         assert res[k].steps == s.step, (k, kinds[k], res[k].steps, s.step)
-        assert abs(res[k].time - s.time) <= 1e-12 * s.time
+        assert abs(res[k].time - s.time) <= ttol * s.time
         ub, uc = b.download(k), c.download()
         exact += int(np.array_equal(ub, uc))
         assert rel(ub, uc) <= tol, (k, kinds[k], rel(ub, uc))
