@@ -26,7 +26,7 @@ EXPORTS = (
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
     "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
-    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_cfl_dt_noalloc",
+    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_nn_gemm_bf16", "efvm_cfl_dt_noalloc",
 )
 
 
@@ -84,6 +84,7 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_batch_run.argtypes = [vp, dp, i64, i64, C.POINTER(abi.EfvmBatchCaseResult)]
     L.efvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_batch_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.efvm_nn_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp]
     L.efvm_cfl_dt_noalloc.argtypes = [vp, vp, vp, vp, i64, C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), vp, vp]
     if L.efvm_abi_version() != abi.ABI_VERSION:
         raise ImportError("libefvm_b200.so ABI version mismatch")

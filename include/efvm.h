@@ -356,6 +356,16 @@ int efvm_batch_launch_count(efvm_batch* batch, uint64_t* out);
 /* The CUDA stream the batch launches on (a cudaStream_t). */
 int efvm_batch_get_stream(efvm_batch* batch, void** stream);
 
+/* ---- learned flux correction: BF16 tensor-core kernels -------------------- */
+
+/* D[m x n] = A[m x k] * B[n x k]^T with BF16 A and B (device pointers, row-major,
+ * k contiguous) and FP32 D, on the tensor cores (tcgen05, FP32 accumulation in
+ * tensor memory): the GEMM tile the correction network is built from, exposed
+ * so that it can be checked against a CPU product.  m a multiple of 128; n and
+ * k multiples of 16 in [16, 256].  Synchronous.  No counterpart in the
+ * reference (the learned correction is this library's addition). */
+int efvm_nn_gemm_bf16(const uint16_t* a, const uint16_t* b, float* d, int32_t m, int32_t n, int32_t k, void* stream);
+
 /* ---- CFL time step without any allocation -------------------------------- */
 
 /* Rows of scratch that efvm_cfl_dt_noalloc keeps in static device memory. */
