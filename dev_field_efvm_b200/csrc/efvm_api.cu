@@ -47,6 +47,12 @@ struct efvm_ctx {
     bool geom_dirty = false;
     std::vector<double> cyl_host;  // cx, cy, r per body
     double stagnant[5] = {0, 0, 0, 0, 0};  // MaskConsts.stagnant
+    // learned face-flux correction (efvm_set_flux_correction)
+    efvm_nn* nn = nullptr;
+    float* corr = nullptr;               // [2][4][ny][nx]
+    unsigned long long* fallbacks = nullptr;
+    float sensor = 0.f;
+    uint64_t corr_faces = 0;
     double ambient[5] = {0, 0, 0, 0, 0};   // MaskConsts.ambient
     double* cyl_dev = nullptr;
     IbmGhostDev* ghosts_dev = nullptr;
@@ -273,7 +279,11 @@ int prologue(efvm_ctx* c) {
 }
 
 void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, bool pdl = true) {
+    if (c->nn)  // the learned corrections of this stage's input
+        c->launches += nn_forward_padded(c->nn, uin, c->g.plane, c->g.pitch, c->g.nx, c->g.ny, c->corr, c->sensor,
+                                         c->fallbacks, S(c));
     StageArgs a{};
+    a.corr = c->nn ? c->corr : nullptr;
     a.g = c->g;
     a.ph = c->ph;
     a.uin = uin;
@@ -567,6 +577,8 @@ int efvm_destroy(efvm_ctx* c) {
     cudaFree(c->force_partials);
     cudaFree(c->force_counter);
     cudaFree(c->history);
+    cudaFree(c->corr);
+    cudaFree(c->fallbacks);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return EFVM_OK;
@@ -645,6 +657,44 @@ int efvm_set_solver_state(efvm_ctx* c, const efvm_solver_state* in) {
     return EFVM_OK;
 }
 
+int efvm_set_flux_correction(efvm_ctx* c, efvm_nn* nn, float sensor) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (!nn) {
+        c->nn = nullptr;
+        c->graph_valid = false;
+        return EFVM_OK;
+    }
+    if (!c->ph.periodic_x || !c->ph.periodic_y || has_halo(c) || c->ibm)
+        return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction needs a periodic grid without IBM or slabs");
+    if (c->params.reconstruction != EFVM_RECON_MUSCL || c->params.flux_scheme != EFVM_FLUX_HLLC)
+        return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction runs with MUSCL + HLLC");
+    if (((long long)c->g.nx * c->g.ny) % 64 || c->g.nx < 5 || c->g.ny < 5)
+        return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction needs nx*ny a multiple of 64 and nx, ny >= 5");
+    if (!c->corr) {
+        CUDA_TRY(c, cudaMalloc(&c->corr, 8ull * c->g.nx * c->g.ny * sizeof(float)));
+        CUDA_TRY(c, cudaMalloc(&c->fallbacks, sizeof(unsigned long long)));
+    }
+    CUDA_TRY(c, cudaMemsetAsync(c->fallbacks, 0, sizeof(unsigned long long), S(c)));
+    if (nn_prepare_launches()) return fail(c, EFVM_ERR_CUDA, "flux correction: kernel attributes");
+    c->nn = nn;
+    c->sensor = sensor;
+    c->corr_faces = 0;
+    c->graph_valid = false;
+    return EFVM_OK;
+}
+
+int efvm_correction_stats(efvm_ctx* c, uint64_t* faces, uint64_t* fallbacks) {
+    if (!c || !faces || !fallbacks) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    unsigned long long fb = 0;
+    if (c->fallbacks) {
+        CUDA_TRY(c, cudaMemcpyAsync(&fb, c->fallbacks, sizeof(fb), cudaMemcpyDeviceToHost, S(c)));
+        CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    }
+    *faces = c->corr_faces;
+    *fallbacks = fb;
+    return EFVM_OK;
+}
+
 int efvm_prepare(efvm_ctx* c) {
     if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     if (c->control_dirty) sync_control(c, 0, 0.0, 0);
@@ -705,6 +755,7 @@ int efvm_substep(efvm_ctx* c) {
         double* in = c->U[s];
         double* outb = c->U[(s + 1) % 3];
         enqueue_substage(c, s, in, outb, s == 0);
+        if (c->nn) c->corr_faces += 2ull * c->g.nx * c->g.ny;
         c->rk_stage = (s + 1) % 3;
     }
     CUDA_TRY(c, cudaGetLastError());
@@ -758,6 +809,7 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
         for (int64_t k = 0; k < n_steps; ++k) {
             CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, S(c)));
             c->launches += c->graph_kernels;
+            if (c->nn) c->corr_faces += 6ull * c->g.nx * c->g.ny;
             if (stop_at_t && (k + 1) % chunk == 0 && k + 1 < n_steps) {
                 DevState s;
                 rc = read_state(c, s);

@@ -144,6 +144,7 @@ struct StageArgs {
     int stage;                        // 0,1,2 for RK3; 3 = Euler
     int completes_step;               // sponge + CFL + clock in the epilogue
     int want_cfl;
+    const float* corr;                // learned face-flux corrections [2][4][ny][nx] or null
 };
 
 // ---- batches of independent cases (efvm_batch.cu) --------------------------
@@ -177,6 +178,12 @@ int launch_batch_stage(const BatchStageArgs& b, int n_tiles, bool pdl, void* str
 int launch_batch_setup(const Physics& ph, const BatchCase* cases, int n_cases, bool pdl, void* stream);
 // Write the device global timer (ns) to *out.
 int launch_clock(unsigned long long* out, void* stream);
+
+// The learned correction (efvm_nn.cu): corrections of every face of one
+// periodic context state, and the kernel attributes its launches need.
+int nn_forward_padded(const efvm_nn* h, const double* q, long long plane, int pitch, int nx, int ny, float* corr,
+                      float sensor, unsigned long long* fallbacks, void* stream);
+int nn_prepare_launches();
 
 // Validation and the device description of one case (efvm_api.cu): global rows
 // [row0, row0 + rows) of `gr`, halo sides when `slab`.  Returns a status and

@@ -288,7 +288,7 @@ constexpr int WPB = 4;     // warps per block
 // on a step's last stage, the sponge, refills the boundary ghosts of the output
 // and takes the wave-speed max for the next step's CFL dt.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, class R, class A>
+template <int SCHEME, int RECON, class R, class A, bool CORR = false>
 __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
     if (!a.st->active) return;
     const Geometry& g = a.g;
@@ -424,6 +424,19 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     acc = __dsub_rn(acc, __dmul_rn(gtv[v], g.inv_y));
                     rhs[v] = acc;
                 }
+                if constexpr (CORR) {
+                    // learned corrections of the four faces (periodic grid): the
+                    // x face on the left of a cell, the y face below it
+                    const long long n = (long long)g.nx * g.ny, c = (long long)j * g.nx + i;
+                    const long long cr = (long long)j * g.nx + (i + 1 == g.nx ? 0 : i + 1);
+                    const long long ct = (long long)(j + 1 == g.ny ? 0 : j + 1) * g.nx + i;
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const float* cx = a.corr + v * n;
+                        const float* cy = a.corr + (4 + v) * n;
+                        rhs[v] += ((double)cx[c] - (double)cx[cr]) * g.inv_x + ((double)cy[c] - (double)cy[ct]) * g.inv_y;
+                    }
+                }
                 const bool ibm = a.mask != nullptr;
                 const bool solid = ibm && a.mask[o];
                 if (ph.viscous && !solid) {
@@ -523,10 +536,10 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
     }
 }
 
-template <int SCHEME, int RECON, class R, int MINB>
+template <int SCHEME, int RECON, class R, int MINB, bool CORR = false>
 __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
     pdl_wait_then_release();
-    stage_strip<SCHEME, RECON, R>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5), blockIdx.y);
+    stage_strip<SCHEME, RECON, R, StageArgs, CORR>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5), blockIdx.y);
 }
 
 // The stage arguments of one batch case, with its geometry and physics in the
@@ -541,6 +554,7 @@ struct BatchView {
     const double* __restrict__ yw;
     DevState* st;
     int stage, completes_step, want_cfl;
+    const float* corr;
 };
 
 // The same stage over a batch of independent cases, one warp per tile: warp w
@@ -556,7 +570,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) batch_stage_kernel(BatchStageA
     const BatchCase& c = b.cases[t.x];
     // the case's geometry and physics are read in place from the case table
     const BatchView v{c.g, c.ph, c.U[b.in_buf], c.U[0], c.U[b.out_buf], nullptr, c.yw, c.st,
-                      b.stage, b.completes_step, b.want_cfl};
+                      b.stage, b.completes_step, b.want_cfl, nullptr};
     stage_strip<SCHEME, RECON, R>(v, c.rows, t.y, t.z);
 }
 
@@ -1114,6 +1128,16 @@ static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
 
 int launch_stage(const StageArgs& a, bool pdl, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
+    if (a.corr) {  // the learned correction runs with MUSCL + HLLC (checked when it is attached)
+        const int rows = rows_per_warp(a.g.nx, a.g.ny, a.ph.precision == EFVM_PREC_FP32_FLUX ? 8 : 5);
+        dim3 grid((stage_strips(a.g.nx) + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
+        if (a.ph.precision == EFVM_PREC_FP32_FLUX)
+            launch_k(stage_kernel<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, float, 8, true>, grid, dim3(32 * WPB), s, pdl, a, rows);
+        else
+            launch_k(stage_kernel<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, double, 5, true>, grid, dim3(32 * WPB), s, pdl, a,
+                     rows);
+        return 1;
+    }
     if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_r<float>(a, pdl, s);
     else launch_stage_r<double>(a, pdl, s);
     return 1;

@@ -26,7 +26,9 @@ EXPORTS = (
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
     "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
-    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_nn_gemm_bf16", "efvm_cfl_dt_noalloc",
+    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_nn_gemm_bf16", "efvm_nn_param_count", "efvm_nn_create",
+    "efvm_nn_destroy", "efvm_nn_get_params", "efvm_nn_set_params", "efvm_nn_get_scale", "efvm_nn_forward",
+    "efvm_nn_loss_grad", "efvm_nn_adam", "efvm_set_flux_correction", "efvm_correction_stats", "efvm_cfl_dt_noalloc",
 )
 
 
@@ -85,6 +87,18 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_batch_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_nn_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp]
+    L.efvm_nn_param_count.restype = C.c_int
+    L.efvm_nn_create.argtypes = [C.c_float, C.c_float, C.c_uint64, C.POINTER(vp)]
+    L.efvm_nn_destroy.argtypes = [vp]
+    L.efvm_nn_get_params.argtypes = [vp, C.POINTER(C.c_float)]
+    L.efvm_nn_set_params.argtypes = [vp, C.POINTER(C.c_float)]
+    L.efvm_nn_get_scale.argtypes = [vp, C.POINTER(C.c_float)]
+    L.efvm_nn_forward.argtypes = [vp, vp, i32, i32, i32, vp, vp]
+    L.efvm_nn_loss_grad.argtypes = [vp, vp, vp, i32, i32, i32, C.c_double, C.c_double, C.POINTER(C.c_float), vp,
+                                    C.POINTER(C.c_double), vp]
+    L.efvm_nn_adam.argtypes = [vp, C.c_float, vp]
+    L.efvm_set_flux_correction.argtypes = [vp, vp, C.c_float]
+    L.efvm_correction_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.efvm_cfl_dt_noalloc.argtypes = [vp, vp, vp, vp, i64, C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), vp, vp]
     if L.efvm_abi_version() != abi.ABI_VERSION:
         raise ImportError("libefvm_b200.so ABI version mismatch")
@@ -156,6 +170,16 @@ class Context:
 
     def substep(self) -> None:
         self._check(self.L.efvm_substep(self.h))
+
+    # ---- learned flux correction ----
+    def set_flux_correction(self, net, sensor: float = 0.2) -> None:
+        self._check(self.L.efvm_set_flux_correction(self.h, net.h if net is not None else None, sensor))
+        self._net = net  # keep the network alive while attached
+
+    def correction_stats(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self.L.efvm_correction_stats(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     # ---- slabs (efvm_create_slab) ----
     def prepare(self) -> None:
@@ -330,4 +354,65 @@ class Batch:
         p = C.c_void_p()
         self._check(self.L.efvm_batch_get_stream(self.h, C.byref(p)))
         return int(p.value or 0)
+
+
+class FluxNet:
+    """The learned face-flux correction network (efvm_nn_*).  States and
+    residuals are device tensors (torch, float64, [batch, 4, ny, nx])."""
+
+    def __init__(self, out_scale: float, gamma: float = 1.4, seed: int = 0):
+        self.L = load()
+        self.P = self.L.efvm_nn_param_count()
+        h = C.c_void_p()
+        rc = self.L.efvm_nn_create(out_scale, gamma, seed, C.byref(h))
+        if rc != abi.OK:
+            raise EfvmError(rc, self.L.efvm_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc: int) -> None:
+        if rc != abi.OK:
+            raise EfvmError(rc, self.L.efvm_last_error(None).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.efvm_nn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.P, dtype=np.float32)
+        self._check(self.L.efvm_nn_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.P
+        self._check(self.L.efvm_nn_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def out_scale(self) -> float:
+        v = C.c_float()
+        self._check(self.L.efvm_nn_get_scale(self.h, C.byref(v)))
+        return float(v.value)
+
+    def forward(self, states, corr) -> None:
+        b, _, ny, nx = states.shape
+        self._check(self.L.efvm_nn_forward(self.h, C.c_void_p(states.data_ptr()), b, nx, ny,
+                                           C.c_void_p(corr.data_ptr()), None))
+
+    def loss_grad(self, states, resid, dx: float, dy: float, w, grad=None) -> float:
+        b, _, ny, nx = states.shape
+        wv = (C.c_float * 4)(*[float(x) for x in w])
+        loss = C.c_double()
+        gp = C.c_void_p(grad.data_ptr()) if grad is not None else None
+        self._check(self.L.efvm_nn_loss_grad(self.h, C.c_void_p(states.data_ptr()), C.c_void_p(resid.data_ptr()), b,
+                                             nx, ny, dx, dy, wv, gp, C.byref(loss), None))
+        return loss.value
+
+    def adam(self, lr: float) -> None:
+        self._check(self.L.efvm_nn_adam(self.h, lr, None))
 

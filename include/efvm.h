@@ -366,6 +366,46 @@ int efvm_batch_get_stream(efvm_batch* batch, void** stream);
  * reference (the learned correction is this library's addition). */
 int efvm_nn_gemm_bf16(const uint16_t* a, const uint16_t* b, float* d, int32_t m, int32_t n, int32_t k, void* stream);
 
+/* The correction network (no counterpart in the reference).  Per face, the
+ * 5 x 5 stencil of primitive variables (rho - 1, normal and tangential
+ * velocity, p - 1) in the face's frame feeds three layers (100 -> 32 -> 32 -> 4,
+ * relu) whose output times out_scale is added to that face's flux, so the
+ * correction is conservative.  BF16 weights on the tensor cores, FP32 biases
+ * and accumulation.  Parameters are FP32, flat:
+ * W1[32][112] (columns >= 100 unused), W2[32][32], W3[4][32], b1[32], b2[32], b3[4]. */
+typedef struct efvm_nn efvm_nn;
+
+int efvm_nn_param_count(void);
+/* Seeded initial weights (He normal, a near-zero output layer, zero biases). */
+int efvm_nn_create(float out_scale, float gamma, uint64_t seed, efvm_nn** out);
+int efvm_nn_destroy(efvm_nn* nn);
+int efvm_nn_get_params(efvm_nn* nn, float* host_params);
+int efvm_nn_set_params(efvm_nn* nn, const float* host_params);
+int efvm_nn_get_scale(efvm_nn* nn, float* out_scale);
+/* Corrections of every face of `batch` periodic states (device, conserved FP64,
+ * [batch][4][ny][nx], rho, rho_u, rho_v, rho_e) into corr (device FP32,
+ * [batch][2][4][ny][nx]: x face on the left of a cell, then y face below it;
+ * grid-frame components).  nx*ny a multiple of 64.  Synchronous. */
+int efvm_nn_forward(efvm_nn* nn, const double* states, int32_t batch, int32_t nx, int32_t ny, float* corr,
+                    void* stream);
+/* Loss and gradient on a batch: per cell e = resid + div(corr), the loss is
+ * sum_v w[v] * mean(e_v^2), and resid (device FP64, [batch][4][ny][nx]) is the
+ * coarse-step residual (target - plain step) / dt.  The gradient (P floats)
+ * goes to grad_out (device, may be NULL) and to the network's own buffer for
+ * efvm_nn_adam; the loss to *loss (host, may be NULL).  Synchronous. */
+int efvm_nn_loss_grad(efvm_nn* nn, const double* states, const double* resid, int32_t batch, int32_t nx, int32_t ny,
+                      double dx, double dy, const float w[4], float* grad_out, double* loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999) with the gradient of the last efvm_nn_loss_grad. */
+int efvm_nn_adam(efvm_nn* nn, float lr, void* stream);
+/* Attach a network to a context (periodic in x and y, MUSCL + HLLC, no IBM,
+ * nx*ny a multiple of 64): every stage then adds its corrections to the face
+ * fluxes.  A face keeps the plain flux where the sensor fires: the pressures of
+ * its two cells differ by more than sensor * min(p), or rho or p is not
+ * positive.  NULL detaches.  The network must outlive its use. */
+int efvm_set_flux_correction(efvm_ctx* ctx, efvm_nn* nn, float sensor);
+/* Faces evaluated and faces that fell back to the plain flux since attach. */
+int efvm_correction_stats(efvm_ctx* ctx, uint64_t* faces, uint64_t* fallbacks);
+
 /* ---- CFL time step without any allocation -------------------------------- */
 
 /* Rows of scratch that efvm_cfl_dt_noalloc keeps in static device memory. */
