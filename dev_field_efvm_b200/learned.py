@@ -192,7 +192,7 @@ def train(states, resid, dt_c: float, epochs: int, batch: int = 32, lr: float = 
             steps += 1
             losses.append(loss)
         hist.append(float(np.mean(losses)))
-        log(f"epoch {ep}: loss {hist[-1]:.4e} (relative to the uncorrected loss 4.0)")
+        log(f"epoch {ep}: loss {hist[-1]:.4e} ({hist[-1] / hist[0]:.4f} of the first epoch's)")
     return net, hist, {"w": w.tolist(), "out_scale": out_scale}
 
 
@@ -246,7 +246,7 @@ def main() -> None:
     ap.add_argument("--eval", type=int, default=200, help="held-out trajectories")
     ap.add_argument("--k-train", type=int, default=4, help="coarse steps per training trajectory")
     ap.add_argument("--k-eval", type=int, default=16, help="coarse steps of the evaluation runs")
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--out", default=None)
     ap.add_argument("--save", default=None, help="write the trained parameters (.npz)")
     args = ap.parse_args()
