@@ -240,6 +240,19 @@ def evaluate(net, seeds, dt_c: float, k_steps: int, sensor: float = 0.2):
     return summary, res
 
 
+MODEL = __import__("os").path.join(__import__("os").path.dirname(__file__), "models", "flux_net_vortex64.npz")
+
+
+def load_trained(path: str = MODEL):
+    """The network trained by `main` (2000 trajectories, 40 epochs), and its coarse dt."""
+    from .device import FluxNet
+
+    d = np.load(path)
+    net = FluxNet(out_scale=float(d["out_scale"]), gamma=GAMMA)
+    net.set_params(d["params"])
+    return net, float(d["dt_coarse"])
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", type=int, default=2000, help="training trajectories")
