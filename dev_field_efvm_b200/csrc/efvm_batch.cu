@@ -13,8 +13,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "efvm_internal.h"
@@ -41,6 +45,9 @@ struct efvm_batch {
     int n_tiles = 0;
     std::vector<char> fresh;         // state uploaded since the last run: CFL pass and ghost fill due
     std::vector<char> active;
+    bool autotune = true;              // tune rows per warp per size bucket on the first run
+    bool tuned = false;
+    std::array<int, 4> bucket_rows{{0, 0, 0, 0}};  // 0 = the default heuristic
     cudaGraphExec_t graph = nullptr;
     unsigned long long* clock_d = nullptr;
     uint64_t launches = 0;
@@ -102,6 +109,26 @@ int build_tiles(efvm_batch* b) {
     return EFVM_OK;
 }
 
+// ---- the autotuner -----------------------------------------------------------
+// Rows per warp is the one tiling choice of the stage kernel that depends on the
+// case size: more rows amortise each strip's first y face, fewer rows give more
+// warps.  Cases are grouped in size buckets (cells < 64^2, < 128^2, < 256^2,
+// larger); for each bucket present the tuner times one batch step with 2, 4 and
+// 8 rows and keeps the fastest, on a copy of the states (restored afterwards, so
+// tuning changes no result).  Choices are cached per process for the device, its
+// SM count, the numerical method and the set of buckets present.
+constexpr int N_BUCKETS = 4;
+constexpr int ROW_CHOICES[3] = {2, 4, 8};
+
+int size_bucket(const Geometry& g) {
+    const long long c = (long long)g.nx * g.ny;
+    return c < 64 * 64 ? 0 : c < 128 * 128 ? 1 : c < 256 * 256 ? 2 : 3;
+}
+
+using TuneKey = std::tuple<int, int, int, int, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, std::array<int, 4>> g_tune_cache;
+
 // One RK3 step of every active case: set-up, then the three stages.
 void enqueue_step(efvm_batch* b) {
     b->launches += launch_batch_setup(b->ph, b->cases_d, b->n, true, b->stream);
@@ -136,6 +163,85 @@ int capture(efvm_batch* b) {
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return bfail(b, EFVM_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
     return EFVM_OK;
+}
+
+// Rows of every case from the per-bucket choice (0 = default), uploaded.
+int apply_rows(efvm_batch* b) {
+    const bool fp32 = b->params.precision == EFVM_PREC_FP32_FLUX;
+    for (int k = 0; k < b->n; ++k) {
+        const int r = b->bucket_rows[size_bucket(b->g[k])];
+        b->cases[k].rows = r > 0 ? r : std::min(stage_rows(b->g[k].nx, b->g[k].ny, fp32), 8);
+    }
+    BATCH_TRY(b, cudaMemcpyAsync(b->cases_d, b->cases.data(), b->n * sizeof(BatchCase), cudaMemcpyHostToDevice,
+                                 b->stream));
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    return EFVM_OK;
+}
+
+int tune(efvm_batch* b) {
+    int present = 0;
+    for (int k = 0; k < b->n; ++k) present |= 1 << size_bucket(b->g[k]);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    const TuneKey key{b->device, sms, b->params.precision, b->params.flux_scheme * 2 + b->params.reconstruction,
+                      b->params.limiter, present};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            b->bucket_rows = it->second;
+            return apply_rows(b);
+        }
+    }
+    // work on the live buffers, then put states and clocks back
+    size_t pool_bytes = 0;
+    for (int k = 0; k < b->n; ++k) pool_bytes += 3 * (((size_t)4 * b->g[k].plane + 31) / 32 * 32) * sizeof(double);
+    double* backup = nullptr;
+    BATCH_TRY(b, cudaMalloc(&backup, pool_bytes));
+    std::vector<DevState> saved;
+    int rc = read_states(b, saved);
+    if (rc) return rc;
+    BATCH_TRY(b, cudaMemcpyAsync(backup, b->pool, pool_bytes, cudaMemcpyDeviceToDevice, b->stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int bucket = 0; bucket < N_BUCKETS && rc == EFVM_OK; ++bucket) {
+        if (!(present & (1 << bucket))) continue;
+        float best_ms = 1e30f;
+        int best = ROW_CHOICES[0];
+        for (int r : ROW_CHOICES) {
+            b->bucket_rows[bucket] = r;
+            if ((rc = apply_rows(b)) || (rc = build_tiles(b)) || (rc = capture(b))) break;
+            cudaGraphLaunch(b->graph, b->stream);  // warm-up
+            cudaEventRecord(e0, b->stream);
+            for (int i = 0; i < 2; ++i) cudaGraphLaunch(b->graph, b->stream);
+            cudaEventRecord(e1, b->stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) {
+                rc = bfail(b, EFVM_ERR_CUDA, std::string("batch autotune: ") + cudaGetErrorString(e));
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = r;
+            }
+        }
+        b->bucket_rows[bucket] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemcpyAsync(b->pool, backup, pool_bytes, cudaMemcpyDeviceToDevice, b->stream);
+    const int rc2 = write_states(b, saved);
+    cudaFree(backup);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache[key] = b->bucket_rows;
+    }
+    return apply_rows(b);
 }
 
 }  // namespace
@@ -329,6 +435,11 @@ int efvm_batch_run(efvm_batch* b, const double* t_stop, int64_t max_steps, int64
     }
     rc = write_states(b, s);
     if (rc) return rc;
+    if (b->autotune && !b->tuned) {
+        rc = tune(b);
+        if (rc) return rc;
+        b->tuned = true;
+    }
     b->launches += launch_clock(b->clock_d, b->stream);
     rc = build_tiles(b);
     if (rc) return rc;
@@ -381,6 +492,23 @@ int efvm_batch_run(efvm_batch* b, const double* t_stop, int64_t max_steps, int64
 int efvm_batch_launch_count(efvm_batch* b, uint64_t* out) {
     if (!b || !out) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
     *out = b->launches;
+    return EFVM_OK;
+}
+
+int efvm_batch_set_autotune(efvm_batch* b, int32_t enable) {
+    if (!b) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
+    b->autotune = enable != 0;
+    if (!b->autotune) {
+        b->bucket_rows = {{0, 0, 0, 0}};
+        b->tuned = false;
+        return apply_rows(b);
+    }
+    return EFVM_OK;
+}
+
+int efvm_batch_get_rows(efvm_batch* b, int32_t rows[4]) {
+    if (!b || !rows) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
+    for (int i = 0; i < 4; ++i) rows[i] = b->bucket_rows[i];
     return EFVM_OK;
 }
 

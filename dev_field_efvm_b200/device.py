@@ -26,7 +26,8 @@ EXPORTS = (
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
     "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
-    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_nn_gemm_bf16", "efvm_nn_param_count", "efvm_nn_create",
+    "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
+    "efvm_nn_gemm_bf16", "efvm_nn_param_count", "efvm_nn_create",
     "efvm_nn_destroy", "efvm_nn_get_params", "efvm_nn_set_params", "efvm_nn_get_scale", "efvm_nn_forward",
     "efvm_nn_loss_grad", "efvm_nn_adam", "efvm_set_flux_correction", "efvm_correction_stats", "efvm_cfl_dt_noalloc",
 )
@@ -86,6 +87,8 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_batch_run.argtypes = [vp, dp, i64, i64, C.POINTER(abi.EfvmBatchCaseResult)]
     L.efvm_batch_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_batch_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.efvm_batch_set_autotune.argtypes = [vp, i32]
+    L.efvm_batch_get_rows.argtypes = [vp, C.POINTER(C.c_int32)]
     L.efvm_nn_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp]
     L.efvm_nn_param_count.restype = C.c_int
     L.efvm_nn_create.argtypes = [C.c_float, C.c_float, C.c_uint64, C.POINTER(vp)]
@@ -354,6 +357,14 @@ class Batch:
         p = C.c_void_p()
         self._check(self.L.efvm_batch_get_stream(self.h, C.byref(p)))
         return int(p.value or 0)
+
+    def set_autotune(self, enable: bool) -> None:
+        self._check(self.L.efvm_batch_set_autotune(self.h, int(enable)))
+
+    def rows(self):
+        r = (C.c_int32 * 4)()
+        self._check(self.L.efvm_batch_get_rows(self.h, r))
+        return list(r)
 
 
 class FluxNet:

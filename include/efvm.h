@@ -355,6 +355,14 @@ int efvm_batch_run(efvm_batch* batch, const double* t_stop, int64_t max_steps, i
 int efvm_batch_launch_count(efvm_batch* batch, uint64_t* out);
 /* The CUDA stream the batch launches on (a cudaStream_t). */
 int efvm_batch_get_stream(efvm_batch* batch, void** stream);
+/* Autotuning (on by default): on the first efvm_batch_run the batch times one
+ * step with 2, 4 and 8 rows per warp for each case-size bucket present (cells
+ * < 64^2, < 128^2, < 256^2, larger) on a copy of the states, keeps the fastest,
+ * and caches the choice per process for the device, the method and the buckets.
+ * Tuning changes no result.  enable = 0 returns to the built-in heuristic. */
+int efvm_batch_set_autotune(efvm_batch* batch, int32_t enable);
+/* Rows per warp chosen for the four buckets (0 = heuristic / not tuned yet). */
+int efvm_batch_get_rows(efvm_batch* batch, int32_t rows[4]);
 
 /* ---- learned flux correction: BF16 tensor-core kernels -------------------- */
 

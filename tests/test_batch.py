@@ -85,3 +85,25 @@ def test_batch_reports_nonphysical_case():
     assert e.value.code == abi.ERR_NONPHYSICAL
     s = b.solver_state(0)
     assert s.time >= t_stop[0]  # the other cases ran to their stop time
+
+
+def test_autotuned_rows_change_no_result():
+    """The tuner times steps on the live states and restores them: a tuned
+    batch and an untuned one end bit-identical."""
+    from dev_field_efvm_b200.device import Batch
+
+    grids, params, states, t_stop, kinds = small_batch(abi.PREC_FP64)
+    out = []
+    for tune in (True, False):
+        b = Batch(grids, params)
+        b.set_autotune(tune)
+        for k, u in enumerate(states):
+            b.upload(k, u)
+        res = b.run(t_stop)
+        out.append(([b.download(k) for k in range(len(grids))], [r.steps for r in res], b.rows()))
+        b.close()
+    (ua, sa, rows_tuned), (ub, sb, rows_plain) = out
+    assert sa == sb
+    for k in range(len(grids)):
+        assert np.array_equal(ua[k], ub[k])
+    assert any(r in (2, 4, 8) for r in rows_tuned) and rows_plain == [0, 0, 0, 0]
