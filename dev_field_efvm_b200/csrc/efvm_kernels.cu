@@ -263,7 +263,7 @@ __device__ __forceinline__ Q4<R> shfl_down_q(const Q4<R>& u, int d) {
 
 // Primitive (u, v, T) of a state (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
 __device__ __forceinline__ void prim_uvt(const U4& u, double gm1, double r_gas, double& vu, double& vv, double& t) {
-    const double inv = 1.0 / u.r;
+    const double inv = rcp_(u.r);
     vu = u.mx * inv;
     vv = u.my * inv;
     const double ke = 0.5 * u.r * (vu * vu + vv * vv);

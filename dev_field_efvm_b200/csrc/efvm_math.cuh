@@ -50,6 +50,16 @@ __device__ __forceinline__ double div_(double a, double b) {
     return fma(r, fma(-b, q, a), q);
 }
 __device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+// 1/sqrt(x) by Newton-Raphson on f(y) = 1/y^2 - x, y <- y (3/2 - x y^2 / 2),
+// seeded with the PTX approximate rsqrt.approx.ftz.f64; two iterations.
+__device__ __forceinline__ double rsqrt_(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    y = y * fma(-h * y, y, 1.5);
+    return y * fma(-h * y, y, 1.5);
+}
+__device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 
 // Gas-dynamic quantities of one face state, each computed once per face side:
 // 1/rho, normal and tangential velocity, |v|^2, pressure and sound speed
@@ -67,7 +77,8 @@ __device__ __forceinline__ Side<R> side_of(const Q4<R>& u, R gamma, R gm1) {
     s.ut = u.mt * s.inv;
     s.q = s.un * s.un + s.ut * s.ut;
     s.p = gm1 * (u.E - R(0.5) * u.r * s.q);
-    s.a = sqrt_(gamma * s.p * s.inv);
+    const R a2 = gamma * s.p * s.inv;
+    s.a = a2 * rsqrt_(a2);  // sqrt(a2); NaN for a non-physical p <= 0, which the stage flags
     return s;
 }
 
@@ -119,7 +130,9 @@ __device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R ga
     if (THORNBER) {
         const R vmax2 = fmax_(l.q, r.q);
         const R amax = fmax_(l.a, r.a);
-        const R z = (vmax2 >= amax * amax) ? R(1) : div_(sqrt_(vmax2), amax);
+        // z = min(|v|max / a_max, 1) as vmax2 / sqrt(vmax2 a_max^2): one reciprocal square root
+        const R amax2 = amax * amax;
+        const R z = (vmax2 >= amax2) ? R(1) : (vmax2 > R(0) ? vmax2 * rsqrt_(vmax2 * amax2) : R(0));
         const R avgn = R(0.5) * (l.un + r.un), avgt = R(0.5) * (l.ut + r.ut);
         const R hz = R(0.5) * z;
         const R dvn = hz * (l.un - r.un), dvt = hz * (l.ut - r.ut);
@@ -146,8 +159,11 @@ __device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R ga
     if (s_l < R(0) && (s_star >= R(0) || s_r >= R(0))) {  // one of the two star regions
         const R sK = useL ? s_l : s_r;
         const R facK = useL ? fac_l : fac_r;
-        const R rho_star = div_(facK, sK - s_star);
-        const R e_star = EK * iK + (s_star - uK) * (s_star + div_(pK, facK));
+        // rho_* = f_K / d_K and p_K / f_K from one reciprocal of f_K d_K (d_K = s_K - s_*)
+        const R dK = sK - s_star;
+        const R inv = rcp_(facK * dK);
+        const R rho_star = facK * facK * inv;
+        const R e_star = EK * iK + (s_star - uK) * (s_star + pK * dK * inv);
         f.r = f.r + sK * (rho_star - rK);
         f.mn = f.mn + sK * (rho_star * s_star - rK * uK);
         f.mt = f.mt + sK * (rho_star * tK - rK * tK);
