@@ -513,10 +513,10 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 write_ghosts(g, ph, a.uout, i, j, nw);
 
                 // non-physical state flag (rho<=0, p<=0, NaN)
-                const double pn_ = pressure_d(nw, gm1);
+                // p > 0 with rho > 0 is 2 E rho > m^2 (no division)
                 int bad = 0;
                 if (!(nw.r > 0.0)) bad |= 1;
-                if (!(pn_ > 0.0)) bad |= 2;
+                if (!(2.0 * nw.E * nw.r > nw.mx * nw.mx + nw.my * nw.my)) bad |= 2;
                 if (nw.r != nw.r || nw.mx != nw.mx || nw.my != nw.my || nw.E != nw.E) bad |= 4;
                 if (bad) atomicOr(&a.st->nonphysical, bad);
 

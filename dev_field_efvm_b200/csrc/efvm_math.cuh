@@ -179,15 +179,22 @@ __device__ __forceinline__ Q4<R> face_flux(const Q4<R>& L, const Q4<R>& Rr, R ga
     return hllc_flux<R, true>(L, Rr, gamma, gm1);
 }
 
-// minmod / monotonized_central, crates/cfd_solver/src/lib.rs:170-192
+// minmod / monotonized_central, crates/cfd_solver/src/lib.rs:170-192.  (Deciding
+// the sign test and the magnitude comparison on the bit patterns, to spare the
+// FP64 pipe, measured 4 % slower at 4096^2: the 64-bit integer work costs more.)
+template <class R>
+__device__ __forceinline__ bool opposite_or_zero(R a, R b) { return a * b <= R(0); }
+template <class R>
+__device__ __forceinline__ bool smaller_magnitude(R a, R b) { return fabs_(a) < fabs_(b); }
+
 template <class R>
 __device__ __forceinline__ R minmod(R a, R b) {
-    if (a * b <= R(0)) return R(0);
-    return fabs_(a) < fabs_(b) ? a : b;
+    if (opposite_or_zero(a, b)) return R(0);
+    return smaller_magnitude(a, b) ? a : b;
 }
 template <class R>
 __device__ __forceinline__ R monotonized_central(R a, R b) {
-    if (a * b <= R(0)) return R(0);
+    if (opposite_or_zero(a, b)) return R(0);
     const R s = a > R(0) ? R(1) : R(-1);
     return s * fmin_(fmin_(R(2) * fabs_(a), R(2) * fabs_(b)), R(0.5) * fabs_(a + b));
 }
