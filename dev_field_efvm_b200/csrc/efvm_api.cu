@@ -53,6 +53,7 @@ struct efvm_ctx {
     unsigned long long* fallbacks = nullptr;
     float sensor = 0.f;
     uint64_t corr_faces = 0;
+    double* out_fields = nullptr;        // efvm_output_fields
     double ambient[5] = {0, 0, 0, 0, 0};   // MaskConsts.ambient
     double* cyl_dev = nullptr;
     IbmGhostDev* ghosts_dev = nullptr;
@@ -211,6 +212,9 @@ int build_ibm_lists(efvm_ctx* c) {
             const double sx = px + offset * nx, sy = py + offset * ny;
             mk.valid = locate_h(g, sx, sy, mk.lo_i, mk.lo_j, mk.tx, mk.ty) ? 1 : 0;
             if (mk.valid) mk.fluid = corner_bits(mk.lo_i, mk.lo_j);
+            mk.pos[0] = px;
+            mk.pos[1] = py;
+            mk.body = b;
             markers.push_back(mk);
         }
     }
@@ -579,6 +583,7 @@ int efvm_destroy(efvm_ctx* c) {
     cudaFree(c->history);
     cudaFree(c->corr);
     cudaFree(c->fallbacks);
+    cudaFree(c->out_fields);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return EFVM_OK;
@@ -680,6 +685,108 @@ int efvm_set_flux_correction(efvm_ctx* c, efvm_nn* nn, float sensor) {
     c->sensor = sensor;
     c->corr_faces = 0;
     c->graph_valid = false;
+    return EFVM_OK;
+}
+
+int efvm_output_fields(efvm_ctx* c, double* host_out, int32_t async) {
+    if (!c || !host_out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    const size_t bytes = (size_t)7 * c->g.nx * c->g.ny * sizeof(double);
+    if (!c->out_fields) CUDA_TRY(c, cudaMalloc(&c->out_fields, bytes));
+    c->launches += launch_output_fields(c->g, c->ph, cur_buf(c), c->out_fields, S(c));
+    CUDA_TRY(c, cudaMemcpyAsync(host_out, c->out_fields, bytes, cudaMemcpyDeviceToHost, S(c)));
+    if (!async) CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    return EFVM_OK;
+}
+
+int efvm_synchronize(efvm_ctx* c) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    return EFVM_OK;
+}
+
+int efvm_write_vtk(efvm_ctx* c, const char* path) {
+    if (!c || !path) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    const int nx = c->g.nx, ny = c->g.ny;
+    const long long n = (long long)nx * ny;
+    std::vector<double> f(7 * (size_t)n);
+    int rc = efvm_output_fields(c, f.data(), 0);
+    if (rc) return rc;
+    FILE* fp = std::fopen(path, "w");
+    if (!fp) return fail(c, EFVM_ERR_INVALID_ARG, std::string("efvm_write_vtk: cannot open ") + path);
+    // fmt_e: %.10e (two or more exponent digits), non-finite values as zero
+    auto e = [&](double x) { std::fprintf(fp, "%.10e", std::isfinite(x) ? x : 0.0); };
+    std::fprintf(fp, "# vtk DataFile Version 3.0\ndev_field_efvm output\nASCII\nDATASET RECTILINEAR_GRID\n");
+    std::fprintf(fp, "DIMENSIONS %d %d %d\n", nx + 1, ny + 1, 2);
+    const int ns[3] = {nx, ny, 1};
+    const char* lab[3] = {"X", "Y", "Z"};
+    for (int a = 0; a < 3; ++a) {
+        std::fprintf(fp, "%s_COORDINATES %d double\n", lab[a], ns[a] + 1);
+        const int off = a == 1 ? c->g.j_off : 0;
+        for (int m = 0; m <= ns[a]; ++m) {
+            // face = centroid - half spacing, then the last centroid + half spacing
+            const int mm = m < ns[a] ? m : ns[a] - 1;
+            const double cc = centre_h(c->g.lo[a], c->g.h[a], mm + off);
+            e(m < ns[a] ? cc - 0.5 * c->g.h[a] : cc + 0.5 * c->g.h[a]);
+            std::fputc('\n', fp);
+        }
+    }
+    std::fprintf(fp, "CELL_DATA %lld\n", n);
+    const char* names[3] = {"density", "pressure", "temperature"};
+    for (int k = 0; k < 3; ++k) {
+        std::fprintf(fp, "SCALARS %s double 1\nLOOKUP_TABLE default\n", names[k]);
+        for (long long t = 0; t < n; ++t) {
+            e(f[k * n + t]);
+            std::fputc('\n', fp);
+        }
+    }
+    std::fprintf(fp, "VECTORS velocity double\n");
+    for (long long t = 0; t < n; ++t) {
+        e(f[3 * n + t]);
+        std::fputc(' ', fp);
+        e(f[4 * n + t]);
+        std::fputc(' ', fp);
+        e(f[5 * n + t]);
+        std::fputc('\n', fp);
+    }
+    std::fprintf(fp, "SCALARS mach double 1\nLOOKUP_TABLE default\n");
+    for (long long t = 0; t < n; ++t) {
+        e(f[6 * n + t]);
+        std::fputc('\n', fp);
+    }
+    const bool ok = std::fclose(fp) == 0;
+    if (!ok) return fail(c, EFVM_ERR_INVALID_ARG, std::string("efvm_write_vtk: write failed for ") + path);
+    return EFVM_OK;
+}
+
+int efvm_body_loads(efvm_ctx* c, int32_t n_bodies, double* out) {
+    if (!c || !out || n_bodies < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid argument");
+    if (!c->ibm) return fail(c, EFVM_ERR_INVALID_ARG, "efvm_body_loads: no cylinders are set");
+    const int nb = (int)(c->cyl_host.size() / 3);
+    if (n_bodies > nb) return fail(c, EFVM_ERR_INVALID_ARG, "efvm_body_loads: more bodies asked than cylinders set");
+    if (c->geom_dirty) {
+        int rc = prologue(c);
+        if (rc) return rc;
+    }
+    const size_t bytes = (size_t)9 * nb * sizeof(double);
+    int rc = ensure_staging(c, bytes);
+    if (rc) return rc;
+    // centres (cx, cy) after the loads in the staging buffer
+    rc = ensure_staging(c, bytes + (size_t)2 * nb * sizeof(double));
+    if (rc) return rc;
+    std::vector<double> centres(2 * nb);
+    for (int b = 0; b < nb; ++b) {
+        centres[2 * b] = c->cyl_host[3 * b];
+        centres[2 * b + 1] = c->cyl_host[3 * b + 1];
+    }
+    double* d_out = c->staging;
+    double* d_cen = c->staging + 9 * nb;
+    CUDA_TRY(c, cudaMemcpyAsync(d_cen, centres.data(), centres.size() * sizeof(double), cudaMemcpyHostToDevice, S(c)));
+    c->launches += launch_body_loads(c->g, c->ph, c->ibm_desc, cur_buf(c), d_cen, nb, c->ibm_desc.n_markers / nb,
+                                     d_out, S(c));
+    std::vector<double> all(9 * nb);
+    CUDA_TRY(c, cudaMemcpyAsync(all.data(), d_out, bytes, cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    std::copy(all.begin(), all.begin() + 9 * n_bodies, out);
     return EFVM_OK;
 }
 

@@ -110,6 +110,9 @@ struct MarkerDev {
     double tx, ty;
     int valid;
     unsigned fluid;          // FLUID_CORNER bits
+    double pos[2];           // marker position (its z is the z-cell centre)
+    int body;                // cylinder index
+    int pad;
 };
 
 struct Ibm {
@@ -219,6 +222,13 @@ int launch_check_state(const Geometry& g, const Physics& ph, const double* q, De
 // Rows j0, j0+1 (all four variables, interior columns) to buf (unpack = 0) or
 // from buf (unpack = 1); buf is [variable][row][i], 8*nx doubles.
 int launch_halo_rows(const Geometry& g, double* q, double* buf, int j0, int unpack, void* stream);
+// Per-body marker loads and torque (compute_marker_loadings_per_body): one warp
+// per body over its n_theta consecutive markers; out[9 b ..] = pressure[3],
+// viscous[3], torque[3] about (centres[2 b], centres[2 b + 1]).
+int launch_body_loads(const Geometry& g, const Physics& ph, const Ibm& ib, const double* q, const double* centres,
+                      int n_bodies, int markers_per_body, double* out, void* stream);
+// The VTK output fields (7 planes of nx*ny doubles) of a state.
+int launch_output_fields(const Geometry& g, const Physics& ph, const double* q, double* out, void* stream);
 int launch_set_control(DevState* st, int active, int stop_at_t, double t_stop, long long hist_cap, void* stream);
 
 }  // namespace efvm

@@ -1210,6 +1210,84 @@ int launch_step_setup(const Physics& ph, DevState* st, bool pdl, void* stream) {
     return 1;
 }
 
+// The output fields of write_vtk_to (crates/cfd_output/src/lib.rs:36-125) per
+// interior cell, x fastest: density, pressure, temperature, velocity (u, v, w)
+// and Mach, as 7 planes of nx*ny doubles.
+__global__ void output_fields_kernel(Geometry g, Physics ph, const double* __restrict__ q, double* __restrict__ out) {
+    const long long n = (long long)g.nx * g.ny;
+    const double gm1 = ph.gamma - 1.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t / g.nx), i = (int)(t - (long long)j * g.nx);
+        const U4 u = load4(q, g.plane, cidx(g, i, j));
+        const double p = pressure_d(u, gm1);                     // IdealGas::pressure
+        const double vu = u.mx / u.r, vv = u.my / u.r;
+        const double ke = 0.5 * u.r * (vu * vu + vv * vv);
+        const double t_ = gm1 * (u.E - ke) / u.r / ph.r_gas;     // cons_to_prim(u).t
+        const double a = sqrt(ph.gamma * p / u.r);               // sound_speed
+        out[t] = u.r;
+        out[n + t] = p;
+        out[2 * n + t] = t_;
+        out[3 * n + t] = vu;
+        out[4 * n + t] = vv;
+        out[5 * n + t] = 0.0;
+        out[6 * n + t] = sqrt(vu * vu + vv * vv) / a;
+    }
+}
+
+int launch_output_fields(const Geometry& g, const Physics& ph, const double* q, double* out, void* stream) {
+    output_fields_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(g, ph, q, out);
+    return 1;
+}
+
+// compute_marker_loadings_per_body, crates/cfd_ibm/src/lib.rs:509-562: warp b
+// sums the traction of body b's markers (lane l takes markers l, l + 32, ...),
+// then a shuffle tree (fixed order) gives the body's loads and torque.
+__global__ void body_loads_kernel(Geometry g, Physics ph, Ibm ib, const double* __restrict__ q,
+                                  const double* __restrict__ centres, int n_bodies, int per_body,
+                                  double* __restrict__ out) {
+    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= n_bodies) return;  // uniform per warp
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int m = b * per_body + lane; m < (b + 1) * per_body; m += 32) {
+        const MarkerDev mk = ib.markers[m];
+        if (!mk.valid) continue;
+        double img[5];
+        if (!sample_bilinear(g, ph, q, mk.fluid, mk.lo_i, mk.lo_j, mk.tx, mk.ty, img)) continue;
+        if (!(isfinite(img[3]) && isfinite(img[4]) && isfinite(img[1]) && isfinite(img[2]))) continue;
+        const double us[3] = {img[1] - mk.wall_velocity[0], img[2] - mk.wall_velocity[1], 0.0 - mk.wall_velocity[2]};
+        const double udotn = us[0] * mk.normal[0] + us[1] * mk.normal[1] + us[2] * mk.normal[2];
+        const double mu = viscosity(ph, img[4]);
+        double df[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double ut = us[d] - udotn * mk.normal[d];
+            const double fp = -img[3] * mk.normal[d] * mk.area;
+            const double fv = mu * ut / ib.sample_offset * mk.area;
+            acc[d] += fp;
+            acc[3 + d] += fv;
+            df[d] = fp + fv;
+        }
+        const double r[3] = {mk.pos[0] - centres[2 * b], mk.pos[1] - centres[2 * b + 1], 0.0};
+        acc[6] += r[1] * df[2] - r[2] * df[1];
+        acc[7] += r[2] * df[0] - r[0] * df[2];
+        acc[8] += r[0] * df[1] - r[1] * df[0];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+    if (lane == 0)
+        for (int k = 0; k < 9; ++k) out[9 * b + k] = acc[k];
+}
+
+int launch_body_loads(const Geometry& g, const Physics& ph, const Ibm& ib, const double* q, const double* centres,
+                      int n_bodies, int markers_per_body, double* out, void* stream) {
+    if (n_bodies <= 0) return 0;
+    body_loads_kernel<<<(n_bodies + 3) / 4, 128, 0, (cudaStream_t)stream>>>(g, ph, ib, q, centres, n_bodies,
+                                                                           markers_per_body, out);
+    return 1;
+}
+
 // Two rows of one y side to/from a contiguous buffer [variable][row][i].
 // unpack == 0: interior rows j0, j0+1 -> buf; unpack == 1: buf -> rows j0, j0+1.
 __global__ void halo_rows_kernel(Geometry g, double* q, double* buf, int j0, int unpack) {

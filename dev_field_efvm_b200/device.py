@@ -27,7 +27,7 @@ EXPORTS = (
     "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
     "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
-    "efvm_nn_gemm_bf16", "efvm_nn_param_count", "efvm_nn_create",
+    "efvm_nn_gemm_bf16", "efvm_body_loads", "efvm_output_fields", "efvm_synchronize", "efvm_write_vtk", "efvm_nn_param_count", "efvm_nn_create",
     "efvm_nn_destroy", "efvm_nn_get_params", "efvm_nn_set_params", "efvm_nn_get_scale", "efvm_nn_forward",
     "efvm_nn_loss_grad", "efvm_nn_adam", "efvm_set_flux_correction", "efvm_correction_stats", "efvm_cfl_dt_noalloc",
 )
@@ -90,6 +90,10 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_batch_set_autotune.argtypes = [vp, i32]
     L.efvm_batch_get_rows.argtypes = [vp, C.POINTER(C.c_int32)]
     L.efvm_nn_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp]
+    L.efvm_body_loads.argtypes = [vp, i32, dp]
+    L.efvm_output_fields.argtypes = [vp, dp, i32]
+    L.efvm_synchronize.argtypes = [vp]
+    L.efvm_write_vtk.argtypes = [vp, C.c_char_p]
     L.efvm_nn_param_count.restype = C.c_int
     L.efvm_nn_create.argtypes = [C.c_float, C.c_float, C.c_uint64, C.POINTER(vp)]
     L.efvm_nn_destroy.argtypes = [vp]
@@ -246,6 +250,26 @@ class Context:
     def marker_force(self) -> np.ndarray:
         out = np.zeros(6)
         self._check(self.L.efvm_marker_force(self.h, _dp(out)))
+        return out
+
+    def output_fields(self, out: np.ndarray | None = None, wait: bool = True) -> np.ndarray:
+        """(7, ny, nx): density, pressure, temperature, u, v, w, Mach.  With
+        wait=False the copy is only enqueued (call synchronize() before use)."""
+        if out is None:
+            out = np.zeros((7, self.ny, self.nx))
+        self._check(self.L.efvm_output_fields(self.h, _dp(out), 0 if wait else 1))
+        return out
+
+    def synchronize(self) -> None:
+        self._check(self.L.efvm_synchronize(self.h))
+
+    def write_vtk(self, path: str) -> None:
+        self._check(self.L.efvm_write_vtk(self.h, path.encode()))
+
+    def body_loads(self, n_bodies: int) -> np.ndarray:
+        """[n_bodies, 9]: pressure force, viscous force, torque about the centre."""
+        out = np.zeros((n_bodies, 9))
+        self._check(self.L.efvm_body_loads(self.h, n_bodies, _dp(out)))
         return out
 
     def wall_force(self) -> np.ndarray:

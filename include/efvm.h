@@ -237,6 +237,26 @@ int efvm_marker_force(efvm_ctx* ctx, double out[6]);
 /* WallForce{pressure,viscous}, the staircase estimate (crates/cfd_ibm/src/
  * lib.rs:309-395). */
 int efvm_wall_force(efvm_ctx* ctx, double out[6]);
+/* ---- output -------------------------------------------------------------- */
+/* The fields write_vtk_to writes (crates/cfd_output/src/lib.rs:36-125) for the
+ * current state, computed on the device: 7 planes of nx*ny doubles, x fastest:
+ * density, pressure, temperature, velocity u, v, w (= 0), Mach.  With async != 0
+ * the copy into host_out (pinned memory for a truly asynchronous copy) is only
+ * enqueued on the context's stream, so a solver can keep stepping; wait with
+ * efvm_synchronize before reading host_out. */
+int efvm_output_fields(efvm_ctx* ctx, double* host_out, int32_t async);
+/* Wait for everything enqueued on the context's stream. */
+int efvm_synchronize(efvm_ctx* ctx);
+/* write_vtk (crates/cfd_output/src/lib.rs:110-125): the current state as a VTK
+ * legacy ASCII RECTILINEAR_GRID file (nz = 1 cell layer), same fields, order and
+ * number format as the reference writer. */
+int efvm_write_vtk(efvm_ctx* ctx, const char* path);
+
+/* compute_marker_loadings_per_body (crates/cfd_ibm/src/lib.rs:509-562) on the
+ * current state: for each of the first n_bodies cylinders, out[9 b ..] =
+ * pressure force[3], viscous force[3] and the torque[3] about its centre (the
+ * centre taken at the z of its markers), from its own 64 markers. */
+int efvm_body_loads(efvm_ctx* ctx, int32_t n_bodies, double* out);
 /* Number of solid cells and of IBM ghost cells (IbmGhostCells.cells.len()). */
 int efvm_ibm_counts(efvm_ctx* ctx, int64_t* n_solid, int64_t* n_ghost);
 /* The interior SolidMask (crates/cfd_state/src/lib.rs:202-206) as nx*ny bytes,

@@ -1197,6 +1197,45 @@ int oracle_apply_geometry(void* hp) {
     return EFVM_OK;
 }
 
+// compute_marker_loadings_per_body, crates/cfd_ibm/src/lib.rs:509-562: per body
+// pressure and viscous force and the torque about the body centre, from the
+// current state; out[9 b ..] = pressure[3], viscous[3], torque[3].  The centre of
+// a cylinder is (cx, cy) at the z of its markers (the z-cell centre).
+int oracle_body_loads(void* hp, int32_t n_bodies, double* out) {
+    Case& cs = ((OracleHandle*)hp)->cs;
+    for (int q = 0; q < 9 * n_bodies; ++q) out[q] = 0.0;
+    const double sample_offset = cs.mesh.h[0];
+    for (const IbmMarker& m : cs.markers) {
+        const int b = (int)m.body_id;
+        if (b >= n_bodies || b >= (int)cs.cyls.size()) continue;
+        const double sp[3] = {m.position[0] + sample_offset * m.normal[0], m.position[1] + sample_offset * m.normal[1],
+                              m.position[2] + sample_offset * m.normal[2]};
+        PrimVar img;
+        if (!cs.sample_trilinear(sp, img)) continue;
+        if (!(std::isfinite(img.p) && std::isfinite(img.t) && std::isfinite(img.u) && std::isfinite(img.v) &&
+              std::isfinite(img.w)))
+            continue;
+        const double us[3] = {img.u - m.wall_velocity[0], img.v - m.wall_velocity[1], img.w - m.wall_velocity[2]};
+        const double udotn = us[0] * m.normal[0] + us[1] * m.normal[1] + us[2] * m.normal[2];
+        const double mu = cs.visc.mu(img.t);
+        double df[3];
+        for (int d = 0; d < 3; ++d) {
+            const double ut = us[d] - udotn * m.normal[d];
+            const double fp = -img.p * m.normal[d] * m.area;
+            const double fv = mu * ut / sample_offset * m.area;
+            out[9 * b + d] += fp;
+            out[9 * b + 3 + d] += fv;
+            df[d] = fp + fv;
+        }
+        const double c[3] = {cs.cyls[b].cx, cs.cyls[b].cy, m.position[2]};
+        const double r[3] = {m.position[0] - c[0], m.position[1] - c[1], m.position[2] - c[2]};
+        out[9 * b + 6] += r[1] * df[2] - r[2] * df[1];
+        out[9 * b + 7] += r[2] * df[0] - r[0] * df[2];
+        out[9 * b + 8] += r[0] * df[1] - r[1] * df[0];
+    }
+    return EFVM_OK;
+}
+
 int oracle_marker_force(void* hp, double out[6]) {
     Case& cs = ((OracleHandle*)hp)->cs;
     for (int d = 0; d < 6; ++d) out[d] = cs.marker_force[d];

@@ -61,6 +61,7 @@ def lib(parallel: bool = False) -> C.CDLL:
     L.oracle_wall_force.argtypes = [vp, dp]
     L.oracle_ibm_counts.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
     L.oracle_apply_geometry.argtypes = [vp]
+    L.oracle_body_loads.argtypes = [vp, i32, dp]
     L.oracle_get_mask.argtypes = [vp, C.POINTER(C.c_uint8)]
     L.oracle_flux.argtypes = [C.c_int, C.c_double, C.c_double, dp, dp, C.c_int, dp]
     L.oracle_flux_normal.argtypes = [C.c_int, C.c_double, C.c_double, dp, dp, dp, dp]
@@ -177,6 +178,11 @@ class OracleCase:
     def wall_force(self) -> np.ndarray:
         out = np.zeros(6)
         self.L.oracle_wall_force(self.h, _dp(out))
+        return out
+
+    def body_loads(self, n_bodies: int) -> np.ndarray:
+        out = np.zeros((n_bodies, 9))
+        self.L.oracle_body_loads(self.h, n_bodies, _dp(out))
         return out
 
     def apply_geometry(self) -> None:
