@@ -28,6 +28,8 @@ struct efvm_ctx {
     Physics ph;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;      // IBM forces, forked from the step graph
+    cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join = nullptr;
     double* U[3] = {nullptr, nullptr, nullptr};  // U0 (= u^n), U1, U2
     uint8_t* mask = nullptr;
     double* yw = nullptr;                          // viscous y weights
@@ -313,16 +315,31 @@ void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool wi
 
 // One whole SSP-RK3 step.  With IBM the forces of a stage and the mirror of the
 // next run in one launch (7 launches a step instead of 10).
-void enqueue_rk3_step(efvm_ctx* c) {
+// One whole SSP-RK3 step, as captured into the step graph.  With IBM the
+// forces of stage s run on a side branch that forks after stage s, in parallel
+// with the mirror and stage s + 1 (they read only fluid cells of the stage-s
+// output and the stage-s z-fill, which the next stage leaves alone); the
+// branch joins at the end of the step, before the next step's mirror rewrites
+// the z-ghost state the last forces read.
+int enqueue_rk3_step(efvm_ctx* c) {
     double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
     if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->st, -1, 0, 1, true, S(c));
     else c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     for (int s = 0; s < 3; ++s) {
         enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1]);
-        if (c->ibm)
-            c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, s, s < 2 ? s + 1 : -1, 0,
-                                      true, S(c));
+        if (c->ibm) {
+            CUDA_TRY(c, cudaEventRecord(c->ev_fork[s], S(c)));
+            CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev_fork[s], 0));
+            c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, s, -1, 0, false, c->side);
+            if (s < 2)
+                c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, -1, s + 1, 0, true, S(c));
+        }
     }
+    if (c->ibm) {
+        CUDA_TRY(c, cudaEventRecord(c->ev_join, c->side));
+        CUDA_TRY(c, cudaStreamWaitEvent(S(c), c->ev_join, 0));
+    }
+    return EFVM_OK;
 }
 
 int capture_step_graph(efvm_ctx* c) {
@@ -330,13 +347,22 @@ int capture_step_graph(efvm_ctx* c) {
         cudaGraphExecDestroy(c->graph_exec);
         c->graph_exec = nullptr;
     }
+    if (c->ibm && !c->side) {
+        CUDA_TRY(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+        for (auto& ev : c->ev_fork) CUDA_TRY(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CUDA_TRY(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    }
     const uint64_t before = c->launches;
     cudaGraph_t graph;
     CUDA_TRY(c, cudaStreamBeginCapture(S(c), cudaStreamCaptureModeThreadLocal));
-    enqueue_rk3_step(c);
+    const int rc_enq = enqueue_rk3_step(c);
     cudaError_t e = cudaStreamEndCapture(S(c), &graph);
     c->graph_kernels = (int)(c->launches - before);
     c->launches = before;
+    if (rc_enq) {
+        if (e == cudaSuccess) cudaGraphDestroy(graph);
+        return rc_enq;
+    }
     if (e != cudaSuccess) return fail(c, EFVM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&c->graph_exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -584,6 +610,10 @@ int efvm_destroy(efvm_ctx* c) {
     cudaFree(c->corr);
     cudaFree(c->fallbacks);
     cudaFree(c->out_fields);
+    for (auto& ev : c->ev_fork)
+        if (ev) cudaEventDestroy(ev);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return EFVM_OK;
