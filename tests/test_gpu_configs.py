@@ -45,8 +45,12 @@ def test_vortex128_periodic_to_t10_matches_oracle_run():
     assert abs(linf - pin["linf"]) <= 1e-8 * pin["linf"]
 
 
-def test_cylinder_1100x205_plateau_drag_meets_reference_gate():
+def plateau_drag(precision=None):
+    from dev_field_efvm_b200 import abi
+
     grid, params, u, ex = cases.cylinder_baseline_case()
+    if precision is not None:
+        params.precision = precision
     d = Context(grid, params)
     d.set_cylinders(ex["cylinders"], ex["freestream"])
     d.upload(u)
@@ -57,7 +61,25 @@ def test_cylinder_1100x205_plateau_drag_meets_reference_gate():
     tail = cd[int(0.9 * len(cd)):]
     mean = float(tail.mean())
     ptp = float((tail.max() - tail.min()) / abs(mean))
+    return mean, ptp, info
+
+
+def test_cylinder_1100x205_plateau_drag_meets_reference_gate():
+    mean, ptp, info = plateau_drag()
     print(f"cylinder 1100x205 t={info.time:.4f} steps={info.steps_done} Cd={mean:.5f} ptp={ptp:.2e} "
           f"dev from DFG={abs(mean - DFG_CD) / DFG_CD:.3%}")
     assert abs(mean - DFG_CD) / DFG_CD <= 0.05
     assert ptp <= 0.02
+
+
+def test_fp32_flux_form_reaches_the_same_plateau_drag():
+    """The bench's chosen form (FP32 reconstruction and fluxes, FP64 state and
+    force integral) on the same run: its plateau drag equals the FP64 one to
+    0.1 %, far inside the gate, so the two forms are at equal drag error."""
+    from dev_field_efvm_b200 import abi
+
+    cd64, _, _ = plateau_drag()
+    cd32, ptp32, info = plateau_drag(abi.PREC_FP32_FLUX)
+    print(f"plateau Cd: FP64 {cd64:.6f}, FP32 fluxes {cd32:.6f} (rel diff {abs(cd32 - cd64) / cd64:.2e})")
+    assert abs(cd32 - cd64) <= 1e-3 * cd64
+    assert ptp32 <= 0.02
