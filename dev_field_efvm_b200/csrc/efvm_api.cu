@@ -52,6 +52,7 @@ struct efvm_ctx {
     // learned face-flux correction (efvm_set_flux_correction)
     efvm_nn* nn = nullptr;
     float* corr = nullptr;               // [2][4][ny][nx]
+    float4* prims = nullptr;             // the network's per-cell inputs
     unsigned long long* fallbacks = nullptr;
     float sensor = 0.f;
     uint64_t corr_faces = 0;
@@ -286,8 +287,8 @@ int prologue(efvm_ctx* c) {
 
 void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, bool pdl = true) {
     if (c->nn)  // the learned corrections of this stage's input
-        c->launches += nn_forward_padded(c->nn, uin, c->g.plane, c->g.pitch, c->g.nx, c->g.ny, c->corr, c->sensor,
-                                         c->fallbacks, S(c));
+        c->launches += nn_forward_padded(c->nn, uin, c->g.plane, c->g.pitch, c->g.nx, c->g.ny, c->corr, c->prims,
+                                         c->sensor, c->fallbacks, S(c));
     StageArgs a{};
     a.corr = c->nn ? c->corr : nullptr;
     a.g = c->g;
@@ -610,6 +611,7 @@ int efvm_destroy(efvm_ctx* c) {
     cudaFree(c->corr);
     cudaFree(c->fallbacks);
     cudaFree(c->out_fields);
+    cudaFree(c->prims);
     for (auto& ev : c->ev_fork)
         if (ev) cudaEventDestroy(ev);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -708,6 +710,7 @@ int efvm_set_flux_correction(efvm_ctx* c, efvm_nn* nn, float sensor) {
     if (!c->corr) {
         CUDA_TRY(c, cudaMalloc(&c->corr, 8ull * c->g.nx * c->g.ny * sizeof(float)));
         CUDA_TRY(c, cudaMalloc(&c->fallbacks, sizeof(unsigned long long)));
+        CUDA_TRY(c, cudaMalloc(&c->prims, (size_t)c->g.nx * c->g.ny * sizeof(float4)));
     }
     CUDA_TRY(c, cudaMemsetAsync(c->fallbacks, 0, sizeof(unsigned long long), S(c)));
     if (nn_prepare_launches()) return fail(c, EFVM_ERR_CUDA, "flux correction: kernel attributes");

@@ -185,7 +185,7 @@ int launch_clock(unsigned long long* out, void* stream);
 // The learned correction (efvm_nn.cu): corrections of every face of one
 // periodic context state, and the kernel attributes its launches need.
 int nn_forward_padded(const efvm_nn* h, const double* q, long long plane, int pitch, int nx, int ny, float* corr,
-                      float sensor, unsigned long long* fallbacks, void* stream);
+                      float4* prims, float sensor, unsigned long long* fallbacks, void* stream);
 int nn_prepare_launches();
 
 // Validation and the device description of one case (efvm_api.cu): global rows

@@ -173,45 +173,97 @@ __device__ __forceinline__ void prim_at(const SV& sv, int b, int i, int j, float
     w[3] = (float)p;
 }
 
-// The stencil features of face `id`, written as row r of X (and of X^T when xt != null).
+// The network's per-cell inputs (rho - 1, u, v, p - 1) in FP32, computed once
+// per cell by nn_prims_kernel; each cell feeds 50 face stencils.
+struct PrimView {
+    const float4* p;
+    int nx, ny;
+    __device__ float4 get(int b, int i, int j) const {
+        i = (i % nx + nx) % nx;
+        j = (j % ny + ny) % ny;
+        return p[((long long)b * ny + j) * nx + i];
+    }
+};
+
 template <class SV>
-__device__ void gather_face(const SV& sv, const FaceId& id, float gamma, unsigned char* x, unsigned char* xt, int r) {
-    for (int c = -2; c <= 2; ++c)
-        for (int a = -3; a <= 1; ++a) {
-            const int ci = id.orient == 0 ? id.i + a : id.i + c;
-            const int cj = id.orient == 0 ? id.j + c : id.j + a;
-            float w[4];
-            prim_at(sv, id.b, ci, cj, gamma, w);
-            const float un = id.orient == 0 ? w[1] : w[2], ut = id.orient == 0 ? w[2] : w[1];
-            const float f[4] = {w[0] - 1.0f, un, ut, w[3] - 1.0f};
-            const int k0 = ((c + 2) * 5 + (a + 3)) * 4;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                put(x, r, k0 + v, 128, f[v]);
-                if (xt) put(xt, k0 + v, r, K1, f[v]);
-            }
-        }
-    for (int k = IN; k < K1; ++k) {
-        put(x, r, k, 128, 0.f);
-        if (xt) put(xt, k, r, K1, 0.f);
+__global__ void nn_prims_kernel(SV sv, int batch, float gamma, float4* __restrict__ out) {
+    const long long n = (long long)sv.nx * sv.ny, total = (long long)batch * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t / n);
+        const long long c = t - (long long)b * n;
+        const int j = (int)(c / sv.nx), i = (int)(c - (long long)j * sv.nx);
+        float w[4];
+        prim_at(sv, b, i, j, gamma, w);
+        out[t] = make_float4(w[0] - 1.0f, w[1], w[2], w[3] - 1.0f);
     }
 }
 
-// Weights into shared memory (and their transposes for the backward pass).
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// The stencil features of face `id`, written as row r of X with one 16-byte
+// store per two stencil cells (8 consecutive K in the canonical layout), and
+// into X^T (element by element) when xt != null.  Feature 4q + v is variable v
+// (rho - 1, normal velocity, tangential velocity, p - 1) of stencil cell
+// q = (c + 2) * 5 + (a + 3), a the offset along the face normal (-3..1), c across.
+__device__ void gather_face(const PrimView& pv, const FaceId& id, unsigned char* x, unsigned char* xt, int r) {
+#pragma unroll 7
+    for (int m = 0; m < K1 / 8; ++m) {
+        float f[8];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int q = 2 * m + h;
+            if (q < 25) {
+                const int c = q / 5 - 2, a = q % 5 - 3;
+                const int ci = id.orient == 0 ? id.i + a : id.i + c;
+                const int cj = id.orient == 0 ? id.j + c : id.j + a;
+                const float4 w = pv.get(id.b, ci, cj);
+                f[4 * h + 0] = w.x;
+                f[4 * h + 1] = id.orient == 0 ? w.y : w.z;
+                f[4 * h + 2] = id.orient == 0 ? w.z : w.y;
+                f[4 * h + 3] = w.w;
+            } else {
+                f[4 * h + 0] = f[4 * h + 1] = f[4 * h + 2] = f[4 * h + 3] = 0.f;
+            }
+        }
+        const uint4 v = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]), pack_bf16x2(f[4], f[5]),
+                                   pack_bf16x2(f[6], f[7]));
+        *reinterpret_cast<uint4*>(x + tc::canon_offset(r, 8 * m, 128)) = v;
+        if (xt)
+#pragma unroll
+            for (int e = 0; e < 8; ++e) put(xt, 8 * m + e, r, K1, f[e]);
+    }
+}
+
+// Weights into shared memory, 16 bytes (8 consecutive K of one row) per copy,
+// and their transposes for the backward pass element by element.
 __device__ void load_weights(const Net& net, unsigned char* sm, bool transposed) {
-    for (int t = threadIdx.x; t < H * K1; t += blockDim.x) {
-        const int o = t / K1, k = t - o * K1;
-        *reinterpret_cast<__nv_bfloat16*>(sm + SM_W1 + tc::canon_offset(o, k, H)) = net.w1[t];
+    const uint4* w1 = reinterpret_cast<const uint4*>(net.w1);
+    for (int t = threadIdx.x; t < H * K1 / 8; t += blockDim.x) {
+        const int o = t / (K1 / 8), g = t - o * (K1 / 8);
+        *reinterpret_cast<uint4*>(sm + SM_W1 + tc::canon_offset(o, 8 * g, H)) = w1[t];
     }
-    for (int t = threadIdx.x; t < H * H; t += blockDim.x) {
-        const int o = t / H, k = t - o * H;
-        *reinterpret_cast<__nv_bfloat16*>(sm + SM_W2 + tc::canon_offset(o, k, H)) = net.w2[t];
-        if (transposed) *reinterpret_cast<__nv_bfloat16*>(sm + SM_W2T + tc::canon_offset(k, o, H)) = net.w2[t];
+    const uint4* w2 = reinterpret_cast<const uint4*>(net.w2);
+    for (int t = threadIdx.x; t < H * H / 8; t += blockDim.x) {
+        const int o = t / (H / 8), g = t - o * (H / 8);
+        *reinterpret_cast<uint4*>(sm + SM_W2 + tc::canon_offset(o, 8 * g, H)) = w2[t];
     }
-    for (int t = threadIdx.x; t < N3 * H; t += blockDim.x) {
-        const int o = t / H, k = t - o * H;
-        *reinterpret_cast<__nv_bfloat16*>(sm + SM_W3 + tc::canon_offset(o, k, N3)) = net.w3[t];
-        if (transposed) *reinterpret_cast<__nv_bfloat16*>(sm + SM_W3T + tc::canon_offset(k, o, H)) = net.w3[t];
+    const uint4* w3 = reinterpret_cast<const uint4*>(net.w3);
+    for (int t = threadIdx.x; t < N3 * H / 8; t += blockDim.x) {
+        const int o = t / (H / 8), g = t - o * (H / 8);
+        *reinterpret_cast<uint4*>(sm + SM_W3 + tc::canon_offset(o, 8 * g, N3)) = w3[t];
+    }
+    if (transposed) {
+        for (int t = threadIdx.x; t < H * H; t += blockDim.x) {
+            const int o = t / H, k = t - o * H;
+            *reinterpret_cast<__nv_bfloat16*>(sm + SM_W2T + tc::canon_offset(k, o, H)) = net.w2[t];
+        }
+        for (int t = threadIdx.x; t < N3 * H; t += blockDim.x) {
+            const int o = t / H, k = t - o * H;
+            *reinterpret_cast<__nv_bfloat16*>(sm + SM_W3T + tc::canon_offset(k, o, H)) = net.w3[t];
+        }
     }
 }
 
@@ -251,21 +303,24 @@ __device__ void relu_epilogue(uint32_t tmem, const float* bias, unsigned char* o
         float v[16];
         tc::tmem_ld16(tmem, c0, v);
 #pragma unroll
-        for (int c = 0; c < 16; ++c) {
-            const float h = fmaxf(v[c] + bias[c0 + c], 0.f);
-            put(out, r, c0 + c, 128, h);
-            if (out_t) put(out_t, c0 + c, r, H, h);
-        }
+        for (int c = 0; c < 16; ++c) v[c] = fmaxf(v[c] + bias[c0 + c], 0.f);
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+            *reinterpret_cast<uint4*>(out + tc::canon_offset(r, c0 + 8 * g, 128)) =
+                make_uint4(pack_bf16x2(v[8 * g], v[8 * g + 1]), pack_bf16x2(v[8 * g + 2], v[8 * g + 3]),
+                           pack_bf16x2(v[8 * g + 4], v[8 * g + 5]), pack_bf16x2(v[8 * g + 6], v[8 * g + 7]));
+        if (out_t)
+#pragma unroll
+            for (int c = 0; c < 16; ++c) put(out_t, c0 + c, r, H, v[c]);
     }
 }
 
 // Forward pass of one tile through layer 2 (H1, H2 in shared memory).
-template <class SV>
-__device__ bool forward_hidden(const SV& sv, const Net& net, unsigned char* sm, TC& t, long long f0, int nx, int ny,
+__device__ bool forward_hidden(const PrimView& pv, const Net& net, unsigned char* sm, TC& t, long long f0,
                                bool keep_transposes) {
     const int r = threadIdx.x;
-    const FaceId id = face_of(f0 + r, nx, ny);
-    gather_face(sv, id, net.gamma, sm + SM_X, keep_transposes ? sm + SM_XT : nullptr, r);
+    const FaceId id = face_of(f0 + r, pv.nx, pv.ny);
+    gather_face(pv, id, sm + SM_X, keep_transposes ? sm + SM_XT : nullptr, r);
     load_weights(net, sm, keep_transposes);
     if (!run_gemm(t, sm + SM_X, sm + SM_W1, H, K1)) return false;
     relu_epilogue(t.tmem, net.p + P_B1, sm + SM_H1, keep_transposes ? sm + SM_H1T : nullptr, r);
@@ -294,8 +349,7 @@ __device__ void tile_teardown(const TC& t) {
 // Forward: the correction of every face, grid frame, corr[((b*2+orient)*4+v)*ny*nx + j*nx + i].
 // sensor > 0 (inference): a face whose two cells differ in pressure by more than
 // sensor * min(p), or where rho or p is not positive, keeps the plain flux.
-template <class SV>
-__global__ void __launch_bounds__(128) nn_forward_kernel(SV sv, Net net, float* __restrict__ corr, float sensor,
+__global__ void __launch_bounds__(128) nn_forward_kernel(PrimView pv, Net net, float* __restrict__ corr, float sensor,
                                                          unsigned long long* fallbacks) {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -304,20 +358,19 @@ __global__ void __launch_bounds__(128) nn_forward_kernel(SV sv, Net net, float* 
     tile_setup(t, &bar, &slot);
     const long long f0 = (long long)blockIdx.x * 128;
     const int r = threadIdx.x;
-    if (forward_hidden(sv, net, sm, t, f0, sv.nx, sv.ny, false) && run_gemm(t, sm + SM_H2, sm + SM_W3, N3, H)) {
+    if (forward_hidden(pv, net, sm, t, f0, false) && run_gemm(t, sm + SM_H2, sm + SM_W3, N3, H)) {
         float v[16];
         tc::tmem_ld16(t.tmem, 0, v);
-        const FaceId id = face_of(f0 + r, sv.nx, sv.ny);
+        const FaceId id = face_of(f0 + r, pv.nx, pv.ny);
         float y[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) y[o] = (v[o] + net.p[P_B3 + o]) * net.out_scale;
         if (sensor > 0.f) {
-            float wl[4], wr[4];
             const int il = id.orient == 0 ? id.i - 1 : id.i, jl = id.orient == 0 ? id.j : id.j - 1;
-            prim_at(sv, id.b, il, jl, net.gamma, wl);
-            prim_at(sv, id.b, id.i, id.j, net.gamma, wr);
-            const bool fire = !(wl[0] > 0.f && wr[0] > 0.f && wl[3] > 0.f && wr[3] > 0.f) ||
-                              fabsf(wr[3] - wl[3]) > sensor * fminf(wl[3], wr[3]);
+            const float4 ql = pv.get(id.b, il, jl), qr = pv.get(id.b, id.i, id.j);
+            const float rl = ql.x + 1.0f, rr = qr.x + 1.0f, pl = ql.w + 1.0f, pr = qr.w + 1.0f;
+            const bool fire = !(rl > 0.f && rr > 0.f && pl > 0.f && pr > 0.f) ||
+                              fabsf(pr - pl) > sensor * fminf(pl, pr);
             if (fire) {
                 y[0] = y[1] = y[2] = y[3] = 0.f;
                 atomicAdd(fallbacks, 1ull);
@@ -325,7 +378,7 @@ __global__ void __launch_bounds__(128) nn_forward_kernel(SV sv, Net net, float* 
         }
         // face frame (rho, m_n, m_t, E) -> grid frame (rho, m_x, m_y, E)
         const float g[4] = {y[0], id.orient == 0 ? y[1] : y[2], id.orient == 0 ? y[2] : y[1], y[3]};
-        const long long cell = (long long)id.j * sv.nx + id.i, nn = (long long)sv.nx * sv.ny;
+        const long long cell = (long long)id.j * pv.nx + id.i, nn = (long long)pv.nx * pv.ny;
 #pragma unroll
         for (int q = 0; q < 4; ++q) corr[((long long)(id.b * 2 + id.orient) * 4 + q) * nn + cell] = g[q];
     }
@@ -363,7 +416,7 @@ __device__ void store_weight_grad(uint32_t tmem, int rows, int ncols, float* out
 // Backward: given dL/dcorr (grid frame, the layout of corr), the gradient of the
 // loss with respect to every parameter, summed over this tile's 128 faces, into
 // partials[tile][P_COUNT].
-__global__ void __launch_bounds__(128) nn_backward_kernel(PackedStates sv, Net net, const float* __restrict__ dcorr,
+__global__ void __launch_bounds__(128) nn_backward_kernel(PrimView sv, Net net, const float* __restrict__ dcorr,
                                                           float* __restrict__ partials) {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -378,7 +431,7 @@ __global__ void __launch_bounds__(128) nn_backward_kernel(PackedStates sv, Net n
     for (int q = threadIdx.x; q < 128 * 128 * 2 / 16; q += blockDim.x)
         reinterpret_cast<uint4*>(sm + SM_AT)[q] = make_uint4(0, 0, 0, 0);
     do {
-        if (!forward_hidden(sv, net, sm, t, f0, sv.nx, sv.ny, true)) break;
+        if (!forward_hidden(sv, net, sm, t, f0, true)) break;
         // output gradient of this face in its own frame, times out_scale
         const FaceId id = face_of(f0 + r, sv.nx, sv.ny);
         const long long cell = (long long)id.j * sv.nx + id.i, nn = (long long)sv.nx * sv.ny;
@@ -389,11 +442,14 @@ __global__ void __launch_bounds__(128) nn_backward_kernel(PackedStates sv, Net n
                              (id.orient == 0 ? g[2] : g[1]) * net.out_scale, g[3] * net.out_scale};
         float dyrow[N3];
 #pragma unroll
-        for (int o = 0; o < N3; ++o) {
-            dyrow[o] = o < NOUT ? __bfloat162float(__float2bfloat16_rn(dy[o])) : 0.f;
-            put(sm + SM_DY, r, o, 128, dyrow[o]);
-            put(sm + SM_AT, o, r, 128, dyrow[o]);
-        }
+        for (int o = 0; o < N3; ++o) dyrow[o] = o < NOUT ? __bfloat162float(__float2bfloat16_rn(dy[o])) : 0.f;
+#pragma unroll
+        for (int g = 0; g < 2; ++g)
+            *reinterpret_cast<uint4*>(sm + SM_DY + tc::canon_offset(r, 8 * g, 128)) =
+                make_uint4(pack_bf16x2(dyrow[8 * g], dyrow[8 * g + 1]), pack_bf16x2(dyrow[8 * g + 2], dyrow[8 * g + 3]),
+                           pack_bf16x2(dyrow[8 * g + 4], dyrow[8 * g + 5]), pack_bf16x2(dyrow[8 * g + 6], dyrow[8 * g + 7]));
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) put(sm + SM_AT, o, r, 128, dyrow[o]);
         column_sums(dyrow, NOUT, red, part + P_B3);
         // dW3 = dY^T H2
         if (!run_gemm(t, sm + SM_AT, sm + SM_H2T, H, 128)) break;
@@ -413,10 +469,12 @@ __global__ void __launch_bounds__(128) nn_backward_kernel(PackedStates sv, Net n
                 }
             }
 #pragma unroll
-            for (int c = 0; c < H; ++c) {
-                put(sm + SM_DZ, r, c, 128, dz[c]);
-                put(sm + SM_AT, c, r, 128, dz[c]);
-            }
+            for (int g = 0; g < H / 8; ++g)
+                *reinterpret_cast<uint4*>(sm + SM_DZ + tc::canon_offset(r, 8 * g, 128)) =
+                    make_uint4(pack_bf16x2(dz[8 * g], dz[8 * g + 1]), pack_bf16x2(dz[8 * g + 2], dz[8 * g + 3]),
+                               pack_bf16x2(dz[8 * g + 4], dz[8 * g + 5]), pack_bf16x2(dz[8 * g + 6], dz[8 * g + 7]));
+#pragma unroll
+            for (int c = 0; c < H; ++c) put(sm + SM_AT, c, r, 128, dz[c]);
             column_sums(dz, H, red, part + P_B2);
         }
         // dW2 = dZ2^T H1
@@ -537,6 +595,8 @@ struct efvm_nn {
     size_t partials_cap = 0;
     float *corr = nullptr, *dcorr = nullptr;
     size_t corr_cap = 0;
+    float4* prims = nullptr;
+    size_t prims_cap = 0;
     double* loss_d = nullptr;
     std::string err;
 };
@@ -554,20 +614,18 @@ nn::Net nn_net(const efvm_nn* h) {
 }
 
 int nn_forward_padded(const efvm_nn* h, const double* q, long long plane, int pitch, int nx, int ny, float* corr,
-                      float sensor, unsigned long long* fallbacks, void* stream) {
+                      float4* prims, float sensor, unsigned long long* fallbacks, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
     nn::PaddedState sv{q, plane, pitch, nx, ny};
+    nn::nn_prims_kernel<nn::PaddedState><<<(nx * ny + 255) / 256, 256, 0, s>>>(sv, 1, h->gamma, prims);
     const int tiles = (int)(2LL * nx * ny / 128);
-    nn::nn_forward_kernel<nn::PaddedState><<<tiles, 128, nn::SM_FWD, (cudaStream_t)stream>>>(sv, nn_net(h), corr, sensor,
-                                                                                           fallbacks);
-    return 1;
+    nn::nn_forward_kernel<<<tiles, 128, nn::SM_FWD, s>>>(nn::PrimView{prims, nx, ny}, nn_net(h), corr, sensor,
+                                                          fallbacks);
+    return 2;
 }
 
 int nn_prepare_launches() {
-    cudaError_t e = cudaFuncSetAttribute(nn::nn_forward_kernel<nn::PaddedState>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, nn::SM_FWD);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(nn::nn_forward_kernel<nn::PackedStates>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 nn::SM_FWD);
+    cudaError_t e = cudaFuncSetAttribute(nn::nn_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, nn::SM_FWD);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(nn::nn_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, nn::SM_TOTAL);
     return e == cudaSuccess ? EFVM_OK : EFVM_ERR_CUDA;
@@ -627,6 +685,13 @@ int ensure_buffers(efvm_nn* h, int batch, int nx, int ny) {
         h->partials_cap = 0;
         NN_TRY(h, cudaMalloc(&h->partials, tiles * nn::P_COUNT * sizeof(float)));
         h->partials_cap = tiles * nn::P_COUNT;
+    }
+    if ((size_t)batch * nx * ny > h->prims_cap) {
+        cudaFree(h->prims);
+        h->prims = nullptr;
+        h->prims_cap = 0;
+        NN_TRY(h, cudaMalloc(&h->prims, (size_t)batch * nx * ny * sizeof(float4)));
+        h->prims_cap = (size_t)batch * nx * ny;
     }
     if (faces * 4 > h->corr_cap) {
         cudaFree(h->corr);
@@ -701,6 +766,7 @@ int efvm_nn_destroy(efvm_nn* h) {
     cudaFree(h->partials);
     cudaFree(h->corr);
     cudaFree(h->dcorr);
+    cudaFree(h->prims);
     cudaFree(h->loss_d);
     delete h;
     return EFVM_OK;
@@ -728,10 +794,14 @@ int efvm_nn_forward(efvm_nn* h, const double* states, int32_t batch, int32_t nx,
     if (!h || !states || !corr) return nfail(h, EFVM_ERR_INVALID_ARG, "null argument");
     int rc = check_shape(h, batch, nx, ny);
     if (rc) return rc;
+    rc = ensure_buffers(h, batch, nx, ny);
+    if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
     nn::PackedStates sv{states, nx, ny};
+    const long long cells = (long long)batch * nx * ny;
+    nn::nn_prims_kernel<nn::PackedStates><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(sv, batch, h->gamma, h->prims);
     const int tiles = (int)(2LL * batch * nx * ny / 128);
-    nn::nn_forward_kernel<nn::PackedStates><<<tiles, 128, nn::SM_FWD, s>>>(sv, nn_net(h), corr, 0.f, nullptr);
+    nn::nn_forward_kernel<<<tiles, 128, nn::SM_FWD, s>>>(nn::PrimView{h->prims, nx, ny}, nn_net(h), corr, 0.f, nullptr);
     NN_TRY(h, cudaGetLastError());
     NN_TRY(h, cudaStreamSynchronize(s));
     return tc_status(h);
@@ -748,12 +818,14 @@ int efvm_nn_loss_grad(efvm_nn* h, const double* states, const double* resid, int
     nn::PackedStates sv{states, nx, ny};
     const long long cells = (long long)batch * nx * ny;
     const int tiles = (int)(2 * cells / 128);
-    nn::nn_forward_kernel<nn::PackedStates><<<tiles, 128, nn::SM_FWD, s>>>(sv, nn_net(h), h->corr, 0.f, nullptr);
+    nn::nn_prims_kernel<nn::PackedStates><<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(sv, batch, h->gamma, h->prims);
+    const nn::PrimView pv{h->prims, nx, ny};
+    nn::nn_forward_kernel<<<tiles, 128, nn::SM_FWD, s>>>(pv, nn_net(h), h->corr, 0.f, nullptr);
     NN_TRY(h, cudaMemsetAsync(h->loss_d, 0, sizeof(double), s));
     nn::nn_residual_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, s>>>(h->corr, resid, batch, nx, ny, 1.0 / dx,
                                                                          1.0 / dy, w[0], w[1], w[2], w[3], h->dcorr,
                                                                          h->loss_d);
-    nn::nn_backward_kernel<<<tiles, 128, nn::SM_TOTAL, s>>>(sv, nn_net(h), h->dcorr, h->partials);
+    nn::nn_backward_kernel<<<tiles, 128, nn::SM_TOTAL, s>>>(pv, nn_net(h), h->dcorr, h->partials);
     nn::nn_reduce_kernel<<<(nn::P_COUNT + 255) / 256, 256, 0, s>>>(h->partials, tiles, h->grad);
     if (grad_out) NN_TRY(h, cudaMemcpyAsync(grad_out, h->grad, nn::P_COUNT * sizeof(float), cudaMemcpyDeviceToDevice, s));
     NN_TRY(h, cudaGetLastError());
