@@ -703,8 +703,8 @@ int efvm_set_flux_correction(efvm_ctx* c, efvm_nn* nn, float sensor) {
     }
     if (!c->ph.periodic_x || !c->ph.periodic_y || has_halo(c) || c->ibm)
         return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction needs a periodic grid without IBM or slabs");
-    if (c->params.reconstruction != EFVM_RECON_MUSCL || c->params.flux_scheme != EFVM_FLUX_HLLC)
-        return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction runs with MUSCL + HLLC");
+    if (c->params.reconstruction != EFVM_RECON_MUSCL || c->params.flux_scheme != EFVM_FLUX_HLLC || c->ph.viscous)
+        return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction runs inviscid with MUSCL + HLLC");
     if (((long long)c->g.nx * c->g.ny) % 64 || c->g.nx < 5 || c->g.ny < 5)
         return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction needs nx*ny a multiple of 64 and nx, ny >= 5");
     if (!c->corr) {

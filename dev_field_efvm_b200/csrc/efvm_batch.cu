@@ -170,7 +170,7 @@ int apply_rows(efvm_batch* b) {
     const bool fp32 = b->params.precision == EFVM_PREC_FP32_FLUX;
     for (int k = 0; k < b->n; ++k) {
         const int r = b->bucket_rows[size_bucket(b->g[k])];
-        b->cases[k].rows = r > 0 ? r : std::min(stage_rows(b->g[k].nx, b->g[k].ny, fp32), 8);
+        b->cases[k].rows = r > 0 ? r : std::min(stage_rows(b->g[k].nx, b->g[k].ny, fp32, b->ph.viscous), 8);
     }
     BATCH_TRY(b, cudaMemcpyAsync(b->cases_d, b->cases.data(), b->n * sizeof(BatchCase), cudaMemcpyHostToDevice,
                                  b->stream));
@@ -307,7 +307,7 @@ int efvm_batch_create(const efvm_grid* grids, int32_t n_cases, const efvm_params
         c.ph = b->phc[k];
         // rows per warp: a batch fills the GPU with many cases, so each case takes
         // the rows it would take alone, at most 8
-        c.rows = std::min(stage_rows(c.g.nx, c.g.ny, fp32), 8);
+        c.rows = std::min(stage_rows(c.g.nx, c.g.ny, fp32, c.ph.viscous), 8);
         const size_t state = ((size_t)4 * c.g.plane + 31) / 32 * 32;
         for (int s = 0; s < 3; ++s) c.U[s] = b->pool + off[k] + s * state;
         c.yw = b->yw_pool + yw_all.size();

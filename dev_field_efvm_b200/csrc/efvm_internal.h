@@ -173,9 +173,9 @@ struct BatchStageArgs {
 };
 
 // Stage-kernel tiling of one case: strips of columns, and rows per warp for a
-// case that runs alone (fp32: the FP32-flux form).
+// case that runs alone (fp32: the FP32-flux form; viscous: with viscous terms).
 int stage_strips(int nx);
-int stage_rows(int nx, int ny, bool fp32);
+int stage_rows(int nx, int ny, bool fp32, bool viscous);
 int launch_batch_stage(const BatchStageArgs& b, int n_tiles, bool pdl, void* stream);
 // Per-step set-up of every case (one thread each).
 int launch_batch_setup(const Physics& ph, const BatchCase* cases, int n_cases, bool pdl, void* stream);

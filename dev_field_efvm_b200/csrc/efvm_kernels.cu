@@ -288,7 +288,7 @@ constexpr int WPB = 4;     // warps per block
 // on a step's last stage, the sponge, refills the boundary ghosts of the output
 // and takes the wave-speed max for the next step's CFL dt.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, class R, class A, bool CORR = false>
+template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true>
 __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
     if (!a.st->active) return;
     const Geometry& g = a.g;
@@ -353,9 +353,53 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
             V4<R> unused;
             slope_faces(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
         }
+        const double dt = a.st->dt;  // set by the step's set-up, constant during the stage
         Q4<R> gb;
         for (int j = jb - 1; j < je; ++j) {
             const V4<R> un2 = ldrow(j + 2);
+            const bool row = j >= jb;  // warp-uniform: the first pass only forms the face below row jb
+
+            // ---- x-face on the left of column i, row j, and the divergence of
+            // the faces below, left and right of the cell ----
+            // Flux divergence in the reference's accumulation order: the face
+            // below (scattered when row j-1 was visited), the face on the left,
+            // then the cell's own +x and +y faces (for_each_face order,
+            // crates/cfd_solver/src/lib.rs:333-337).  Only these four partial
+            // sums stay live through the y-face flux below.
+            double part[4];
+            auto x_face = [&]() {
+                V4<R> ul = shfl_up_v(uc, 1), ur = shfl_down_v(uc, 1);
+                V4<R> ull = ul;  // column i-2 (lane 0 only)
+                if (lane == 0) {
+                    ul = toR<R>(ld(i0 - 1, j));
+                    if (MUSCL) ull = toR<R>(ld(i0 - 2, j));
+                }
+                if (MUSCL && lane == 31) ur = toR<R>(ld(min(i0 + 32, g.nx + NG - 1), j));
+                Q4<R> fx;
+                if (MUSCL) {
+                    V4<R> pp, mm;  // this column's +x and -x face states
+                    slope_faces(ph.limiter, ul, uc, ur, pp, mm);
+                    V4<R> lp = shfl_up_v(pp, 1);  // +x state of column i-1
+                    if (lane == 0) {
+                        V4<R> unused;
+                        slope_faces(ph.limiter, ull, ul, uc, lp, unused);
+                    }
+                    fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : uc), rg, rgm1);
+                } else {
+                    fx = face_flux<SCHEME, R>(xq(ul), xq(uc), rg, rgm1);
+                }
+                const Q4<R> fxr = shfl_down_q(fx, 1);  // face on the right of column i
+                const double fl[4] = {(double)fx.r, (double)fx.mn, (double)fx.mt, (double)fx.E};
+                const double fr[4] = {(double)fxr.r, (double)fxr.mn, (double)fxr.mt, (double)fxr.E};
+                const double gbv[4] = {(double)gb.r, (double)gb.mt, (double)gb.mn, (double)gb.E};
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    double acc = __dmul_rn(gbv[v], g.inv_y);
+                    acc = __dadd_rn(acc, __dmul_rn(fl[v], g.inv_x));
+                    part[v] = __dsub_rn(acc, __dmul_rn(fr[v], g.inv_x));
+                }
+            };
+            if (XFIRST && row) x_face();
 
             // ---- y-face above row j ----
             Q4<R> gt;
@@ -372,58 +416,17 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
             } else {
                 gt = face_flux<SCHEME, R>(yq(uc), yq(un), rg, rgm1);
             }
-            if (j < jb) {  // warp-uniform: the face below the first row only
-                gb = gt;
-                uc = un;
-                un = un2;
-                pc = pn;
-                continue;
-            }
 
-            // ---- x-face on the left of column i, row j ----
-            V4<R> ul = shfl_up_v(uc, 1), ur = shfl_down_v(uc, 1);
-            V4<R> ull = ul;  // column i-2 (lane 0 only)
-            if (lane == 0) {
-                ul = toR<R>(ld(i0 - 1, j));
-                if (MUSCL) ull = toR<R>(ld(i0 - 2, j));
-            }
-            if (MUSCL && lane == 31) ur = toR<R>(ld(min(i0 + 32, g.nx + NG - 1), j));
-            Q4<R> fx;
-            if (MUSCL) {
-                V4<R> pp, mm;  // this column's +x and -x face states
-                slope_faces(ph.limiter, ul, uc, ur, pp, mm);
-                V4<R> lp = shfl_up_v(pp, 1);  // +x state of column i-1
-                if (lane == 0) {
-                    V4<R> unused;
-                    slope_faces(ph.limiter, ull, ul, uc, lp, unused);
-                }
-                fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : uc), rg, rgm1);
-            } else {
-                fx = face_flux<SCHEME, R>(xq(ul), xq(uc), rg, rgm1);
-            }
-            const Q4<R> fxr = shfl_down_q(fx, 1);  // face on the right of column i
+            if (!XFIRST && row) x_face();
 
-            if (owner) {
+            if (row && owner) {
                 const long long o = cidx(g, i, j);
                 // the cell's state in FP64 (the FP32 path reads it again)
                 const U4 ucd = FP64 ? toU4(uc) : ld(i, j);
-                // Flux divergence in the reference's accumulation order: the face
-                // below (scattered when row j-1 was visited), the face on the
-                // left, then the cell's own +x and +y faces (for_each_face order,
-                // crates/cfd_solver/src/lib.rs:333-337).
-                const double fl[4] = {(double)fx.r, (double)fx.mn, (double)fx.mt, (double)fx.E};
-                const double fr[4] = {(double)fxr.r, (double)fxr.mn, (double)fxr.mt, (double)fxr.E};
-                const double gbv[4] = {(double)gb.r, (double)gb.mt, (double)gb.mn, (double)gb.E};
                 const double gtv[4] = {(double)gt.r, (double)gt.mt, (double)gt.mn, (double)gt.E};
                 double rhs[4];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    double acc = __dmul_rn(gbv[v], g.inv_y);
-                    acc = __dadd_rn(acc, __dmul_rn(fl[v], g.inv_x));
-                    acc = __dsub_rn(acc, __dmul_rn(fr[v], g.inv_x));
-                    acc = __dsub_rn(acc, __dmul_rn(gtv[v], g.inv_y));
-                    rhs[v] = acc;
-                }
+                for (int v = 0; v < 4; ++v) rhs[v] = __dsub_rn(part[v], __dmul_rn(gtv[v], g.inv_y));
                 if constexpr (CORR) {
                     // learned corrections of the four faces (periodic grid): the
                     // x face on the left of a cell, the y face below it
@@ -439,13 +442,12 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 }
                 const bool ibm = a.mask != nullptr;
                 const bool solid = ibm && a.mask[o];
-                if (ph.viscous && !solid) {
+                if (VISC && !solid) {
                     // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D)
                     double us, vs, ts;
                     prim_uvt(ucd, gm1, ph.r_gas, us, vs, ts);
                     double nu[4], nv[4], nt[4];  // +x, -x, +y, -y
-                    const U4 nbs[4] = {FP64 ? toU4(ur) : ld(i + 1, j), FP64 ? toU4(ul) : ld(i - 1, j),
-                                       FP64 ? toU4(un) : ld(i, j + 1), ld(i, j - 1)};
+                    const U4 nbs[4] = {ld(i + 1, j), ld(i - 1, j), FP64 ? toU4(un) : ld(i, j + 1), ld(i, j - 1)};
                     const long long no[4] = {o + 1, o - 1, o + g.pitch, o - g.pitch};
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
@@ -475,7 +477,6 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 }
 
                 // Rk3Integrator / EulerIntegrator::substep, crates/cfd_solver/src/integrate.rs:48-101
-                const double dt = a.st->dt;
                 const double ucv[4] = {ucd.r, ucd.mx, ucd.my, ucd.E};
                 double un_[4];
                 if (a.stage == 1 || a.stage == 2) {
@@ -536,10 +537,11 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
     }
 }
 
-template <int SCHEME, int RECON, class R, int MINB, bool CORR = false>
+template <int SCHEME, int RECON, class R, int MINB, bool VISC, bool CORR = false, bool XFIRST = true>
 __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
     pdl_wait_then_release();
-    stage_strip<SCHEME, RECON, R, StageArgs, CORR>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5), blockIdx.y);
+    stage_strip<SCHEME, RECON, R, VISC, StageArgs, CORR, XFIRST>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5),
+                                                                   blockIdx.y);
 }
 
 // The stage arguments of one batch case, with its geometry and physics in the
@@ -561,7 +563,7 @@ struct BatchView {
 // of block b runs tiles[b * WPB + w] = (case, strip, row block) of that case,
 // with the case's geometry, boundary conditions, buffers and clock.  Warps are
 // the unit so that small cases waste no lanes of a block.
-template <int SCHEME, int RECON, class R, int MINB>
+template <int SCHEME, int RECON, class R, int MINB, bool VISC, bool XFIRST>
 __global__ void __launch_bounds__(32 * WPB, MINB) batch_stage_kernel(BatchStageArgs b, int n_tiles) {
     pdl_wait_then_release();
     const int tile = blockIdx.x * WPB + (threadIdx.x >> 5);
@@ -571,7 +573,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) batch_stage_kernel(BatchStageA
     // the case's geometry and physics are read in place from the case table
     const BatchView v{c.g, c.ph, c.U[b.in_buf], c.U[0], c.U[b.out_buf], nullptr, c.yw, c.st,
                       b.stage, b.completes_step, b.want_cfl, nullptr};
-    stage_strip<SCHEME, RECON, R>(v, c.rows, t.y, t.z);
+    stage_strip<SCHEME, RECON, R, VISC, BatchView, false, XFIRST>(v, c.rows, t.y, t.z);
 }
 
 
@@ -1082,6 +1084,28 @@ static int grid_for(long long n, int block) {
     return (int)b;
 }
 
+// Resident blocks per SM (the register budget: 65536 / (MINB x 128 threads))
+// and the loop order of each stage-kernel form, from a sweep of MINB 4..8, both
+// orders and 2..8 rows per warp, timed as whole steps:
+//  * FP64 inviscid (4096^2 vortex): 6 blocks (80 registers), x-face first --
+//    2.674 ms per step against 2.747 at 5 blocks with the y-face first;
+//  * FP64 viscous (1100x205 cylinder): 5 blocks (96), x-face first; the
+//    cylinder is latency-bound and within 0.2 % for every choice;
+//  * FP32-flux inviscid: 8 blocks (64), y-face first (x-face first costs 20 %);
+//  * FP32-flux viscous: 5 blocks (96), y-face first: 92.2 us per cylinder step
+//    against 96.3 at 8 blocks, where the FP64 viscous terms spill.
+template <class R, bool VISC>
+struct StageForm {
+    static constexpr bool FP64 = sizeof(R) == sizeof(double);
+    static constexpr int MINB = FP64 ? (VISC ? 5 : 6) : (VISC ? 5 : 8);
+    static constexpr bool XFIRST = FP64;
+};
+
+static int form_minb(bool fp32, bool viscous) {
+    return fp32 ? (viscous ? StageForm<float, true>::MINB : StageForm<float, false>::MINB)
+                : (viscous ? StageForm<double, true>::MINB : StageForm<double, false>::MINB);
+}
+
 // Rows each warp marches.  Small grids take the fewest rows that still fill the
 // resident slots in one wave (the warp's first row also pays for the face below
 // it); large grids take 8, measured fastest at 4096^2: with longer runs the rows
@@ -1096,46 +1120,56 @@ static int rows_per_warp(int nx, int ny, int blocks_per_sm) {
     return (int)rows;
 }
 
-template <int SCHEME, int RECON, class R>
+template <int SCHEME, int RECON, class R, bool VISC>
 static void launch_stage_t(const StageArgs& a, bool pdl, cudaStream_t s) {
-    // Resident blocks per SM, measured at 4096^2: the FP64 flux is fastest at 96
-    // registers/thread (5 blocks of 4 warps), the FP32 flux at 64 (8 blocks).
-    constexpr int MINB = sizeof(R) == sizeof(double) ? 5 : 8;
-    const int rows = rows_per_warp(a.g.nx, a.g.ny, MINB);
+    using F = StageForm<R, VISC>;
+    const int rows = rows_per_warp(a.g.nx, a.g.ny, F::MINB);
     const int strips = (a.g.nx + STRIP - 1) / STRIP;
     dim3 block(32 * WPB);
     dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
-    launch_k(stage_kernel<SCHEME, RECON, R, MINB>, grid, block, s, pdl, a, rows);
+    launch_k(stage_kernel<SCHEME, RECON, R, F::MINB, VISC, false, F::XFIRST>, grid, block, s, pdl, a, rows);
 }
 
-template <class R>
-static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
+template <class R, bool VISC>
+static void launch_stage_v(const StageArgs& a, bool pdl, cudaStream_t s) {
     const bool muscl = a.ph.reconstruction == EFVM_RECON_MUSCL;
     switch (a.ph.flux_scheme) {
         case EFVM_FLUX_RUSANOV:
-            muscl ? launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R>(a, pdl, s)
-                  : launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
+            muscl ? launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R, VISC>(a, pdl, s)
+                  : launch_stage_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R, VISC>(a, pdl, s);
             break;
         case EFVM_FLUX_HLLC_TEXTBOOK:
-            muscl ? launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R>(a, pdl, s)
-                  : launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
+            muscl ? launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R, VISC>(a, pdl, s)
+                  : launch_stage_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R, VISC>(a, pdl, s);
             break;
         default:
-            muscl ? launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R>(a, pdl, s)
-                  : launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
+            muscl ? launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R, VISC>(a, pdl, s)
+                  : launch_stage_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R, VISC>(a, pdl, s);
     }
+}
+
+// The viscous terms are a compile-time branch: the inviscid kernels carry none
+// of their registers.
+template <class R>
+static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
+    if (a.ph.viscous) launch_stage_v<R, true>(a, pdl, s);
+    else launch_stage_v<R, false>(a, pdl, s);
 }
 
 int launch_stage(const StageArgs& a, bool pdl, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if (a.corr) {  // the learned correction runs with MUSCL + HLLC (checked when it is attached)
-        const int rows = rows_per_warp(a.g.nx, a.g.ny, a.ph.precision == EFVM_PREC_FP32_FLUX ? 8 : 5);
+        using F32 = StageForm<float, false>;
+        using F64 = StageForm<double, false>;
+        const bool fp32 = a.ph.precision == EFVM_PREC_FP32_FLUX;
+        const int rows = rows_per_warp(a.g.nx, a.g.ny, form_minb(fp32, false));
         dim3 grid((stage_strips(a.g.nx) + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
-        if (a.ph.precision == EFVM_PREC_FP32_FLUX)
-            launch_k(stage_kernel<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, float, 8, true>, grid, dim3(32 * WPB), s, pdl, a, rows);
+        if (fp32)
+            launch_k(stage_kernel<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, float, F32::MINB, false, true, F32::XFIRST>, grid,
+                     dim3(32 * WPB), s, pdl, a, rows);
         else
-            launch_k(stage_kernel<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, double, 5, true>, grid, dim3(32 * WPB), s, pdl, a,
-                     rows);
+            launch_k(stage_kernel<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, double, F64::MINB, false, true, F64::XFIRST>, grid,
+                     dim3(32 * WPB), s, pdl, a, rows);
         return 1;
     }
     if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_r<float>(a, pdl, s);
@@ -1145,13 +1179,20 @@ int launch_stage(const StageArgs& a, bool pdl, void* stream) {
 
 int stage_strips(int nx) { return (nx + STRIP - 1) / STRIP; }
 
-int stage_rows(int nx, int ny, bool fp32) { return rows_per_warp(nx, ny, fp32 ? 8 : 5); }
+int stage_rows(int nx, int ny, bool fp32, bool viscous) { return rows_per_warp(nx, ny, form_minb(fp32, viscous)); }
+
+template <int SCHEME, int RECON, class R, bool VISC>
+static void launch_batch_f(const BatchStageArgs& b, int n_tiles, bool pdl, cudaStream_t s) {
+    using F = StageForm<R, VISC>;
+    launch_k(batch_stage_kernel<SCHEME, RECON, R, F::MINB, VISC, F::XFIRST>, dim3((n_tiles + WPB - 1) / WPB),
+             dim3(32 * WPB), s, pdl, b, n_tiles);
+}
 
 template <int SCHEME, int RECON, class R>
 static void launch_batch_t(const BatchStageArgs& b, int n_tiles, bool pdl, cudaStream_t s) {
-    constexpr int MINB = sizeof(R) == sizeof(double) ? 5 : 8;
-    launch_k(batch_stage_kernel<SCHEME, RECON, R, MINB>, dim3((n_tiles + WPB - 1) / WPB), dim3(32 * WPB), s, pdl, b,
-             n_tiles);
+    // every case of a batch shares the viscous setting
+    if (b.ph.viscous) launch_batch_f<SCHEME, RECON, R, true>(b, n_tiles, pdl, s);
+    else launch_batch_f<SCHEME, RECON, R, false>(b, n_tiles, pdl, s);
 }
 
 template <class R>
