@@ -261,9 +261,9 @@ __device__ __forceinline__ Q4<R> shfl_down_q(const Q4<R>& u, int d) {
                  __shfl_down_sync(0xffffffffu, u.mt, d), __shfl_down_sync(0xffffffffu, u.E, d)};
 }
 
-// Primitive (u, v, T) of a state (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
-__device__ __forceinline__ void prim_uvt(const U4& u, double gm1, double r_gas, double& vu, double& vv, double& t) {
-    const double inv = rcp_(u.r);
+// Primitive (u, v, T) of a state given 1/rho (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
+__device__ __forceinline__ void prim_uvt(const U4& u, double inv, double gm1, double r_gas, double& vu, double& vv,
+                                         double& t) {
     vu = u.mx * inv;
     vv = u.my * inv;
     const double ke = 0.5 * u.r * (vu * vu + vv * vv);
@@ -444,17 +444,34 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 const bool solid = ibm && a.mask[o];
                 if (VISC && !solid) {
                     // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D)
-                    double us, vs, ts;
-                    prim_uvt(ucd, gm1, ph.r_gas, us, vs, ts);
                     double nu[4], nv[4], nt[4];  // +x, -x, +y, -y
                     const U4 nbs[4] = {ld(i + 1, j), ld(i - 1, j), FP64 ? toU4(un) : ld(i, j + 1), ld(i, j - 1)};
                     const long long no[4] = {o + 1, o - 1, o + g.pitch, o - g.pitch};
+                    bool sn[4];  // solid neighbours take (0, 0, T of the cell)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) sn[k] = ibm && a.mask[no[k]];
+                    // the five reciprocal densities from one reciprocal of their
+                    // product (running products forward, then peeled off backward)
+                    const double r0 = ucd.r, r1 = sn[0] ? 1.0 : nbs[0].r, r2 = sn[1] ? 1.0 : nbs[1].r;
+                    const double r3 = sn[2] ? 1.0 : nbs[2].r, r4 = sn[3] ? 1.0 : nbs[3].r;
+                    const double p1 = r0 * r1, p2 = p1 * r2, p3 = p2 * r3;
+                    double w = rcp_(p3 * r4);
+                    const double i4 = p3 * w;
+                    w = w * r4;
+                    const double i3 = p2 * w;
+                    w = w * r3;
+                    const double i2 = p1 * w;
+                    w = w * r2;
+                    const double ninv[4] = {r0 * w, i2, i3, i4};
+                    const double i0 = r1 * w;
+                    double us, vs, ts;
+                    prim_uvt(ucd, i0, gm1, ph.r_gas, us, vs, ts);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        if (ibm && a.mask[no[k]]) {
+                        if (sn[k]) {
                             nu[k] = 0.0; nv[k] = 0.0; nt[k] = ts;
                         } else {
-                            prim_uvt(nbs[k], gm1, ph.r_gas, nu[k], nv[k], nt[k]);
+                            prim_uvt(nbs[k], ninv[k], gm1, ph.r_gas, nu[k], nv[k], nt[k]);
                         }
                     }
                     const double y_im = a.yw[j], y_ip = a.yw[g.ny + j], y_is = a.yw[2 * g.ny + j];

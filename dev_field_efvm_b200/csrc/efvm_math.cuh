@@ -43,13 +43,6 @@ __device__ __forceinline__ double rcp_(double b) {
     return fma(r, e, r);
 }
 __device__ __forceinline__ float rcp_(float b) { return __fdividef(1.0f, b); }
-// a / b as q = a (1/b) followed by one residual correction q + (1/b)(a - b q).
-__device__ __forceinline__ double div_(double a, double b) {
-    const double r = rcp_(b);
-    const double q = a * r;
-    return fma(r, fma(-b, q, a), q);
-}
-__device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
 // 1/sqrt(x) by Newton-Raphson on f(y) = 1/y^2 - x, y <- y (3/2 - x y^2 / 2),
 // seeded with the PTX approximate rsqrt.approx.ftz.f64; two iterations.
 __device__ __forceinline__ double rsqrt_(double x) {
@@ -70,9 +63,9 @@ struct Side {
     R inv, un, ut, q, p, a;
 };
 template <class R>
-__device__ __forceinline__ Side<R> side_of(const Q4<R>& u, R gamma, R gm1) {
+__device__ __forceinline__ Side<R> side_with(const Q4<R>& u, R inv, R gamma, R gm1) {
     Side<R> s;
-    s.inv = rcp_(u.r);
+    s.inv = inv;
     s.un = u.mn * s.inv;
     s.ut = u.mt * s.inv;
     s.q = s.un * s.un + s.ut * s.ut;
@@ -80,6 +73,14 @@ __device__ __forceinline__ Side<R> side_of(const Q4<R>& u, R gamma, R gm1) {
     const R a2 = gamma * s.p * s.inv;
     s.a = a2 * rsqrt_(a2);  // sqrt(a2); NaN for a non-physical p <= 0, which the stage flags
     return s;
+}
+// Both sides of a face, with 1/rho_L = rho_R w and 1/rho_R = rho_L w from one
+// reciprocal w = 1/(rho_L rho_R) (a few ulps from the two separate reciprocals).
+template <class R>
+__device__ __forceinline__ void sides_of(const Q4<R>& L, const Q4<R>& Rr, R gamma, R gm1, Side<R>& l, Side<R>& r) {
+    const R w = rcp_(L.r * Rr.r);
+    l = side_with(L, Rr.r * w, gamma, gm1);
+    r = side_with(Rr, L.r * w, gamma, gm1);
 }
 
 // physical_flux_inline along the face normal for a state with known normal
@@ -98,7 +99,8 @@ __device__ __forceinline__ Q4<R> physical_flux(R rho, R un, R ut, R E, R p) {
 // Rusanov::flux_inline, crates/cfd_riemann/src/lib.rs:222-240
 template <class R>
 __device__ __forceinline__ Q4<R> rusanov_flux(const Q4<R>& L, const Q4<R>& Rr, R gamma, R gm1) {
-    const Side<R> l = side_of(L, gamma, gm1), r = side_of(Rr, gamma, gm1);
+    Side<R> l, r;
+    sides_of(L, Rr, gamma, gm1, l, r);
     const Q4<R> fl = physical_flux(L.r, l.un, l.ut, L.E, l.p);
     const Q4<R> fr = physical_flux(Rr.r, r.un, r.ut, Rr.E, r.p);
     const R hl = R(0.5) * fmax_(fabs_(l.un) + l.a, fabs_(r.un) + r.a);
@@ -121,11 +123,16 @@ __device__ __forceinline__ Q4<R> rusanov_flux(const Q4<R>& L, const Q4<R>& Rr, R
 //  * the upwind side K (left for s_l >= 0 or s_* >= 0, else right) is selected
 //    first and one star state is built, F = F(U_K) + s_K (U*_K - U_K), with
 //    rho_* = f_K/(s_K - s_*) and p_K/(rho_K (s_K - u_K)) = p_K/f_K where
-//    f_K = rho_K (s_K - u_K) is the same factor that enters s_*.
+//    f_K = rho_K (s_K - u_K) is the same factor that enters s_*;
+//  * s_* = n/d is only formed on the faces that need its value (the star
+//    regions); elsewhere its sign is read from the signs of n and d.  Where it
+//    is formed, s_* and 1/(f_K (s_K - s_*)) = d/(f_K (s_K d - n)) come from one
+//    reciprocal of d f_K (s_K d - n).
 // The results agree with the literal evaluation to a few ulps.
 template <class R, bool THORNBER>
 __device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R gamma, R gm1) {
-    const Side<R> l = side_of(L, gamma, gm1), r = side_of(Rr, gamma, gm1);
+    Side<R> l, r;
+    sides_of(L, Rr, gamma, gm1, l, r);
     R lcn = l.un, lct = l.ut, rcn = r.un, rct = r.ut, ELc = L.E, ERc = Rr.E;
     if (THORNBER) {
         const R vmax2 = fmax_(l.q, r.q);
@@ -147,8 +154,11 @@ __device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R ga
     const R s_r = fmax_(lcn + l.a, rcn + r.a);
     const R fac_l = L.r * (s_l - lcn);
     const R fac_r = Rr.r * (s_r - rcn);
-    const R s_star = div_((r.p - l.p) + fac_l * lcn - fac_r * rcn, fac_l - fac_r);
-    const bool useL = (s_l >= R(0)) || (s_star >= R(0));
+    const R num = (r.p - l.p) + fac_l * lcn - fac_r * rcn;
+    const R den = fac_l - fac_r;
+    // s_* = num / den >= 0 without the division (false for den = 0 or NaN)
+    const bool star_nonneg = den > R(0) ? num >= R(0) : (den < R(0) ? num <= R(0) : false);
+    const bool useL = (s_l >= R(0)) || star_nonneg;
     const R rK = useL ? L.r : Rr.r;
     const R uK = useL ? lcn : rcn;
     const R tK = useL ? lct : rct;
@@ -156,12 +166,16 @@ __device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R ga
     const R pK = useL ? l.p : r.p;
     const R iK = useL ? l.inv : r.inv;
     Q4<R> f = physical_flux(rK, uK, tK, EK, pK);
-    if (s_l < R(0) && (s_star >= R(0) || s_r >= R(0))) {  // one of the two star regions
+    if (s_l < R(0) && (star_nonneg || s_r >= R(0))) {  // one of the two star regions
         const R sK = useL ? s_l : s_r;
         const R facK = useL ? fac_l : fac_r;
-        // rho_* = f_K / d_K and p_K / f_K from one reciprocal of f_K d_K (d_K = s_K - s_*)
+        // s_* = num/den and inv = 1/(f_K d_K), d_K = s_K - s_*, from one reciprocal;
+        // rho_* = f_K / d_K and p_K / f_K follow from inv
+        const R X = facK * (sK * den - num);
+        const R w = rcp_(den * X);
+        const R s_star = num * (X * w);
         const R dK = sK - s_star;
-        const R inv = rcp_(facK * dK);
+        const R inv = den * den * w;
         const R rho_star = facK * facK * inv;
         const R e_star = EK * iK + (s_star - uK) * (s_star + pK * dK * inv);
         f.r = f.r + sK * (rho_star - rK);
