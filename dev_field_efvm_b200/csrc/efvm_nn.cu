@@ -98,13 +98,19 @@ struct Net {
     float gamma;
 };
 
+// Periodic index for -n <= i < 2n.  Every caller is within 3 cells of the
+// grid (the 5x5 stencil, the residual's neighbours) and every entry point
+// requires nx, ny >= 5, so one conditional wrap replaces an integer modulo
+// (whose division sequence would run per stencil cell).
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
 // Conserved states [B][4][n][n] (FP64, periodic), as the training batches hold them.
 struct PackedStates {
     const double* q;
     int nx, ny;
     __device__ double get(int b, int v, int i, int j) const {
-        i = (i % nx + nx) % nx;
-        j = (j % ny + ny) % ny;
+        i = wrap(i, nx);
+        j = wrap(j, ny);
         return q[(((long long)b * 4 + v) * ny + j) * nx + i];
     }
 };
@@ -114,8 +120,8 @@ struct PaddedState {
     long long plane;
     int pitch, nx, ny;
     __device__ double get(int, int v, int i, int j) const {
-        i = (i % nx + nx) % nx;
-        j = (j % ny + ny) % ny;
+        i = wrap(i, nx);
+        j = wrap(j, ny);
         return q[(long long)v * plane + (long long)(YO + j) * pitch + XO + i];
     }
 };
@@ -152,6 +158,16 @@ struct FaceId {
 __device__ __forceinline__ FaceId face_of(long long f, int nx, int ny) {
     const long long per = 2LL * nx * ny;
     FaceId id;
+    if (f < 0x7fffffffLL && per < 0x7fffffffLL) {  // the same quotients in 32-bit arithmetic
+        const unsigned uf = (unsigned)f, up = (unsigned)per, un = (unsigned)nx * (unsigned)ny;
+        id.b = (int)(uf / up);
+        unsigned rem = uf - (unsigned)id.b * up;
+        id.orient = (int)(rem / un);
+        rem -= (unsigned)id.orient * un;
+        id.j = (int)(rem / (unsigned)nx);
+        id.i = (int)(rem - (unsigned)id.j * (unsigned)nx);
+        return id;
+    }
     id.b = (int)(f / per);
     long long rem = f - (long long)id.b * per;
     id.orient = (int)(rem / ((long long)nx * ny));
@@ -179,8 +195,8 @@ struct PrimView {
     const float4* p;
     int nx, ny;
     __device__ float4 get(int b, int i, int j) const {
-        i = (i % nx + nx) % nx;
-        j = (j % ny + ny) % ny;
+        i = wrap(i, nx);
+        j = wrap(j, ny);
         return p[((long long)b * ny + j) * nx + i];
     }
 };
@@ -528,17 +544,17 @@ __global__ void nn_residual_kernel(const float* __restrict__ corr, const double*
         const long long cell = t - (long long)b * n;
         const int j = (int)(cell / nx), i = (int)(cell - (long long)j * nx);
         auto cx = [&](int v, int ii, int jj) {  // x-face correction on the left of cell (ii, jj)
-            ii = (ii % nx + nx) % nx;
-            jj = (jj % ny + ny) % ny;
+            ii = wrap(ii, nx);
+            jj = wrap(jj, ny);
             return (double)corr[((long long)(b * 2 + 0) * 4 + v) * n + (long long)jj * nx + ii];
         };
         auto cy = [&](int v, int ii, int jj) {
-            ii = (ii % nx + nx) % nx;
-            jj = (jj % ny + ny) % ny;
+            ii = wrap(ii, nx);
+            jj = wrap(jj, ny);
             return (double)corr[((long long)(b * 2 + 1) * 4 + v) * n + (long long)jj * nx + ii];
         };
         auto err = [&](int v, int ii, int jj) {
-            const int i2 = (ii % nx + nx) % nx, j2 = (jj % ny + ny) % ny;
+            const int i2 = wrap(ii, nx), j2 = wrap(jj, ny);
             const double div = (cx(v, ii + 1, jj) - cx(v, ii, jj)) * inv_dx + (cy(v, ii, jj + 1) - cy(v, ii, jj)) * inv_dy;
             return resid[((long long)b * 4 + v) * n + (long long)j2 * nx + i2] + div;
         };
