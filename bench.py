@@ -360,7 +360,10 @@ def main():
                 "traffic": traffic, "peak_source": peak_kind,
                 "kernel": "stage_kernel (fused MUSCL/HLLC/viscous/RK3 substage)",
                 "stage_ms_per_launch": stage_ms_per_launch,
-                "share_of_step": prof[0] / prof[3] if prof[3] > 0 else None}
+                # the three stage launches per step against the graph-timed step above
+                # (the per-kernel events of the profile pass wait on the host between
+                # stages, so its own whole-step time is not a step of the timed loop)
+                "share_of_step": 3 * stage_ms_per_launch / (ms / args.steps)}
 
     # ---- chosen form: FP32 reconstruction/fluxes, FP64 accumulation -------
     p32 = abi.make_params(**{f: getattr(params, f) for f, _ in abi.EfvmParams._fields_})
