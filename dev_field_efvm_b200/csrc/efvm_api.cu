@@ -33,6 +33,7 @@ struct efvm_ctx {
     double* U[3] = {nullptr, nullptr, nullptr};  // U0 (= u^n), U1, U2
     uint8_t* mask = nullptr;
     double* yw = nullptr;                          // viscous y weights
+    double* zw = nullptr;                          // viscous z weights (3-D)
     DevState* st = nullptr;                        // device
     double* partial = nullptr;                     // reduction partials
     int n_partial = 0;
@@ -122,6 +123,12 @@ double* cur_buf(efvm_ctx* c) {
     if (c->params.integrator == EFVM_INTEGRATOR_EULER) return c->U[c->euler_cur];
     return c->U[c->rk_stage];
 }
+
+// Entry points built for the 2-D layout answer a 3-D context (nz > 1) with this.
+int refuse_3d(efvm_ctx* c, const char* what) {
+    return fail(c, EFVM_ERR_UNSUPPORTED, std::string(what) + " is built for 2-D meshes (nz == 1)");
+}
+bool is_3d(const efvm_ctx* c) { return c && c->g.nz > 1; }
 
 int ensure_staging(efvm_ctx* c, size_t bytes) {
     if (c->staging_bytes >= bytes) return EFVM_OK;
@@ -298,6 +305,7 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
     a.uout = uout;
     a.mask = c->ibm ? c->mask : nullptr;
     a.yw = c->yw;
+    a.zw = c->zw;
     a.st = c->st;
     a.stage = stage;
     a.completes_step = (stage == 2 || stage == 3) ? 1 : 0;
@@ -395,8 +403,15 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
         err = m;
         return code;
     };
-    if (gr.nz != 1) return bad(EFVM_ERR_UNSUPPORTED, "only 2-D meshes (nz == 1) are supported");
+    if (gr.nz < 1) return bad(EFVM_ERR_INVALID_ARG, "nz must be >= 1");
     if (gr.ng != 2) return bad(EFVM_ERR_UNSUPPORTED, "only ng == 2 ghost layers are supported");
+    const bool d3 = gr.nz > 1;  // a 3-D mesh: 5 conserved planes, z faces (efvm_kernels3d.cuh)
+    if (d3) {
+        if (slab) return bad(EFVM_ERR_UNSUPPORTED, "slabs are built for 2-D meshes (nz == 1)");
+        if (p.precision != EFVM_PREC_FP64) return bad(EFVM_ERR_UNSUPPORTED, "3-D meshes run in FP64");
+        if (p.parabolic_inflow || p.sponge)
+            return bad(EFVM_ERR_UNSUPPORTED, "the parabolic inlet and the outlet sponge are 2-D case systems");
+    }
     if (gr.nx < 2 || gr.ny < 1) return bad(EFVM_ERR_INVALID_ARG, "nx must be >= 2 and ny >= 1");
     for (int a = 0; a < 3; ++a)
         if (!(gr.hi[a] > gr.lo[a])) return bad(EFVM_ERR_INVALID_ARG, "bounds_hi must exceed bounds_lo");
@@ -411,7 +426,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
         if (!bc_supported(gr.bc[s].kind)) return bad(EFVM_ERR_INVALID_ARG, "unknown boundary kind");
     if ((gr.bc[EFVM_XLO].kind == EFVM_BC_PERIODIC && gr.nx < 2) || (gr.bc[EFVM_YLO].kind == EFVM_BC_PERIODIC && gr.ny < 2))
         return bad(EFVM_ERR_INVALID_ARG, "a periodic axis needs at least 2 cells (two ghost layers wrap)");
-    if (gr.bc[EFVM_ZLO].kind == EFVM_BC_PERIODIC)
+    if (!d3 && gr.bc[EFVM_ZLO].kind == EFVM_BC_PERIODIC)
         return bad(EFVM_ERR_UNSUPPORTED, "a periodic z axis has no meaning on a 2-D mesh");
     if (!(p.gamma > 1.0) || !(p.r_gas > 0.0)) return bad(EFVM_ERR_INVALID_ARG, "gamma must exceed 1, r_gas > 0");
     if (!(p.cfl > 0.0) && !(p.fixed_dt > 0.0)) return bad(EFVM_ERR_INVALID_ARG, "cfl or fixed_dt must be > 0");
@@ -431,6 +446,9 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     g.j_off = row0;
     g.pitch = ((XO + gr.nx + NG) + 7) / 8 * 8;
     g.plane = ((long long)(rows + 2 * YO) * g.pitch + 31) / 32 * 32;
+    g.nz = gr.nz;
+    g.layer = (long long)(rows + 2 * YO) * g.pitch;
+    if (d3) g.plane = ((long long)(gr.nz + 4) * g.layer + 31) / 32 * 32;
     const int n[3] = {gr.nx, gr.ny, gr.nz};
     for (int a = 0; a < 3; ++a) {
         g.lo[a] = gr.lo[a];
@@ -440,6 +458,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     g.cell_volume = g.h[0] * g.h[1] * g.h[2];
     g.inv_x = (g.h[1] * g.h[2]) / g.cell_volume;
     g.inv_y = (g.h[0] * g.h[2]) / g.cell_volume;
+    g.inv_z = (g.h[0] * g.h[1]) / g.cell_volume;
     ph.gamma = p.gamma;
     ph.r_gas = p.r_gas;
     ph.cfl = p.cfl;
@@ -455,6 +474,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     ph.periodic_seam = p.periodic_seam;
     ph.periodic_x = gr.bc[EFVM_XLO].kind == EFVM_BC_PERIODIC;
     ph.periodic_y = gr.bc[EFVM_YLO].kind == EFVM_BC_PERIODIC;
+    ph.periodic_z = d3 && gr.bc[EFVM_ZLO].kind == EFVM_BC_PERIODIC;
     if (slab) {
         // the periodic wrap of y, like the edges between slabs, goes through halos
         const bool per_y = ph.periodic_y != 0;
@@ -464,7 +484,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
         ph.seam_yhi = per_y && row0 + rows == gr.ny;
         ph.periodic_y = 0;
     }
-    for (int s = 0; s < 4; ++s) {
+    for (int s = 0; s < 6; ++s) {
         ph.bc[s].kind = gr.bc[s].kind;
         ph.bc[s].rho = gr.bc[s].rho;
         ph.bc[s].u = gr.bc[s].u;
@@ -507,6 +527,19 @@ std::vector<double> viscous_y_weights(const Geometry& g) {
     return yw;
 }
 
+// The same weights along z (z_im, z_ip, z_is per layer) for a 3-D mesh.
+std::vector<double> viscous_z_weights(const Geometry& g) {
+    std::vector<double> zw(3 * (size_t)g.nz);
+    for (int k = 0; k < g.nz; ++k) {
+        const double hm = centre_h(g.lo[2], g.h[2], k) - centre_h(g.lo[2], g.h[2], k - 1);
+        const double hp = centre_h(g.lo[2], g.h[2], k + 1) - centre_h(g.lo[2], g.h[2], k);
+        zw[k] = 1.0 / hm;
+        zw[g.nz + k] = 1.0 / hp;
+        zw[2 * g.nz + k] = 2.0 / (hm + hp);
+    }
+    return zw;
+}
+
 }  // namespace efvm
 
 extern "C" {
@@ -546,7 +579,7 @@ static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t
         delete c;
         return EFVM_ERR_CUDA;
     }
-    const size_t state_bytes = (size_t)4 * g.plane * sizeof(double);
+    const size_t state_bytes = (size_t)(g.nz > 1 ? 5 : 4) * g.plane * sizeof(double);
     for (int k = 0; k < 3; ++k) {
         e = cudaMalloc(&c->U[k], state_bytes);
         if (e != cudaSuccess) {
@@ -561,6 +594,12 @@ static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t
     const std::vector<double> yw = viscous_y_weights(g);
     if (cudaMalloc(&c->yw, yw.size() * sizeof(double)) != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
     cudaMemcpyAsync(c->yw, yw.data(), yw.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (g.nz > 1) {
+        const std::vector<double> zw = viscous_z_weights(g);
+        if (cudaMalloc(&c->zw, zw.size() * sizeof(double)) != cudaSuccess)
+            return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
+        cudaMemcpyAsync(c->zw, zw.data(), zw.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    }
     if (cudaMalloc(&c->st, sizeof(DevState)) != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc"));
     DevState s0{};
     s0.active = 1;
@@ -596,6 +635,7 @@ int efvm_destroy(efvm_ctx* c) {
     for (int k = 0; k < 3; ++k) cudaFree(c->U[k]);
     cudaFree(c->mask);
     cudaFree(c->yw);
+    cudaFree(c->zw);
     cudaFree(c->st);
     cudaFree(c->partial);
     cudaFree(c->staging);
@@ -655,11 +695,55 @@ static int transfer_state(efvm_ctx* c, double* base, int64_t si, int64_t sj, int
 }
 
 int efvm_upload_state(efvm_ctx* c, const double* base, int64_t si, int64_t sj, int64_t sv) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_upload_state (use efvm_upload_state_3d)");
     return transfer_state(c, const_cast<double*>(base), si, sj, sv, true);
 }
 
 int efvm_download_state(efvm_ctx* c, double* base, int64_t si, int64_t sj, int64_t sv) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_download_state (use efvm_download_state_3d)");
     return transfer_state(c, base, si, sj, sv, false);
+}
+
+// The 3-D form of transfer_state: element (i, j, k, v) at i si + j sj + k sk + v sv.
+static int transfer_state3(efvm_ctx* c, double* base, int64_t si, int64_t sj, int64_t sk, int64_t sv, bool upload) {
+    if (!c || !base) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (!is_3d(c)) return transfer_state(c, base, si, sj, sv, upload);
+    const Geometry& g = c->g;
+    int64_t lo = 0, hi = 0;
+    const int64_t corners[4] = {(int64_t)(g.nx - 1) * si, (int64_t)(g.ny - 1) * sj, (int64_t)(g.nz - 1) * sk, 4 * sv};
+    for (int k = 0; k < 4; ++k) {
+        lo += std::min<int64_t>(0, corners[k]);
+        hi += std::max<int64_t>(0, corners[k]);
+    }
+    const int64_t span = hi - lo + 1;
+    const bool dense = span == (int64_t)g.nx * g.ny * g.nz * 5;
+    int rc = ensure_staging(c, (size_t)span * sizeof(double));
+    if (rc) return rc;
+    double* host0 = base + lo;
+    double* dev0 = c->staging - lo;
+    double* q = cur_buf(c);
+    if (upload) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->staging, host0, (size_t)span * sizeof(double), cudaMemcpyHostToDevice, S(c)));
+        c->launches += launch_pack3(g, dev0, si, sj, sk, sv, q, 1, S(c));
+        c->lam_stale = true;
+        c->ghosts_stale = true;
+    } else {
+        if (!dense)
+            CUDA_TRY(c, cudaMemcpyAsync(c->staging, host0, (size_t)span * sizeof(double), cudaMemcpyHostToDevice, S(c)));
+        c->launches += launch_pack3(g, dev0, si, sj, sk, sv, q, 0, S(c));
+        CUDA_TRY(c, cudaMemcpyAsync(host0, c->staging, (size_t)span * sizeof(double), cudaMemcpyDeviceToHost, S(c)));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    CUDA_TRY(c, cudaGetLastError());
+    return EFVM_OK;
+}
+
+int efvm_upload_state_3d(efvm_ctx* c, const double* base, int64_t si, int64_t sj, int64_t sk, int64_t sv) {
+    return transfer_state3(c, const_cast<double*>(base), si, sj, sk, sv, true);
+}
+
+int efvm_download_state_3d(efvm_ctx* c, double* base, int64_t si, int64_t sj, int64_t sk, int64_t sv) {
+    return transfer_state3(c, base, si, sj, sk, sv, false);
 }
 
 int efvm_get_solver_state(efvm_ctx* c, efvm_solver_state* out) {
@@ -701,6 +785,7 @@ int efvm_set_flux_correction(efvm_ctx* c, efvm_nn* nn, float sensor) {
         c->graph_valid = false;
         return EFVM_OK;
     }
+    if (is_3d(c)) return refuse_3d(c, "the flux correction");
     if (!c->ph.periodic_x || !c->ph.periodic_y || has_halo(c) || c->ibm)
         return fail(c, EFVM_ERR_UNSUPPORTED, "the flux correction needs a periodic grid without IBM or slabs");
     if (c->params.reconstruction != EFVM_RECON_MUSCL || c->params.flux_scheme != EFVM_FLUX_HLLC || c->ph.viscous)
@@ -722,6 +807,7 @@ int efvm_set_flux_correction(efvm_ctx* c, efvm_nn* nn, float sensor) {
 }
 
 int efvm_output_fields(efvm_ctx* c, double* host_out, int32_t async) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_output_fields");
     if (!c || !host_out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     const size_t bytes = (size_t)7 * c->g.nx * c->g.ny * sizeof(double);
     if (!c->out_fields) CUDA_TRY(c, cudaMalloc(&c->out_fields, bytes));
@@ -738,6 +824,7 @@ int efvm_synchronize(efvm_ctx* c) {
 }
 
 int efvm_write_vtk(efvm_ctx* c, const char* path) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_write_vtk");
     if (!c || !path) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     const int nx = c->g.nx, ny = c->g.ny;
     const long long n = (long long)nx * ny;
@@ -792,6 +879,7 @@ int efvm_write_vtk(efvm_ctx* c, const char* path) {
 }
 
 int efvm_body_loads(efvm_ctx* c, int32_t n_bodies, double* out) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_body_loads");
     if (!c || !out || n_bodies < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid argument");
     if (!c->ibm) return fail(c, EFVM_ERR_INVALID_ARG, "efvm_body_loads: no cylinders are set");
     const int nb = (int)(c->cyl_host.size() / 3);
@@ -845,6 +933,7 @@ int efvm_prepare(efvm_ctx* c) {
 }
 
 static int halo_rows(efvm_ctx* c, int32_t side, double* buf, int unpack) {
+    if (is_3d(c)) return refuse_3d(c, "the slab halo exchange");
     if (!c || !buf) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     if (side != EFVM_YLO && side != EFVM_YHI) return fail(c, EFVM_ERR_INVALID_ARG, "side must be EFVM_YLO or EFVM_YHI");
     if (c->g.ny < 2) return fail(c, EFVM_ERR_INVALID_ARG, "halo rows need ny >= 2");
@@ -865,6 +954,7 @@ int efvm_halo_unpack(efvm_ctx* c, int32_t side, const double* dev_buf) {
 }
 
 int efvm_wave_speed_slot(efvm_ctx* c, uint64_t** dev_slot) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_wave_speed_slot");
     if (!c || !dev_slot) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     DevState s;
     int rc = read_state(c, s);
@@ -999,6 +1089,7 @@ int efvm_cfl(efvm_ctx* c, double* dt_out) {
 }
 
 int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const double fs[5]) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_set_cylinders");
     if (!c || (n > 0 && (!cyl || !fs)) || n < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid cylinder arguments");
     if (n == 0) {
         c->ibm = false;
@@ -1055,6 +1146,7 @@ int efvm_ibm_counts(efvm_ctx* c, int64_t* n_solid, int64_t* n_ghost) {
 }
 
 int efvm_get_solid_mask(efvm_ctx* c, uint8_t* out) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_get_solid_mask");
     if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     if (c->ibm && c->geom_dirty) {
         int rc = prologue(c);
@@ -1068,6 +1160,7 @@ int efvm_get_solid_mask(efvm_ctx* c, uint8_t* out) {
 }
 
 int efvm_density_error(efvm_ctx* c, const efvm_vortex* v, double out[2]) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_density_error");
     if (!c || !v || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     c->launches += launch_density_error(c->g, *v, cur_buf(c), c->st, c->partial, c->n_partial, S(c));
     std::vector<double> part(2 * (size_t)c->n_partial);
@@ -1085,6 +1178,7 @@ int efvm_density_error(efvm_ctx* c, const efvm_vortex* v, double out[2]) {
 }
 
 int efvm_init_vortex(efvm_ctx* c, const efvm_vortex* v) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_init_vortex");
     if (!c || !v) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     c->launches += launch_init_vortex(c->g, *v, cur_buf(c), S(c));
     c->lam_stale = true;

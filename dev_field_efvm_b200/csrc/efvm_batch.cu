@@ -261,6 +261,11 @@ int efvm_batch_create(const efvm_grid* grids, int32_t n_cases, const efvm_params
     b->phc.resize(n_cases);
     for (int k = 0; k < n_cases; ++k) {
         std::string err;
+        if (grids[k].nz != 1) {
+            delete b;
+            return bfail(nullptr, EFVM_ERR_UNSUPPORTED, "efvm_batch_create: case " + std::to_string(k) +
+                                                            ": batches hold 2-D cases (nz == 1)");
+        }
         const int rc = setup_case(grids[k], *params, 0, grids[k].ny, false, b->g[k], b->phc[k], err);
         if (rc) {
             delete b;

@@ -8,6 +8,9 @@
 //   (rows likewise).  XO = 4 makes every interior row start on a 32-byte
 //   sector; the pitch is a multiple of 8 doubles.  rho_w is identically zero in
 //   2-D and is not stored.
+// A 3-D state (nz > 1) has 5 planes (rho, rho_u, rho_v, rho_w, rho_e), each
+// (nz + 4) layers of `layer` doubles; interior cell (i, j, k) sits in layer 2 + k
+// (efvm_kernels3d.cuh).
 #pragma once
 
 #include <cstdint>
@@ -54,6 +57,10 @@ struct Geometry {
     int nx, ny;
     int pitch;            // doubles per row
     long long plane;      // doubles per plane
+    int nz;               // 1 for the 2-D layout
+    int pad3_;
+    long long layer;      // doubles per z layer (3-D)
+    double inv_z;         // face area / cell volume for z faces
     double lo[3], hi[3];
     double h[3];          // spacing dx, dy, dz
     double inv_x, inv_y;  // face area / cell volume for x and y faces
@@ -69,12 +76,12 @@ struct Physics {
     int viscous, viscosity_model;
     double mu;
     int precision, periodic_seam;
-    int periodic_x, periodic_y;
+    int periodic_x, periodic_y, periodic_z, pad_z;
     // Slabs (efvm_create_slab): a y side whose ghosts come from a neighbouring
     // slab, and whether that side is the global periodic seam.
     int halo_ylo, halo_yhi;
     int seam_ylo, seam_yhi;
-    DevBC bc[4];  // XLO, XHI, YLO, YHI
+    DevBC bc[6];  // XLO, XHI, YLO, YHI, ZLO, ZHI
     int parabolic_inflow;
     double inflow_u_max, inflow_height, inflow_rho;
     int sponge;
@@ -143,6 +150,7 @@ struct StageArgs {
     double* uout;
     const uint8_t* __restrict__ mask; // solid mask (same layout as one plane, bytes) or null
     const double* __restrict__ yw;    // 3*ny viscous y weights: y_im, y_ip, y_is
+    const double* __restrict__ zw;    // 3*nz viscous z weights (3-D) or null
     DevState* st;
     int stage;                        // 0,1,2 for RK3; 3 = Euler
     int completes_step;               // sponge + CFL + clock in the epilogue
@@ -194,6 +202,7 @@ int nn_prepare_launches();
 int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bool slab, Geometry& g, Physics& ph,
                std::string& err);
 std::vector<double> viscous_y_weights(const Geometry& g);
+std::vector<double> viscous_z_weights(const Geometry& g);
 
 // Sets the message efvm_last_error(NULL) returns (efvm_api.cu).
 void set_global_error(const std::string& msg);
@@ -213,6 +222,9 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
 int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, DevState* st,
                int force_stage, int mirror_stage, int setup, bool pdl, void* stream);
 int launch_pack(const Geometry& g, const double* host_like, int64_t si, int64_t sj, int64_t sv, double* q,
+                 int to_device, void* stream);
+// The same for a 3-D state: element (i, j, k, v) at i si + j sj + k sk + v sv.
+int launch_pack3(const Geometry& g, double* host_like, int64_t si, int64_t sj, int64_t sk, int64_t sv, double* q,
                  int to_device, void* stream);
 int launch_init_vortex(const Geometry& g, const efvm_vortex& v, double* q, void* stream);
 int launch_density_error(const Geometry& g, const efvm_vortex& v, const double* q, const DevState* st,

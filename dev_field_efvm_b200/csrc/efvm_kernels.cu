@@ -1173,8 +1173,11 @@ static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
     else launch_stage_v<R, false>(a, pdl, s);
 }
 
+#include "efvm_kernels3d.cuh"
+
 int launch_stage(const StageArgs& a, bool pdl, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
+    if (a.g.nz > 1) return launch_stage3(a, pdl, s);
     if (a.corr) {  // the learned correction runs with MUSCL + HLLC (checked when it is attached)
         using F32 = StageForm<float, false>;
         using F64 = StageForm<double, false>;
@@ -1251,6 +1254,10 @@ int launch_clock(unsigned long long* out, void* stream) {
 
 int launch_fill_ghosts(const Geometry& g, const Physics& ph, double* q, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
+    if (g.nz > 1) {
+        fill_ghosts3_kernel<<<grid_for((long long)g.nx * g.ny * g.nz, 256), 256, 0, s>>>(g, ph, q);
+        return 1;
+    }
     fill_ghosts_x_kernel<<<(g.ny + 127) / 128, 128, 0, s>>>(g, ph, q);
     fill_ghosts_y_kernel<<<(g.nx + 127) / 128, 128, 0, s>>>(g, ph, q);
     return 2;
@@ -1259,6 +1266,10 @@ int launch_fill_ghosts(const Geometry& g, const Physics& ph, double* q, void* st
 int launch_cfl(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     reset_lam_kernel<<<1, 1, 0, s>>>(st);
+    if (g.nz > 1) {
+        cfl3_kernel<<<grid_for((long long)g.nx * g.ny * g.nz, 256), 256, 0, s>>>(g, ph, q, st);
+        return 2;
+    }
     cfl_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, s>>>(g, ph, q, st);
     return 2;
 }
@@ -1416,12 +1427,23 @@ int launch_density_error(const Geometry& g, const efvm_vortex& v, const double* 
 }
 
 int launch_total_mass(const Geometry& g, const double* q, double* partial, int nblocks, void* stream) {
+    if (g.nz > 1) {
+        total_mass3_kernel<<<nblocks, 256, 0, (cudaStream_t)stream>>>(g, q, partial);
+        return 1;
+    }
     total_mass_kernel<<<nblocks, 256, 0, (cudaStream_t)stream>>>(g, q, partial);
     return 1;
 }
 
 int launch_check_state(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream) {
     check_state_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(g, ph, q, st);
+    return 1;
+}
+
+int launch_pack3(const Geometry& g, double* host_like, int64_t si, int64_t sj, int64_t sk, int64_t sv, double* q,
+                 int to_device, void* stream) {
+    pack3_kernel<<<grid_for((long long)g.nx * g.ny * g.nz, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, host_like, si, sj, sk, sv, q, to_device);
     return 1;
 }
 

@@ -1,0 +1,539 @@
+// efvm_kernels3d.cuh — the 3-D (nz > 1) forms of the stage, ghost-fill, CFL,
+// transfer and mass kernels.  Included by efvm_kernels.cu inside namespace
+// efvm after its 2-D helpers (the rounding wrappers, the gas model, the launch
+// helper), which these kernels share.
+//
+// HBM layout of one 3-D state: 5 FP64 planes (rho, rho_u, rho_v, rho_w,
+// rho_e), each (nz + 2 ZO) layers of (ny + 2 YO) rows x `pitch` doubles; cell
+// (i, j, k) sits at layer ZO + k, row YO + j, column XO + i.  Layers ZO-2,
+// ZO-1 and ZO+nz, ZO+nz+1 are the two z ghost layers of FIELD's ng = 2.
+//
+// The stage kernel keeps the 2-D kernel's organisation: a warp owns a strip of
+// 31 columns of one layer k and marches `rows` rows with the carried y window,
+// the x faces come from warp shuffles, and each lane also forms the two z
+// faces of its cell from the layers k-2..k+2 of its column.  A z face between
+// layers k and k+1 is formed by the warps of both layers; both go through the
+// same (non-unrolled) loop body, so the two results agree bit for bit and the
+// scheme stays conservative across layers.
+
+namespace {
+
+constexpr int ZO = 2;  // layer of interior cell k = 0
+
+__device__ __forceinline__ long long cidx3(const Geometry& g, int i, int j, int k) {
+    return (long long)(ZO + k) * g.layer + (long long)(YO + j) * g.pitch + (XO + i);
+}
+
+struct U5 {
+    double r, mx, my, mz, E;
+};
+__device__ __forceinline__ U5 load5(const double* q, long long P, long long o) {
+    return U5{q[o], q[P + o], q[2 * P + o], q[3 * P + o], q[4 * P + o]};
+}
+__device__ __forceinline__ void store5(double* q, long long P, long long o, const U5& u) {
+    q[o] = u.r;
+    q[P + o] = u.mx;
+    q[2 * P + o] = u.my;
+    q[3 * P + o] = u.mz;
+    q[4 * P + o] = u.E;
+}
+
+// IdealGas::pressure (crates/cfd_eos/src/lib.rs:61-64) and prim_to_cons (:55-59),
+// every operation rounded explicitly (evaluated by the stage epilogue and the
+// stand-alone ghost fill / CFL pass alike).
+__device__ __forceinline__ double pressure5(const U5& u, double gm1) {
+    const double mm = add_(add_(mul_(u.mx, u.mx), mul_(u.my, u.my)), mul_(u.mz, u.mz));
+    return mul_(gm1, sub_(u.E, mul_(0.5, mm) / u.r));
+}
+__device__ __forceinline__ U5 prim_to_cons5(double rho, double u, double v, double w, double p, double gm1) {
+    const double ke = mul_(mul_(0.5, rho), add_(add_(mul_(u, u), mul_(v, v)), mul_(w, w)));
+    return U5{rho, mul_(rho, u), mul_(rho, v), mul_(rho, w), add_(p / gm1, ke)};
+}
+
+// BoundaryCondition::ghost_at, crates/cfd_boundary/src/lib.rs:172-362, for
+// side 0..5 (XLO, XHI, YLO, YHI, ZLO, ZHI).
+__device__ __forceinline__ U5 bc_ghost5(const DevBC& bc, int side, const U5& in, double gm1) {
+    switch (bc.kind) {
+        case EFVM_BC_SLIP_WALL:
+        case EFVM_BC_SYMMETRY: {
+            double n[3] = {0.0, 0.0, 0.0};
+            n[side / 2] = (side % 2 == 1) ? 1.0 : -1.0;
+            const double mn = add_(add_(mul_(in.mx, n[0]), mul_(in.my, n[1])), mul_(in.mz, n[2]));
+            U5 g = in;
+            g.mx = sub_(in.mx, mul_(mul_(2.0, mn), n[0]));
+            g.my = sub_(in.my, mul_(mul_(2.0, mn), n[1]));
+            g.mz = sub_(in.mz, mul_(mul_(2.0, mn), n[2]));
+            return g;
+        }
+        case EFVM_BC_NO_SLIP_WALL:
+            return U5{in.r, -in.mx, -in.my, -in.mz, in.E};
+        case EFVM_BC_SUPERSONIC_INFLOW:
+            return prim_to_cons5(bc.rho, bc.u, bc.v, bc.w, bc.p, gm1);
+        case EFVM_BC_SUBSONIC_INFLOW:
+            return prim_to_cons5(bc.rho, bc.u, bc.v, bc.w, pressure5(in, gm1), gm1);
+        case EFVM_BC_PRESSURE_OUTLET: {
+            const double inv = 1.0 / in.r;
+            return prim_to_cons5(in.r, mul_(in.mx, inv), mul_(in.my, inv), mul_(in.mz, inv), bc.p, gm1);
+        }
+        default:
+            return in;
+    }
+}
+
+// The Halo (periodic wrap of both ghost layers) and Boundary (first ghost
+// layer) phases for the ghosts whose source is interior cell (i, j, k) with
+// value u, written by the thread that owns that cell.
+__device__ __forceinline__ void write_ghosts3(const Geometry& g, const Physics& ph, double* q, int i, int j, int k,
+                                              const U5& u) {
+    const long long P = g.plane;
+    const double gm1 = ph.gamma - 1.0;
+    if (ph.periodic_x) {
+        if (i >= g.nx - NG) store5(q, P, cidx3(g, i - g.nx, j, k), u);
+        if (i < NG) store5(q, P, cidx3(g, i + g.nx, j, k), u);
+    } else {
+        if (i == 0) store5(q, P, cidx3(g, -1, j, k), bc_ghost5(ph.bc[0], 0, u, gm1));
+        if (i == g.nx - 1) store5(q, P, cidx3(g, g.nx, j, k), bc_ghost5(ph.bc[1], 1, u, gm1));
+    }
+    if (ph.periodic_y) {
+        if (j >= g.ny - NG) store5(q, P, cidx3(g, i, j - g.ny, k), u);
+        if (j < NG) store5(q, P, cidx3(g, i, j + g.ny, k), u);
+    } else {
+        if (j == 0) store5(q, P, cidx3(g, i, -1, k), bc_ghost5(ph.bc[2], 2, u, gm1));
+        if (j == g.ny - 1) store5(q, P, cidx3(g, i, g.ny, k), bc_ghost5(ph.bc[3], 3, u, gm1));
+    }
+    if (ph.periodic_z) {
+        if (k >= g.nz - NG) store5(q, P, cidx3(g, i, j, k - g.nz), u);
+        if (k < NG) store5(q, P, cidx3(g, i, j, k + g.nz), u);
+    } else {
+        if (k == 0) store5(q, P, cidx3(g, i, j, -1), bc_ghost5(ph.bc[4], 4, u, gm1));
+        if (k == g.nz - 1) store5(q, P, cidx3(g, i, j, g.nz), bc_ghost5(ph.bc[5], 5, u, gm1));
+    }
+}
+
+// Local max wave speed of cfl_system, crates/cfd_solver/src/lib.rs:647-669.
+__device__ __forceinline__ double wave_speed3(const Geometry& g, const Physics& ph, const U5& u) {
+    if (!(u.r > 0.0)) return 0.0;
+    const double gm1 = ph.gamma - 1.0;
+    const double inv = 1.0 / u.r;
+    const double vx = mul_(u.mx, inv), vy = mul_(u.my, inv), vz = mul_(u.mz, inv);
+    const double p = pressure5(u, gm1);
+    const double a = sqrt(mul_(ph.gamma, p) / u.r);
+    double lam = add_(add_(add_(fabs(vx), a) / g.h[0], add_(fabs(vy), a) / g.h[1]), add_(fabs(vz), a) / g.h[2]);
+    if (ph.viscous) {
+        const double ke = mul_(mul_(0.5, u.r), add_(add_(mul_(vx, vx), mul_(vy, vy)), mul_(vz, vz)));
+        const double pp = mul_(gm1, sub_(u.E, ke));
+        const double t = mul_(pp, inv) / ph.r_gas;
+        const double nu = viscosity(ph, t) / u.r;
+        lam = add_(lam, mul_(mul_(2.0, nu), ph.cfl_visc_sum));
+    }
+    return lam;
+}
+
+// A conserved state in the grid frame and its face-frame views.
+struct V5 {
+    double r, mx, my, mz, E;
+};
+__device__ __forceinline__ V5 toV5(const U5& u) { return V5{u.r, u.mx, u.my, u.mz, u.E}; }
+__device__ __forceinline__ U5 toU5(const V5& u) { return U5{u.r, u.mx, u.my, u.mz, u.E}; }
+__device__ __forceinline__ Q5<double> xq5(const V5& u) { return Q5<double>{u.r, u.mx, u.my, u.mz, u.E}; }
+__device__ __forceinline__ Q5<double> yq5(const V5& u) { return Q5<double>{u.r, u.my, u.mx, u.mz, u.E}; }
+__device__ __forceinline__ Q5<double> zq5(const V5& u) { return Q5<double>{u.r, u.mz, u.mx, u.my, u.E}; }
+// A face flux back in the grid frame (x, y, z faces).
+__device__ __forceinline__ V5 xg5(const Q5<double>& f) { return V5{f.r, f.mn, f.mt, f.ms, f.E}; }
+__device__ __forceinline__ V5 yg5(const Q5<double>& f) { return V5{f.r, f.mt, f.mn, f.ms, f.E}; }
+__device__ __forceinline__ V5 zg5(const Q5<double>& f) { return V5{f.r, f.mt, f.ms, f.mn, f.E}; }
+
+// The +face and -face states c +- s/2 of a cell, s = lim(p - c, c - m)
+// (limited_slope_cons and reconstruct_to_face, crates/cfd_solver/src/lib.rs:199-211,273-286).
+__device__ __forceinline__ void slope_faces5(int limiter, const V5& m, const V5& c, const V5& p, V5& plus, V5& minus) {
+    const double hr = half_slope(limiter, m.r, c.r, p.r), hx = half_slope(limiter, m.mx, c.mx, p.mx);
+    const double hy = half_slope(limiter, m.my, c.my, p.my), hz = half_slope(limiter, m.mz, c.mz, p.mz);
+    const double he = half_slope(limiter, m.E, c.E, p.E);
+    plus = V5{c.r + hr, c.mx + hx, c.my + hy, c.mz + hz, c.E + he};
+    minus = V5{c.r - hr, c.mx - hx, c.my - hy, c.mz - hz, c.E - he};
+}
+
+__device__ __forceinline__ V5 shfl_up5(const V5& u, int d) {
+    return V5{__shfl_up_sync(0xffffffffu, u.r, d), __shfl_up_sync(0xffffffffu, u.mx, d),
+              __shfl_up_sync(0xffffffffu, u.my, d), __shfl_up_sync(0xffffffffu, u.mz, d),
+              __shfl_up_sync(0xffffffffu, u.E, d)};
+}
+__device__ __forceinline__ V5 shfl_down5(const V5& u, int d) {
+    return V5{__shfl_down_sync(0xffffffffu, u.r, d), __shfl_down_sync(0xffffffffu, u.mx, d),
+              __shfl_down_sync(0xffffffffu, u.my, d), __shfl_down_sync(0xffffffffu, u.mz, d),
+              __shfl_down_sync(0xffffffffu, u.E, d)};
+}
+
+// Primitive (u, v, w, T) of a state given 1/rho (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
+__device__ __forceinline__ void prim5(const U5& u, double inv, double gm1, double r_gas, double& vu, double& vv,
+                                      double& vw, double& t) {
+    vu = u.mx * inv;
+    vv = u.my * inv;
+    vw = u.mz * inv;
+    const double ke = 0.5 * u.r * (vu * vu + vv * vv + vw * vw);
+    t = gm1 * (u.E - ke) * inv / r_gas;
+}
+
+constexpr int MINB3 = 4;  // resident blocks per SM of the 3-D stage kernel (128 registers)
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// The 3-D stage kernel: one RK substage of layer blockIdx.z.
+// ---------------------------------------------------------------------------
+template <int SCHEME, int RECON, bool VISC>
+__global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, int rows) {
+    pdl_wait_then_release();
+    if (!a.st->active) return;
+    const Geometry& g = a.g;
+    const Physics& ph = a.ph;
+    const long long P = g.plane;
+    const int lane = threadIdx.x & 31;
+    const int strip = blockIdx.x * WPB + (threadIdx.x >> 5);
+    const int by = blockIdx.y, k = blockIdx.z;
+    if (strip == 0 && by == 0 && k == 0 && lane == 0) {
+        // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
+        DevState* st = a.st;
+        if (a.stage >= 2) {
+            st->rk_stage = 0;
+            st->completed = 1;
+            st->step += 1;
+            st->time += st->dt;
+        } else {
+            st->rk_stage = a.stage + 1;
+            st->completed = 0;
+        }
+    }
+    const int i0 = strip * STRIP;
+    const int jb = by * rows;
+    double lam = 0.0;
+    if (i0 < g.nx && jb < g.ny) {  // uniform across the warp
+        constexpr bool MUSCL = RECON == EFVM_RECON_MUSCL;
+        const int je = min(jb + rows, g.ny);
+        const int i = i0 + lane;
+        const int ic = min(i, g.nx + NG - 1);
+        const bool owner = lane < STRIP && i < g.nx;
+        const bool true_seam = ph.periodic_seam == EFVM_SEAM_TRUE_PERIODIC;
+        const double gm1 = ph.gamma - 1.0;
+        const double rg = ph.gamma;
+        const double* __restrict__ uin = a.uin;
+        auto ld = [&](int ii, int jj, int kk) { return load5(uin, P, cidx3(g, ii, jj, kk)); };
+        const double* __restrict__ colp = uin + cidx3(g, ic, 0, k);
+        auto ldrow = [&](int jj) { return toV5(load5(colp, P, (long long)jj * g.pitch)); };
+        auto ldz = [&](int jj, int dk) { return toV5(load5(colp, P, (long long)jj * g.pitch + (long long)dk * g.layer)); };
+
+        // reconstruction flags of the faces on the domain edges (as the 2-D kernel)
+        bool rec_l = MUSCL, rec_r = MUSCL;
+        if (i == 0) {
+            rec_l = MUSCL && ph.periodic_x && true_seam;
+            rec_r = MUSCL && ph.periodic_x;
+        } else if (i == g.nx) {
+            rec_l = MUSCL && ph.periodic_x;
+            rec_r = MUSCL && ph.periodic_x && true_seam;
+        }
+        const bool seam_rec_y = MUSCL && ph.periodic_y && true_seam;
+        const bool edge_rec_y = MUSCL && ph.periodic_y;
+        // z faces: below (k - 1/2) and above (k + 1/2); side A is the lower cell
+        bool zrA[2] = {MUSCL, MUSCL}, zrB[2] = {MUSCL, MUSCL};
+        if (k == 0) {
+            zrA[0] = MUSCL && ph.periodic_z && true_seam;
+            zrB[0] = MUSCL && ph.periodic_z;
+        }
+        if (k == g.nz - 1) {
+            zrA[1] = MUSCL && ph.periodic_z;
+            zrB[1] = MUSCL && ph.periodic_z && true_seam;
+        }
+        const double dt = a.st->dt;
+
+        V5 uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
+        if (MUSCL) {
+            V5 unused;
+            slope_faces5(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
+        }
+        V5 gb;  // flux of the y face below row j, grid frame
+        for (int j = jb - 1; j < je; ++j) {
+            const V5 un2 = ldrow(j + 2);
+            const bool row = j >= jb;  // warp-uniform: the first pass only forms the face below row jb
+
+            // Flux divergence in the reference's accumulation order for an interior
+            // cell: the z face below, the y face below, the x face on the left (all
+            // scattered when their owners were visited), then the cell's own +x, +y
+            // and +z faces (for_each_face order, crates/cfd_solver/src/lib.rs:333-337).
+            double part[5];
+            V5 fzt;
+            if (row) {
+                // ---- the two z faces of the cell, one code path ----
+                const V5 zm1 = ldz(j, -1), zp1 = ldz(j, 1);
+                V5 zm2 = zm1, zp2 = zp1;
+                if (MUSCL) {
+                    zm2 = ldz(j, -2);
+                    zp2 = ldz(j, 2);
+                }
+                V5 fzb;
+#pragma unroll 1
+                for (int s = 0; s < 2; ++s) {
+                    const V5 A_lo = s ? zm1 : zm2, A = s ? uc : zm1, B = s ? zp1 : uc, B_hi = s ? zp2 : zp1;
+                    V5 L = A, Rv = B;
+                    if (MUSCL) {
+                        V5 pl, mi;
+                        if (s ? zrA[1] : zrA[0]) {
+                            slope_faces5(ph.limiter, A_lo, A, B, pl, mi);
+                            L = pl;
+                        }
+                        if (s ? zrB[1] : zrB[0]) {
+                            slope_faces5(ph.limiter, A, B, B_hi, pl, mi);
+                            Rv = mi;
+                        }
+                    }
+                    const V5 f = zg5(face_flux5<SCHEME, double>(zq5(L), zq5(Rv), rg, gm1));
+                    if (s) fzt = f;
+                    else fzb = f;
+                }
+
+                // ---- x face on the left of column i ----
+                V5 ul = shfl_up5(uc, 1), ur = shfl_down5(uc, 1);
+                V5 ull = ul;
+                if (lane == 0) {
+                    ul = toV5(ld(i0 - 1, j, k));
+                    if (MUSCL) ull = toV5(ld(i0 - 2, j, k));
+                }
+                if (MUSCL && lane == 31) ur = toV5(ld(min(i0 + 32, g.nx + NG - 1), j, k));
+                Q5<double> xl = xq5(ul), xr = xq5(uc);
+                if (MUSCL) {
+                    V5 pp, mm;
+                    slope_faces5(ph.limiter, ul, uc, ur, pp, mm);
+                    V5 lp = shfl_up5(pp, 1);
+                    if (lane == 0) {
+                        V5 unused;
+                        slope_faces5(ph.limiter, ull, ul, uc, lp, unused);
+                    }
+                    xl = xq5(rec_l ? lp : ul);
+                    xr = xq5(rec_r ? mm : uc);
+                }
+                const V5 fx = xg5(face_flux5<SCHEME, double>(xl, xr, rg, gm1));
+                const V5 fxr = shfl_down5(fx, 1);
+                const double zb[5] = {fzb.r, fzb.mx, fzb.my, fzb.mz, fzb.E};
+                const double yb[5] = {gb.r, gb.mx, gb.my, gb.mz, gb.E};
+                const double fl[5] = {fx.r, fx.mx, fx.my, fx.mz, fx.E};
+                const double fr[5] = {fxr.r, fxr.mx, fxr.my, fxr.mz, fxr.E};
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                    double acc = __dmul_rn(zb[v], g.inv_z);
+                    acc = __dadd_rn(acc, __dmul_rn(yb[v], g.inv_y));
+                    acc = __dadd_rn(acc, __dmul_rn(fl[v], g.inv_x));
+                    part[v] = __dsub_rn(acc, __dmul_rn(fr[v], g.inv_x));
+                }
+            }
+
+            // ---- y face above row j ----
+            V5 pn = un;
+            Q5<double> yb_, yt_;
+            if (MUSCL) {
+                V5 mn;
+                slope_faces5(ph.limiter, uc, un, un2, pn, mn);
+                const bool lo_edge = j == -1, hi_edge = j + 1 == g.ny;
+                const bool rb = lo_edge ? seam_rec_y : (hi_edge ? edge_rec_y : true);
+                const bool rt = lo_edge ? edge_rec_y : (hi_edge ? seam_rec_y : true);
+                yb_ = yq5(rb ? pc : uc);
+                yt_ = yq5(rt ? mn : un);
+            } else {
+                yb_ = yq5(uc);
+                yt_ = yq5(un);
+            }
+            const V5 gt = yg5(face_flux5<SCHEME, double>(yb_, yt_, rg, gm1));
+
+            if (row && owner) {
+                const long long o = cidx3(g, i, j, k);
+                const U5 ucd = toU5(uc);
+                const double yt[5] = {gt.r, gt.mx, gt.my, gt.mz, gt.E};
+                const double zt[5] = {fzt.r, fzt.mx, fzt.my, fzt.mz, fzt.E};
+                double rhs[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v)
+                    rhs[v] = __dsub_rn(__dsub_rn(part[v], __dmul_rn(yt[v], g.inv_y)), __dmul_rn(zt[v], g.inv_z));
+                if (VISC) {
+                    // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (7-point stencil)
+                    const U5 nbs[6] = {ld(i + 1, j, k), ld(i - 1, j, k), toU5(un), ld(i, j - 1, k),
+                                       ld(i, j, k + 1), ld(i, j, k - 1)};
+                    // the seven reciprocal densities from one reciprocal of their product
+                    double pr[7];
+                    pr[0] = ucd.r;
+#pragma unroll
+                    for (int n = 0; n < 6; ++n) pr[n + 1] = pr[n] * nbs[n].r;
+                    double w = rcp_(pr[6]);
+                    double inv[7];
+#pragma unroll
+                    for (int n = 6; n >= 1; --n) {
+                        inv[n] = pr[n - 1] * w;
+                        w = w * nbs[n - 1].r;  // now 1 / pr[n - 1]
+                    }
+                    inv[0] = w;
+                    double us, vs, ws, ts;
+                    prim5(ucd, inv[0], gm1, ph.r_gas, us, vs, ws, ts);
+                    double nu[6], nv[6], nw[6], nt[6];  // +x, -x, +y, -y, +z, -z
+#pragma unroll
+                    for (int n = 0; n < 6; ++n) prim5(nbs[n], inv[n + 1], gm1, ph.r_gas, nu[n], nv[n], nw[n], nt[n]);
+                    const double y_im = a.yw[j], y_ip = a.yw[g.ny + j], y_is = a.yw[2 * g.ny + j];
+                    const double z_im = a.zw[k], z_ip = a.zw[g.nz + k], z_is = a.zw[2 * g.nz + k];
+                    const double dxi2 = ph.dx_inv2;
+                    auto d2x = [&](double m, double p, double c) { return (p - 2.0 * c + m) * dxi2; };
+                    auto d2y = [&](double m, double p, double c) { return ((p - c) * y_ip - (c - m) * y_im) * y_is; };
+                    auto d2z = [&](double m, double p, double c) { return ((p - c) * z_ip - (c - m) * z_im) * z_is; };
+                    const double mu = viscosity(ph, ts);
+                    const double kappa = mu * ph.cp / 0.72;  // thermal_conductivity, crates/cfd_eos/src/lib.rs:83-87
+                    const double fxv = mu * (d2x(nu[1], nu[0], us) + d2y(nu[3], nu[2], us) + d2z(nu[5], nu[4], us));
+                    const double fyv = mu * (d2x(nv[1], nv[0], vs) + d2y(nv[3], nv[2], vs) + d2z(nv[5], nv[4], vs));
+                    const double fzv = mu * (d2x(nw[1], nw[0], ws) + d2y(nw[3], nw[2], ws) + d2z(nw[5], nw[4], ws));
+                    const double d2t = d2x(nt[1], nt[0], ts) + d2y(nt[3], nt[2], ts) + d2z(nt[5], nt[4], ts);
+                    rhs[1] += fxv;
+                    rhs[2] += fyv;
+                    rhs[3] += fzv;
+                    rhs[4] += us * fxv + vs * fyv + ws * fzv + kappa * d2t;
+                }
+                if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
+                    rhs[1] += ucd.r * ph.body_force_x;
+                    rhs[4] += ph.body_force_x * ucd.mx;
+                }
+                // Rk3Integrator / EulerIntegrator::substep, crates/cfd_solver/src/integrate.rs:48-101
+                const double ucv[5] = {ucd.r, ucd.mx, ucd.my, ucd.mz, ucd.E};
+                double nwv[5];
+                if (a.stage == 1 || a.stage == 2) {
+                    const double w0 = a.stage == 1 ? 0.75 : (1.0 / 3.0);
+                    const double w1 = a.stage == 1 ? 0.25 : (2.0 / 3.0);
+#pragma unroll
+                    for (int v = 0; v < 5; ++v)
+                        nwv[v] = __dadd_rn(__dmul_rn(w0, a.u0[v * P + o]),
+                                           __dmul_rn(w1, __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt))));
+                } else {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) nwv[v] = __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt));
+                }
+                const U5 nwu{nwv[0], nwv[1], nwv[2], nwv[3], nwv[4]};
+                store5(a.uout, P, o, nwu);
+                write_ghosts3(g, ph, a.uout, i, j, k, nwu);
+                int bad = 0;
+                if (!(nwu.r > 0.0)) bad |= 1;
+                if (!(2.0 * nwu.E * nwu.r > nwu.mx * nwu.mx + nwu.my * nwu.my + nwu.mz * nwu.mz)) bad |= 2;
+                if (nwu.r != nwu.r || nwu.mx != nwu.mx || nwu.my != nwu.my || nwu.mz != nwu.mz || nwu.E != nwu.E)
+                    bad |= 4;
+                if (bad) atomicOr(&a.st->nonphysical, bad);
+                if (a.completes_step && a.want_cfl) lam = fmax(lam, wave_speed3(g, ph, nwu));
+            }
+            gb = gt;
+            uc = un;
+            un = un2;
+            pc = pn;
+        }
+    }
+    if (a.completes_step && a.want_cfl) {
+        for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
+        if (lane == 0 && lam > 0.0 && lam == lam)
+            atomicMax(lam_slot(a.st), (unsigned long long)__double_as_longlong(lam));
+    }
+}
+
+// Halo + Boundary of a whole 3-D state (after an upload): every interior cell
+// writes the ghosts it is the source of, as the stage epilogue does.
+__global__ void fill_ghosts3_kernel(Geometry g, Physics ph, double* q) {
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ((long long)g.nx * g.ny));
+        const long long r = t - (long long)k * g.nx * g.ny;
+        const int j = (int)(r / g.nx), i = (int)(r - (long long)j * g.nx);
+        write_ghosts3(g, ph, q, i, j, k, load5(q, g.plane, cidx3(g, i, j, k)));
+    }
+}
+
+__global__ void cfl3_kernel(Geometry g, Physics ph, const double* __restrict__ q, DevState* st) {
+    double lam = 0.0;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ((long long)g.nx * g.ny));
+        const long long r = t - (long long)k * g.nx * g.ny;
+        const int j = (int)(r / g.nx), i = (int)(r - (long long)j * g.nx);
+        lam = fmax(lam, wave_speed3(g, ph, load5(q, g.plane, cidx3(g, i, j, k))));
+    }
+    block_max_atomic(lam, lam_slot(st));
+}
+
+// Strided host-like buffer (element (i, j, k, v) at i si + j sj + k sk + v sv)
+// to or from the device layout.
+__global__ void pack3_kernel(Geometry g, double* h, int64_t si, int64_t sj, int64_t sk, int64_t sv, double* q,
+                             int to_device) {
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ((long long)g.nx * g.ny));
+        const long long r = t - (long long)k * g.nx * g.ny;
+        const int j = (int)(r / g.nx), i = (int)(r - (long long)j * g.nx);
+        const long long o = cidx3(g, i, j, k);
+        double* e = h + i * si + j * sj + k * sk;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            if (to_device) q[v * g.plane + o] = e[v * sv];
+            else e[v * sv] = q[v * g.plane + o];
+        }
+    }
+}
+
+__global__ void total_mass3_kernel(Geometry g, const double* __restrict__ q, double* partial) {
+    __shared__ double s1[256];
+    double a = 0.0;
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ((long long)g.nx * g.ny));
+        const long long r = t - (long long)k * g.nx * g.ny;
+        const int j = (int)(r / g.nx), i = (int)(r - (long long)j * g.nx);
+        a += q[cidx3(g, i, j, k)] * g.cell_volume;
+    }
+    s1[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) s1[threadIdx.x] += s1[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = s1[0];
+}
+
+// ---- launches ---------------------------------------------------------------
+// Rows per warp of the 3-D stage: the fewest that fill the resident slots in one
+// wave, clamped to [2, 8] as in 2-D.
+static int rows_per_warp3(int nx, int ny, int nz) {
+    const long long strips = (nx + STRIP - 1) / STRIP;
+    const long long slots = 148LL * MINB3 * WPB;
+    long long rows = (strips * ny * nz + slots - 1) / slots;
+    if (rows < 2) rows = 2;
+    if (rows > 8) rows = 8;
+    return (int)rows;
+}
+
+template <int SCHEME, int RECON, bool VISC>
+static void launch_stage3_t(const StageArgs& a, bool pdl, cudaStream_t s) {
+    const int rows = rows_per_warp3(a.g.nx, a.g.ny, a.g.nz);
+    const int strips = (a.g.nx + STRIP - 1) / STRIP;
+    dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows, a.g.nz);
+    launch_k(stage3_kernel<SCHEME, RECON, VISC>, grid, dim3(32 * WPB), s, pdl, a, rows);
+}
+
+template <bool VISC>
+static void launch_stage3_v(const StageArgs& a, bool pdl, cudaStream_t s) {
+    const bool muscl = a.ph.reconstruction == EFVM_RECON_MUSCL;
+    switch (a.ph.flux_scheme) {
+        case EFVM_FLUX_RUSANOV:
+            muscl ? launch_stage3_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, VISC>(a, pdl, s)
+                  : launch_stage3_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, VISC>(a, pdl, s);
+            break;
+        case EFVM_FLUX_HLLC_TEXTBOOK:
+            muscl ? launch_stage3_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, VISC>(a, pdl, s)
+                  : launch_stage3_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, VISC>(a, pdl, s);
+            break;
+        default:
+            muscl ? launch_stage3_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, VISC>(a, pdl, s)
+                  : launch_stage3_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, VISC>(a, pdl, s);
+    }
+}
+
+static int launch_stage3(const StageArgs& a, bool pdl, cudaStream_t s) {
+    if (a.ph.viscous) launch_stage3_v<true>(a, pdl, s);
+    else launch_stage3_v<false>(a, pdl, s);
+    return 1;
+}

@@ -20,7 +20,7 @@ _LIB = None
 # every entry point of include/efvm.h
 EXPORTS = (
     "efvm_abi_version", "efvm_create", "efvm_destroy", "efvm_last_error", "efvm_upload_state",
-    "efvm_download_state", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
+    "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
@@ -56,6 +56,8 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_last_error.argtypes = [vp]
     L.efvm_upload_state.argtypes = [vp, dp, i64, i64, i64]
     L.efvm_download_state.argtypes = [vp, dp, i64, i64, i64]
+    L.efvm_upload_state_3d.argtypes = [vp, dp, i64, i64, i64, i64]
+    L.efvm_download_state_3d.argtypes = [vp, dp, i64, i64, i64, i64]
     L.efvm_get_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.efvm_set_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.efvm_substep.argtypes = [vp]
@@ -125,7 +127,7 @@ class Context:
         """rows = (row0, n): a slab of global rows [row0, row0 + n) (efvm_create_slab)."""
         self.L = load()
         self.grid, self.params = grid, params
-        self.nx = grid.nx
+        self.nx, self.nz = grid.nx, grid.nz
         self.row0, self.ny = (0, grid.ny) if rows is None else (int(rows[0]), int(rows[1]))
         h = C.c_void_p()
         if rows is None:
@@ -159,7 +161,12 @@ class Context:
 
     # conserved state as an (ny, nx, 5) array: rho, rho_u, rho_v, rho_w, rho_e
     def upload(self, u: np.ndarray) -> None:
+        """u: [ny, nx, 5] (2-D) or [nz, ny, nx, 5] (3-D) conserved states."""
         u = np.ascontiguousarray(u, dtype=np.float64)
+        if self.nz > 1:
+            assert u.shape == (self.nz, self.ny, self.nx, 5), u.shape
+            self._check(self.L.efvm_upload_state_3d(self.h, _dp(u), 5, 5 * self.nx, 5 * self.nx * self.ny, 1))
+            return
         assert u.shape == (self.ny, self.nx, 5), u.shape
         self._check(self.L.efvm_upload_state(self.h, _dp(u), 5, 5 * self.nx, 1))
 
@@ -167,6 +174,11 @@ class Context:
         self._check(self.L.efvm_upload_state(self.h, C.cast(ptr, C.POINTER(C.c_double)), si, sj, sv))
 
     def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if self.nz > 1:
+            if out is None:
+                out = np.zeros((self.nz, self.ny, self.nx, 5))
+            self._check(self.L.efvm_download_state_3d(self.h, _dp(out), 5, 5 * self.nx, 5 * self.nx * self.ny, 1))
+            return out
         if out is None:
             out = np.zeros((self.ny, self.nx, 5))
         self._check(self.L.efvm_download_state(self.h, _dp(out), 5, 5 * self.nx, 1))
@@ -174,6 +186,12 @@ class Context:
 
     def download_ptr(self, ptr: int, si: int, sj: int, sv: int) -> None:
         self._check(self.L.efvm_download_state(self.h, C.cast(ptr, C.POINTER(C.c_double)), si, sj, sv))
+
+    def upload_ptr3(self, ptr: int, si: int, sj: int, sk: int, sv: int) -> None:
+        self._check(self.L.efvm_upload_state_3d(self.h, C.cast(ptr, C.POINTER(C.c_double)), si, sj, sk, sv))
+
+    def download_ptr3(self, ptr: int, si: int, sj: int, sk: int, sv: int) -> None:
+        self._check(self.L.efvm_download_state_3d(self.h, C.cast(ptr, C.POINTER(C.c_double)), si, sj, sk, sv))
 
     def substep(self) -> None:
         self._check(self.L.efvm_substep(self.h))

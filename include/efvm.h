@@ -66,10 +66,13 @@ typedef struct {
     double rho, u, v, w, p, t; /* parameters of the inflow/outlet kinds */
 } efvm_bc;
 
-/* A 2-D uniform mesh (FIELD UniformMeshConfig{nx,ny,nz,ng,bounds_lo,bounds_hi}
- * with nz == 1 and ng == 2) plus one boundary condition per side
- * (BoundaryRegistry, crates/cfd_boundary/src/lib.rs:370-449).  The z extent
- * enters the CFL (crates/cfd_solver/src/lib.rs:659-661) and the marker area. */
+/* A uniform mesh (FIELD UniformMeshConfig{nx,ny,nz,ng,bounds_lo,bounds_hi}
+ * with ng == 2) plus one boundary condition per side (BoundaryRegistry,
+ * crates/cfd_boundary/src/lib.rs:370-449).  nz == 1 is the 2-D form of the
+ * benchmark cases: the z extent enters the CFL (crates/cfd_solver/src/lib.rs:
+ * 659-661) and the marker area.  nz > 1 is a 3-D mesh with z faces (FP64; no
+ * IBM, slabs, batches, flux correction or output fields; state through
+ * efvm_upload_state_3d / efvm_download_state_3d). */
 typedef struct {
     int32_t nx, ny, nz, ng;
     double lo[3], hi[3];
@@ -168,8 +171,8 @@ typedef struct efvm_ctx efvm_ctx;
  * GasPlugin + BoundaryPlugin/StructuredBoundaryPlugin + FluxPlugin/MusclPlugin
  * + IntegratorPlugin + SolverPlugin + app.prepare()
  * (crates/cfd_solver/src/lib.rs:691-940, crates/cfd_boundary/src/lib.rs:
- * 457-533).  Validates the configuration (half-periodic axes, nz != 1, ng != 2
- * are rejected) and allocates the device state.  The state must then be
+ * 457-533).  Validates the configuration (half-periodic axes, ng != 2 and, on
+ * 3-D meshes, the 2-D-only options are rejected) and allocates the device state.  The state must then be
  * uploaded (the reference's init_state_system, crates/cfd_solver/src/lib.rs:
  * 681-686, is a host closure). */
 int efvm_create(const efvm_grid* grid, const efvm_params* params, efvm_ctx** out);
@@ -191,6 +194,15 @@ int efvm_upload_state(efvm_ctx* ctx, const double* base, int64_t stride_i, int64
 /* The inverse of efvm_upload_state; writes rho_w = 0. */
 int efvm_download_state(efvm_ctx* ctx, double* base, int64_t stride_i, int64_t stride_j,
                         int64_t stride_var);
+/* The state of a 3-D context (nz > 1), as CfdState.u over all layers: element
+ * (i,j,k) component v (0..4 = rho, rho_u, rho_v, rho_w, rho_e) at
+ * base[i*stride_i + j*stride_j + k*stride_k + v*stride_var].  On a 2-D context
+ * they act as efvm_upload_state / efvm_download_state (stride_k unused).  The
+ * 2-D calls above refuse a 3-D context. */
+int efvm_upload_state_3d(efvm_ctx* ctx, const double* base, int64_t stride_i, int64_t stride_j, int64_t stride_k,
+                         int64_t stride_var);
+int efvm_download_state_3d(efvm_ctx* ctx, double* base, int64_t stride_i, int64_t stride_j, int64_t stride_k,
+                           int64_t stride_var);
 
 int efvm_get_solver_state(efvm_ctx* ctx, efvm_solver_state* out);
 /* Restores dt/time/step/rk_stage (checkpoint resume, crates/cfd_solver/src/

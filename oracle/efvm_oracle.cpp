@@ -1024,6 +1024,35 @@ int oracle_download_state(void* hp, double* base, int64_t si, int64_t sj, int64_
     return EFVM_OK;
 }
 
+// 3-D forms: element (i, j, k, v) at i si + j sj + k sk + v sv over all layers.
+int oracle_upload_state3(void* hp, const double* base, int64_t si, int64_t sj, int64_t sk, int64_t sv) {
+    Case& cs = ((OracleHandle*)hp)->cs;
+    const Mesh& m = cs.mesh;
+    for (int k = 0; k < m.N[2]; ++k)
+        for (int j = 0; j < m.N[1]; ++j)
+            for (int i = 0; i < m.N[0]; ++i) {
+                const int ii = std::min(std::max(i - m.ng, 0), m.n[0] - 1);
+                const int jj = std::min(std::max(j - m.ng, 0), m.n[1] - 1);
+                const int kk = std::min(std::max(k - m.ng, 0), m.n[2] - 1);
+                const double* e = base + ii * si + jj * sj + kk * sk;
+                cs.u[m.idx_raw(i, j, k)] = ConsVar(e[0], e[sv], e[2 * sv], e[3 * sv], e[4 * sv]);
+            }
+    return EFVM_OK;
+}
+
+int oracle_download_state3(void* hp, double* base, int64_t si, int64_t sj, int64_t sk, int64_t sv) {
+    Case& cs = ((OracleHandle*)hp)->cs;
+    const Mesh& m = cs.mesh;
+    for (int k = 0; k < m.n[2]; ++k)
+        for (int j = 0; j < m.n[1]; ++j)
+            for (int i = 0; i < m.n[0]; ++i) {
+                const ConsVar& c = cs.u[m.idx(i, j, k)];
+                double* e = base + i * si + j * sj + k * sk;
+                e[0] = c.rho; e[sv] = c.rho_u; e[2 * sv] = c.rho_v; e[3 * sv] = c.rho_w; e[4 * sv] = c.rho_e;
+            }
+    return EFVM_OK;
+}
+
 // Full raw array (all layers, 5 doubles per cell, FIELD raw order).
 int64_t oracle_raw_size(void* hp) { return (int64_t)((OracleHandle*)hp)->cs.mesh.n_raw(); }
 int oracle_get_raw_state(void* hp, double* out) {

@@ -43,6 +43,8 @@ def lib(parallel: bool = False) -> C.CDLL:
     L.oracle_set_option.argtypes = [vp, C.c_char_p, C.c_double]
     for fn in ("oracle_upload_state", "oracle_download_state"):
         getattr(L, fn).argtypes = [vp, dp, i64, i64, i64]
+    for fn in ("oracle_upload_state3", "oracle_download_state3"):
+        getattr(L, fn).argtypes = [vp, dp, i64, i64, i64, i64]
     L.oracle_raw_size.restype = i64
     L.oracle_raw_size.argtypes = [vp]
     L.oracle_get_raw_state.argtypes = [vp, dp]
@@ -104,7 +106,7 @@ class OracleCase:
         self.h = self.L.oracle_create(C.byref(grid), C.byref(params))
         if not self.h:
             raise ValueError(self.L.oracle_create_error().decode())
-        self.nx, self.ny = grid.nx, grid.ny
+        self.nx, self.ny, self.nz = grid.nx, grid.ny, grid.nz
 
     def close(self):
         if self.h:
@@ -120,13 +122,22 @@ class OracleCase:
     def set_option(self, name: str, value: float) -> None:
         assert self.L.oracle_set_option(self.h, name.encode(), float(value)) == 0
 
-    # state as an (ny, nx, 5) array: rho, rho_u, rho_v, rho_w, rho_e
+    # state as an (ny, nx, 5) array (2-D) or an (nz, ny, nx, 5) array (3-D):
+    # rho, rho_u, rho_v, rho_w, rho_e
     def upload(self, u: np.ndarray) -> None:
         u = arr(u)
+        if self.nz > 1:
+            assert u.shape == (self.nz, self.ny, self.nx, 5)
+            self.L.oracle_upload_state3(self.h, _dp(u), 5, 5 * self.nx, 5 * self.nx * self.ny, 1)
+            return
         assert u.shape == (self.ny, self.nx, 5)
         self.L.oracle_upload_state(self.h, _dp(u), 5, 5 * self.nx, 1)
 
     def download(self) -> np.ndarray:
+        if self.nz > 1:
+            out = np.zeros((self.nz, self.ny, self.nx, 5))
+            self.L.oracle_download_state3(self.h, _dp(out), 5, 5 * self.nx, 5 * self.nx * self.ny, 1)
+            return out
         out = np.zeros((self.ny, self.nx, 5))
         self.L.oracle_download_state(self.h, _dp(out), 5, 5 * self.nx, 1)
         return out

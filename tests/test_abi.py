@@ -65,6 +65,13 @@ def test_create_without_a_gpu_fails_loudly_or_rejects_bad_config(lib):
     rc = lib.efvm_create(C.byref(g), C.byref(abi.make_params()), C.byref(h))
     assert rc == abi.ERR_INVALID_ARG
     assert b"periodic" in lib.efvm_last_error(None)
-    # 3-D meshes are outside the 2-D device layout.
+    # 3-D meshes run in FP64 without the 2-D case systems: those options are
+    # rejected before any device work.
     g3 = abi.make_grid(8, 8, nz=4)
-    assert lib.efvm_create(C.byref(g3), C.byref(abi.make_params()), C.byref(h)) == abi.ERR_UNSUPPORTED
+    p32 = abi.make_params(precision=abi.PREC_FP32_FLUX)
+    assert lib.efvm_create(C.byref(g3), C.byref(p32), C.byref(h)) == abi.ERR_UNSUPPORTED
+    assert b"FP64" in lib.efvm_last_error(None)
+    ps = abi.make_params(sponge=1, sponge_x_start=0.5, sponge_x_end=1.0)
+    assert lib.efvm_create(C.byref(g3), C.byref(ps), C.byref(h)) == abi.ERR_UNSUPPORTED
+    g0 = abi.make_grid(8, 8, nz=0)
+    assert lib.efvm_create(C.byref(g0), C.byref(abi.make_params()), C.byref(h)) == abi.ERR_INVALID_ARG
