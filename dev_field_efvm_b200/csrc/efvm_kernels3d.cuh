@@ -179,7 +179,10 @@ constexpr int MINB3 = 4;  // resident blocks per SM of the 3-D stage kernel (128
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// The 3-D stage kernel: one RK substage of layer blockIdx.z.
+// The 3-D stage kernel: one RK substage.  Warp w of block b works on the pair
+// (strip, layer) = ((b WPB + w) mod strips, (b WPB + w) div strips), so every
+// warp slot has work whatever the number of strips per layer; blockIdx.y is
+// the row block.
 // ---------------------------------------------------------------------------
 template <int SCHEME, int RECON, bool VISC>
 __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, int rows) {
@@ -189,8 +192,10 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
     const Physics& ph = a.ph;
     const long long P = g.plane;
     const int lane = threadIdx.x & 31;
-    const int strip = blockIdx.x * WPB + (threadIdx.x >> 5);
-    const int by = blockIdx.y, k = blockIdx.z;
+    const int strips = (g.nx + STRIP - 1) / STRIP;
+    const int wid = blockIdx.x * WPB + (threadIdx.x >> 5);
+    const int k = wid / strips, strip = wid - k * strips;
+    const int by = blockIdx.y;
     if (strip == 0 && by == 0 && k == 0 && lane == 0) {
         // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
         DevState* st = a.st;
@@ -207,7 +212,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
     const int i0 = strip * STRIP;
     const int jb = by * rows;
     double lam = 0.0;
-    if (i0 < g.nx && jb < g.ny) {  // uniform across the warp
+    if (k < g.nz && jb < g.ny) {  // uniform across the warp
         constexpr bool MUSCL = RECON == EFVM_RECON_MUSCL;
         const int je = min(jb + rows, g.ny);
         const int i = i0 + lane;
@@ -252,45 +257,17 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
         }
         V5 gb;  // flux of the y face below row j, grid frame
         for (int j = jb - 1; j < je; ++j) {
-            const V5 un2 = ldrow(j + 2);
             const bool row = j >= jb;  // warp-uniform: the first pass only forms the face below row jb
 
-            // Flux divergence in the reference's accumulation order for an interior
-            // cell: the z face below, the y face below, the x face on the left (all
-            // scattered when their owners were visited), then the cell's own +x, +y
-            // and +z faces (for_each_face order, crates/cfd_solver/src/lib.rs:333-337).
-            double part[5];
-            V5 fzt;
+            // Flux divergence, accumulated as each face is formed: the y face below
+            // (carried), the x faces left and right, the z faces below and above,
+            // then the y face above.  The reference sums an interior cell's faces in
+            // for_each_face order (z below, y below, x left, +x, +y, +z;
+            // crates/cfd_solver/src/lib.rs:333-337); the order here keeps at most
+            // one face flux live at a time and differs from it only in rounding.
+            double acc[5];
             if (row) {
-                // ---- the two z faces of the cell, one code path ----
-                const V5 zm1 = ldz(j, -1), zp1 = ldz(j, 1);
-                V5 zm2 = zm1, zp2 = zp1;
-                if (MUSCL) {
-                    zm2 = ldz(j, -2);
-                    zp2 = ldz(j, 2);
-                }
-                V5 fzb;
-#pragma unroll 1
-                for (int s = 0; s < 2; ++s) {
-                    const V5 A_lo = s ? zm1 : zm2, A = s ? uc : zm1, B = s ? zp1 : uc, B_hi = s ? zp2 : zp1;
-                    V5 L = A, Rv = B;
-                    if (MUSCL) {
-                        V5 pl, mi;
-                        if (s ? zrA[1] : zrA[0]) {
-                            slope_faces5(ph.limiter, A_lo, A, B, pl, mi);
-                            L = pl;
-                        }
-                        if (s ? zrB[1] : zrB[0]) {
-                            slope_faces5(ph.limiter, A, B, B_hi, pl, mi);
-                            Rv = mi;
-                        }
-                    }
-                    const V5 f = zg5(face_flux5<SCHEME, double>(zq5(L), zq5(Rv), rg, gm1));
-                    if (s) fzt = f;
-                    else fzb = f;
-                }
-
-                // ---- x face on the left of column i ----
+                // ---- x faces on the left and right of column i ----
                 V5 ul = shfl_up5(uc, 1), ur = shfl_down5(uc, 1);
                 V5 ull = ul;
                 if (lane == 0) {
@@ -312,20 +289,44 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                 }
                 const V5 fx = xg5(face_flux5<SCHEME, double>(xl, xr, rg, gm1));
                 const V5 fxr = shfl_down5(fx, 1);
-                const double zb[5] = {fzb.r, fzb.mx, fzb.my, fzb.mz, fzb.E};
                 const double yb[5] = {gb.r, gb.mx, gb.my, gb.mz, gb.E};
                 const double fl[5] = {fx.r, fx.mx, fx.my, fx.mz, fx.E};
                 const double fr[5] = {fxr.r, fxr.mx, fxr.my, fxr.mz, fxr.E};
 #pragma unroll
                 for (int v = 0; v < 5; ++v) {
-                    double acc = __dmul_rn(zb[v], g.inv_z);
-                    acc = __dadd_rn(acc, __dmul_rn(yb[v], g.inv_y));
-                    acc = __dadd_rn(acc, __dmul_rn(fl[v], g.inv_x));
-                    part[v] = __dsub_rn(acc, __dmul_rn(fr[v], g.inv_x));
+                    double t = __dmul_rn(yb[v], g.inv_y);
+                    t = __dadd_rn(t, __dmul_rn(fl[v], g.inv_x));
+                    acc[v] = __dsub_rn(t, __dmul_rn(fr[v], g.inv_x));
+                }
+
+                // ---- the two z faces of the cell through one code path: face s
+                // lies between layers k - 1 + s and k + s; its four cells are
+                // loaded here, so no z stencil stays live across the loop ----
+#pragma unroll 1
+                for (int s = 0; s < 2; ++s) {
+                    const V5 A = ldz(j, s - 1), B = ldz(j, s);
+                    V5 L = A, Rv = B;
+                    if (MUSCL) {
+                        V5 pl, mi;
+                        if (s ? zrA[1] : zrA[0]) {
+                            slope_faces5(ph.limiter, ldz(j, s - 2), A, B, pl, mi);
+                            L = pl;
+                        }
+                        if (s ? zrB[1] : zrB[0]) {
+                            slope_faces5(ph.limiter, A, B, ldz(j, s + 1), pl, mi);
+                            Rv = mi;
+                        }
+                    }
+                    const V5 f = zg5(face_flux5<SCHEME, double>(zq5(L), zq5(Rv), rg, gm1));
+                    const double fv[5] = {f.r, f.mx, f.my, f.mz, f.E};
+                    const double w = s ? -g.inv_z : g.inv_z;  // in through the face below, out through the one above
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) acc[v] = __dadd_rn(acc[v], __dmul_rn(fv[v], w));
                 }
             }
 
             // ---- y face above row j ----
+            const V5 un2 = ldrow(j + 2);
             V5 pn = un;
             Q5<double> yb_, yt_;
             if (MUSCL) {
@@ -346,49 +347,61 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                 const long long o = cidx3(g, i, j, k);
                 const U5 ucd = toU5(uc);
                 const double yt[5] = {gt.r, gt.mx, gt.my, gt.mz, gt.E};
-                const double zt[5] = {fzt.r, fzt.mx, fzt.my, fzt.mz, fzt.E};
                 double rhs[5];
 #pragma unroll
-                for (int v = 0; v < 5; ++v)
-                    rhs[v] = __dsub_rn(__dsub_rn(part[v], __dmul_rn(yt[v], g.inv_y)), __dmul_rn(zt[v], g.inv_z));
+                for (int v = 0; v < 5; ++v) rhs[v] = __dsub_rn(acc[v], __dmul_rn(yt[v], g.inv_y));
                 if (VISC) {
-                    // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (7-point stencil)
-                    const U5 nbs[6] = {ld(i + 1, j, k), ld(i - 1, j, k), toU5(un), ld(i, j - 1, k),
-                                       ld(i, j, k + 1), ld(i, j, k - 1)};
-                    // the seven reciprocal densities from one reciprocal of their product
+                    // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (7-point stencil),
+                    // one axis pair of neighbours at a time.  The seven reciprocal
+                    // densities come from one reciprocal of their product.
+                    const long long nbo[6] = {cidx3(g, i + 1, j, k), cidx3(g, i - 1, j, k), cidx3(g, i, j + 1, k),
+                                              cidx3(g, i, j - 1, k), cidx3(g, i, j, k + 1), cidx3(g, i, j, k - 1)};
                     double pr[7];
                     pr[0] = ucd.r;
 #pragma unroll
-                    for (int n = 0; n < 6; ++n) pr[n + 1] = pr[n] * nbs[n].r;
+                    for (int n = 0; n < 6; ++n) pr[n + 1] = pr[n] * uin[nbo[n]];
                     double w = rcp_(pr[6]);
                     double inv[7];
 #pragma unroll
                     for (int n = 6; n >= 1; --n) {
                         inv[n] = pr[n - 1] * w;
-                        w = w * nbs[n - 1].r;  // now 1 / pr[n - 1]
+                        w = w * uin[nbo[n - 1]];  // now 1 / pr[n - 1]
                     }
                     inv[0] = w;
                     double us, vs, ws, ts;
                     prim5(ucd, inv[0], gm1, ph.r_gas, us, vs, ws, ts);
-                    double nu[6], nv[6], nw[6], nt[6];  // +x, -x, +y, -y, +z, -z
-#pragma unroll
-                    for (int n = 0; n < 6; ++n) prim5(nbs[n], inv[n + 1], gm1, ph.r_gas, nu[n], nv[n], nw[n], nt[n]);
-                    const double y_im = a.yw[j], y_ip = a.yw[g.ny + j], y_is = a.yw[2 * g.ny + j];
-                    const double z_im = a.zw[k], z_ip = a.zw[g.nz + k], z_is = a.zw[2 * g.nz + k];
-                    const double dxi2 = ph.dx_inv2;
-                    auto d2x = [&](double m, double p, double c) { return (p - 2.0 * c + m) * dxi2; };
-                    auto d2y = [&](double m, double p, double c) { return ((p - c) * y_ip - (c - m) * y_im) * y_is; };
-                    auto d2z = [&](double m, double p, double c) { return ((p - c) * z_ip - (c - m) * z_im) * z_is; };
                     const double mu = viscosity(ph, ts);
                     const double kappa = mu * ph.cp / 0.72;  // thermal_conductivity, crates/cfd_eos/src/lib.rs:83-87
-                    const double fxv = mu * (d2x(nu[1], nu[0], us) + d2y(nu[3], nu[2], us) + d2z(nu[5], nu[4], us));
-                    const double fyv = mu * (d2x(nv[1], nv[0], vs) + d2y(nv[3], nv[2], vs) + d2z(nv[5], nv[4], vs));
-                    const double fzv = mu * (d2x(nw[1], nw[0], ws) + d2y(nw[3], nw[2], ws) + d2z(nw[5], nw[4], ws));
-                    const double d2t = d2x(nt[1], nt[0], ts) + d2y(nt[3], nt[2], ts) + d2z(nt[5], nt[4], ts);
+                    double lu = 0.0, lv = 0.0, lw = 0.0, lt = 0.0;  // d2x + d2y + d2z of u, v, w, T
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) {
+                        double pu, pv, pw, pt, mu_, mv, mw, mt;
+                        prim5(load5(uin, P, nbo[2 * ax]), inv[2 * ax + 1], gm1, ph.r_gas, pu, pv, pw, pt);
+                        prim5(load5(uin, P, nbo[2 * ax + 1]), inv[2 * ax + 2], gm1, ph.r_gas, mu_, mv, mw, mt);
+                        double im = 0.0, ip = 0.0, is = 0.0;
+                        if (ax == 1) {
+                            im = a.yw[j];
+                            ip = a.yw[g.ny + j];
+                            is = a.yw[2 * g.ny + j];
+                        } else if (ax == 2) {
+                            im = a.zw[k];
+                            ip = a.zw[g.nz + k];
+                            is = a.zw[2 * g.nz + k];
+                        }
+                        auto d2 = [&](double m, double p, double c) {
+                            return ax == 0 ? (p - 2.0 * c + m) * ph.dx_inv2 : ((p - c) * ip - (c - m) * im) * is;
+                        };
+                        const double du = d2(mu_, pu, us), dv = d2(mv, pv, vs), dw = d2(mw, pw, ws), dt_ = d2(mt, pt, ts);
+                        lu = ax == 0 ? du : lu + du;
+                        lv = ax == 0 ? dv : lv + dv;
+                        lw = ax == 0 ? dw : lw + dw;
+                        lt = ax == 0 ? dt_ : lt + dt_;
+                    }
+                    const double fxv = mu * lu, fyv = mu * lv, fzv = mu * lw;
                     rhs[1] += fxv;
                     rhs[2] += fyv;
                     rhs[3] += fzv;
-                    rhs[4] += us * fxv + vs * fyv + ws * fzv + kappa * d2t;
+                    rhs[4] += us * fxv + vs * fyv + ws * fzv + kappa * lt;
                 }
                 if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
                     rhs[1] += ucd.r * ph.body_force_x;
@@ -496,21 +509,23 @@ __global__ void total_mass3_kernel(Geometry g, const double* __restrict__ q, dou
 
 // ---- launches ---------------------------------------------------------------
 // Rows per warp of the 3-D stage: the fewest that fill the resident slots in one
-// wave, clamped to [2, 8] as in 2-D.
+// wave, clamped to [2, 12].  A sweep at 256^3 over 4-16 rows and 3-5 resident
+// blocks per SM measured 12 rows and 4 blocks fastest (6.53 ms per inviscid step
+// against 6.65 at 8 rows; 3 and 5 blocks 15 % and 10 % slower).
 static int rows_per_warp3(int nx, int ny, int nz) {
     const long long strips = (nx + STRIP - 1) / STRIP;
     const long long slots = 148LL * MINB3 * WPB;
     long long rows = (strips * ny * nz + slots - 1) / slots;
     if (rows < 2) rows = 2;
-    if (rows > 8) rows = 8;
+    if (rows > 12) rows = 12;
     return (int)rows;
 }
 
 template <int SCHEME, int RECON, bool VISC>
 static void launch_stage3_t(const StageArgs& a, bool pdl, cudaStream_t s) {
     const int rows = rows_per_warp3(a.g.nx, a.g.ny, a.g.nz);
-    const int strips = (a.g.nx + STRIP - 1) / STRIP;
-    dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows, a.g.nz);
+    const long long pairs = (long long)((a.g.nx + STRIP - 1) / STRIP) * a.g.nz;
+    dim3 grid((unsigned)((pairs + WPB - 1) / WPB), (a.g.ny + rows - 1) / rows);
     launch_k(stage3_kernel<SCHEME, RECON, VISC>, grid, dim3(32 * WPB), s, pdl, a, rows);
 }
 
