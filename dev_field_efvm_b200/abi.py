@@ -126,6 +126,15 @@ class EfvmCylinder(C.Structure):
     _fields_ = [("cx", C.c_double), ("cy", C.c_double), ("radius", C.c_double)]
 
 
+class EfvmSphere(C.Structure):
+    """centre, radius, translational velocity, angular velocity (efvm_sphere)."""
+    _fields_ = [(n, C.c_double) for n in ("cx", "cy", "cz", "radius", "vx", "vy", "vz", "wx", "wy", "wz")]
+
+
+def make_sphere(centre, radius, velocity=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0)) -> EfvmSphere:
+    return EfvmSphere(*(float(x) for x in (*centre, radius, *velocity, *omega)))
+
+
 class EfvmVortex(C.Structure):
     _fields_ = [
         ("gamma", C.c_double),

@@ -49,6 +49,11 @@ struct efvm_ctx {
     bool ibm = false;
     bool geom_dirty = false;
     std::vector<double> cyl_host;  // cx, cy, r per body
+    std::vector<double> sph_host;  // 3-D spheres: efvm_sphere's 10 doubles per body
+    double* sph_dev = nullptr;
+    int sphere_markers = 2000;     // Fibonacci markers per sphere
+    IbmGhost3Dev* ghosts3_dev = nullptr;
+    Marker3Dev* markers3_dev = nullptr;
     double stagnant[5] = {0, 0, 0, 0, 0};  // MaskConsts.stagnant
     // learned face-flux correction (efvm_set_flux_correction)
     efvm_nn* nn = nullptr;
@@ -268,6 +273,158 @@ int build_ibm_lists(efvm_ctx* c) {
     return EFVM_OK;
 }
 
+// The 3-D lists after the mask changed (compute_sphere_ghosts and
+// compute_sphere_markers, crates/cfd_ibm/src/sphere.rs:116-245), built on the host
+// from the device mask with the reference's arithmetic, then uploaded.  The mask
+// of a ghost layer is the interior's image on a periodic axis (the reference's
+// halo copies it with the state) and fluid elsewhere.
+int build_ibm_lists3(efvm_ctx* c) {
+    const Geometry& g = c->g;
+    std::vector<uint8_t> m((size_t)g.plane);
+    CUDA_TRY(c, cudaMemcpyAsync(m.data(), c->mask, (size_t)g.plane, cudaMemcpyDeviceToHost, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const bool per[3] = {c->ph.periodic_x != 0, c->ph.periodic_y != 0, c->ph.periodic_z != 0};
+    auto at = [&](int i, int j, int k) {
+        return (size_t)(2 + k) * (size_t)g.layer + (size_t)(YO + j) * g.pitch + (size_t)(XO + i);
+    };
+    // solid at interior coordinates, ghost layers included (-2 .. n+1)
+    auto solid = [&](int i, int j, int k) {
+        int q[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a) {
+            if (q[a] >= 0 && q[a] < n[a]) continue;
+            if (!per[a]) return false;
+            q[a] = q[a] < 0 ? q[a] + n[a] : q[a] - n[a];
+        }
+        return m[at(q[0], q[1], q[2])] != 0;
+    };
+    // FIELD locate(): low corner floor(f) of the 2x2x2 block of cell centres
+    // around p, f = (p - lo)/h - 0.5; valid when the block stays inside the raw array
+    auto locate3 = [&](const double p[3], int lo[3], double t[3]) {
+        bool ok = true;
+        for (int a = 0; a < 3; ++a) {
+            const double f = (p[a] - g.lo[a]) / g.h[a] - 0.5;
+            const double fl = std::floor(f);
+            lo[a] = (int)fl;
+            t[a] = f - fl;
+            ok = ok && lo[a] + NG >= 0 && lo[a] + NG + 1 < n[a] + 2 * NG;
+        }
+        return ok;
+    };
+    auto corner_bits = [&](const int lo[3]) {
+        unsigned b = 0;
+        for (int di = 0; di < 2; ++di)
+            for (int dj = 0; dj < 2; ++dj)
+                for (int dk = 0; dk < 2; ++dk)
+                    if (!solid(lo[0] + di, lo[1] + dj, lo[2] + dk))
+                        b |= 1u << (FLUID3_CORNER_SHIFT + 4 * di + 2 * dj + dk);
+        return b;
+    };
+    const int nb = (int)(c->sph_host.size() / 10);
+    auto sd_of = [&](int b, const double p[3], double nrm[3]) {
+        const double* s = &c->sph_host[10 * b];
+        const double d0 = p[0] - s[0], d1 = p[1] - s[1], d2 = p[2] - s[2];
+        const double rr = std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        if (rr < 1e-12) { nrm[0] = 1.0; nrm[1] = 0.0; nrm[2] = 0.0; }
+        else { nrm[0] = d0 / rr; nrm[1] = d1 / rr; nrm[2] = d2 / rr; }
+        return rr - s[3];
+    };
+    auto wall_velocity = [&](int b, const double p[3], double out[3]) {
+        const double* s = &c->sph_host[10 * b];
+        const double r0 = p[0] - s[0], r1 = p[1] - s[1], r2 = p[2] - s[2];
+        out[0] = s[4] + s[8] * r2 - s[9] * r1;
+        out[1] = s[5] + s[9] * r0 - s[7] * r2;
+        out[2] = s[6] + s[7] * r1 - s[8] * r0;
+    };
+    std::vector<IbmGhost3Dev> ghosts;
+    c->n_solid = 0;
+    for (int k = 0; k < g.nz; ++k)
+        for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i) {
+                if (!m[at(i, j, k)]) continue;
+                ++c->n_solid;
+                const int nbd[6][3] = {{i + 1, j, k}, {i - 1, j, k}, {i, j + 1, k}, {i, j - 1, k}, {i, j, k + 1}, {i, j, k - 1}};
+                unsigned fl = 0;
+                for (int q = 0; q < 6; ++q)
+                    if (!solid(nbd[q][0], nbd[q][1], nbd[q][2])) fl |= 1u << q;
+                if (!fl) continue;  // fully buried
+                const double cc[3] = {centre_h(g.lo[0], g.h[0], i), centre_h(g.lo[1], g.h[1], j),
+                                      centre_h(g.lo[2], g.h[2], k)};
+                double best_abs = std::numeric_limits<double>::max(), best_signed = 0.0;
+                double best_n[3] = {1.0, 0.0, 0.0}, best_w[3] = {0.0, 0.0, 0.0};
+                for (int b = 0; b < nb; ++b) {
+                    double nrm[3];
+                    const double sd = sd_of(b, cc, nrm);
+                    if (std::fabs(sd) < best_abs) {
+                        best_abs = std::fabs(sd);
+                        best_signed = sd;
+                        for (int d = 0; d < 3; ++d) best_n[d] = nrm[d];
+                        const double foot[3] = {cc[0] - sd * best_n[0], cc[1] - sd * best_n[1], cc[2] - sd * best_n[2]};
+                        wall_velocity(b, foot, best_w);
+                    }
+                }
+                const double push = 2.0 * (-best_signed);
+                const double ip[3] = {cc[0] + push * best_n[0], cc[1] + push * best_n[1], cc[2] + push * best_n[2]};
+                IbmGhost3Dev gh{};
+                gh.i = i;
+                gh.j = j;
+                gh.k = k;
+                gh.fluid = fl;
+                gh.valid = locate3(ip, gh.lo, gh.t) ? 1 : 0;
+                if (gh.valid) gh.fluid |= corner_bits(gh.lo);
+                for (int d = 0; d < 3; ++d) gh.uw[d] = best_w[d];
+                ghosts.push_back(gh);
+            }
+    // sphere_markers: the golden-angle Fibonacci lattice, area 4 pi R^2 / n
+    std::vector<Marker3Dev> markers;
+    const double PI = 3.141592653589793;
+    const int nm = std::max(c->sphere_markers, 12);
+    const double golden = PI * (3.0 - std::sqrt(5.0));
+    const double offset = g.h[0];  // marker_force_system: sample offset = spacing(0, 0)
+    for (int b = 0; b < nb; ++b) {
+        const double* s = &c->sph_host[10 * b];
+        const double area = 4.0 * PI * s[3] * s[3] / (double)nm;
+        for (int q = 0; q < nm; ++q) {
+            const double zr = 1.0 - 2.0 * ((double)q + 0.5) / (double)nm;
+            const double rr = std::sqrt(std::max(1.0 - zr * zr, 0.0));
+            const double phi = golden * (double)q;
+            const double dir[3] = {rr * std::cos(phi), rr * std::sin(phi), zr};
+            const double pos[3] = {s[0] + s[3] * dir[0], s[1] + s[3] * dir[1], s[2] + s[3] * dir[2]};
+            Marker3Dev mk{};
+            for (int d = 0; d < 3; ++d) mk.normal[d] = dir[d];
+            mk.area = area;
+            wall_velocity(b, pos, mk.uw);
+            const double sp[3] = {pos[0] + offset * dir[0], pos[1] + offset * dir[1], pos[2] + offset * dir[2]};
+            mk.valid = locate3(sp, mk.lo, mk.t) ? 1 : 0;
+            if (mk.valid) mk.fluid = corner_bits(mk.lo);
+            mk.body = b;
+            markers.push_back(mk);
+        }
+    }
+    cudaFree(c->ghosts3_dev);
+    cudaFree(c->markers3_dev);
+    c->ghosts3_dev = nullptr;
+    c->markers3_dev = nullptr;
+    CUDA_TRY(c, cudaMalloc(&c->ghosts3_dev, std::max<size_t>(ghosts.size(), 1) * sizeof(IbmGhost3Dev)));
+    CUDA_TRY(c, cudaMalloc(&c->markers3_dev, std::max<size_t>(markers.size(), 1) * sizeof(Marker3Dev)));
+    if (!ghosts.empty())
+        CUDA_TRY(c, cudaMemcpyAsync(c->ghosts3_dev, ghosts.data(), ghosts.size() * sizeof(IbmGhost3Dev),
+                                    cudaMemcpyHostToDevice, S(c)));
+    if (!markers.empty())
+        CUDA_TRY(c, cudaMemcpyAsync(c->markers3_dev, markers.data(), markers.size() * sizeof(Marker3Dev),
+                                    cudaMemcpyHostToDevice, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    Ibm& d = c->ibm_desc;
+    d.enabled = 1;
+    d.n_ghost = (int)ghosts.size();
+    d.n_markers = (int)markers.size();
+    d.ghosts3 = c->ghosts3_dev;
+    d.markers3 = c->markers3_dev;
+    d.sample_offset = offset;
+    d.force_out = c->force_out;
+    return EFVM_OK;
+}
+
 // Setup-phase work that precedes a step boundary's first stage, in the
 // reference's Setup order: CFL (SolverPlugin) before the geometry refresh
 // (CylinderIbmPlugin), then Halo/Boundary for a state that changed on the host.
@@ -277,9 +434,16 @@ int prologue(efvm_ctx* c) {
         c->lam_stale = false;
     }
     if (c->ibm && c->geom_dirty) {
-        c->launches += launch_geometry(c->g, c->cyl_dev, (int)(c->cyl_host.size() / 3), c->stagnant, c->ambient,
-                                       cur_buf(c), c->mask, S(c));
-        int rc = build_ibm_lists(c);
+        int rc;
+        if (is_3d(c)) {
+            c->launches += launch_geometry3(c->g, c->ph, c->sph_dev, (int)(c->sph_host.size() / 10), c->stagnant,
+                                            c->ambient, cur_buf(c), c->mask, S(c));
+            rc = build_ibm_lists3(c);
+        } else {
+            c->launches += launch_geometry(c->g, c->cyl_dev, (int)(c->cyl_host.size() / 3), c->stagnant, c->ambient,
+                                           cur_buf(c), c->mask, S(c));
+            rc = build_ibm_lists(c);
+        }
         if (rc) return rc;
         c->geom_dirty = false;
         c->ghosts_stale = true;
@@ -316,6 +480,13 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
 // Launch the kernels of one substage at RK stage `stage` (0..2, or 3 = Euler):
 // [step set-up +] IBM mirror of uin, the stage, the IBM forces of uout.
 void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool with_setup) {
+    if (c->ibm && is_3d(c)) {  // spheres: [set-up], mirror, stage, forces, all on the main stream
+        if (with_setup) c->launches += launch_step_setup(c->ph, c->st, true, S(c));
+        c->launches += launch_mirror3(c->g, c->ph, c->ibm_desc, uin, true, S(c));
+        enqueue_stage_kernel(c, stage, uin, uout);
+        c->launches += launch_forces3(c->g, c->ph, c->ibm_desc, uout, c->st, true, S(c));
+        return;
+    }
     if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uin, c->st, -1, stage, with_setup, true, S(c));
     else if (with_setup) c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     enqueue_stage_kernel(c, stage, uin, uout);
@@ -332,6 +503,10 @@ void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool wi
 // the z-ghost state the last forces read.
 int enqueue_rk3_step(efvm_ctx* c) {
     double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
+    if (c->ibm && is_3d(c)) {
+        for (int s = 0; s < 3; ++s) enqueue_substage(c, s, bufs[s], bufs[s + 1], s == 0);
+        return EFVM_OK;
+    }
     if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->st, -1, 0, 1, true, S(c));
     else c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     for (int s = 0; s < 3; ++s) {
@@ -356,7 +531,7 @@ int capture_step_graph(efvm_ctx* c) {
         cudaGraphExecDestroy(c->graph_exec);
         c->graph_exec = nullptr;
     }
-    if (c->ibm && !c->side) {
+    if (c->ibm && !is_3d(c) && !c->side) {
         CUDA_TRY(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
         for (auto& ev : c->ev_fork) CUDA_TRY(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         CUDA_TRY(c, cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
@@ -640,6 +815,9 @@ int efvm_destroy(efvm_ctx* c) {
     cudaFree(c->partial);
     cudaFree(c->staging);
     cudaFree(c->cyl_dev);
+    cudaFree(c->sph_dev);
+    cudaFree(c->ghosts3_dev);
+    cudaFree(c->markers3_dev);
     cudaFree(c->ghosts_dev);
     cudaFree(c->markers_dev);
     cudaFree(c->zg0);
@@ -1120,6 +1298,44 @@ int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const d
     return EFVM_OK;
 }
 
+int efvm_set_spheres(efvm_ctx* c, const efvm_sphere* sph, int32_t n, int32_t n_markers, const double fs[5]) {
+    if (!c || n < 0 || n_markers < 0 || (n > 0 && (!sph || !fs)))
+        return fail(c, EFVM_ERR_INVALID_ARG, "invalid sphere arguments");
+    if (!is_3d(c))
+        return fail(c, EFVM_ERR_UNSUPPORTED,
+                    "spheres are 3-D bodies: efvm_set_spheres needs nz > 1 (efvm_set_cylinders is the 2-D form)");
+    if (n == 0) {
+        c->ibm = false;
+        c->graph_valid = false;
+        return EFVM_OK;
+    }
+    std::vector<double> h;
+    for (int b = 0; b < n; ++b) {
+        if (!(sph[b].radius > 0.0)) return fail(c, EFVM_ERR_INVALID_ARG, "sphere radius must be > 0");
+        const double v[10] = {sph[b].cx, sph[b].cy, sph[b].cz, sph[b].radius, sph[b].vx,
+                              sph[b].vy, sph[b].vz, sph[b].wx, sph[b].wy, sph[b].wz};
+        h.insert(h.end(), v, v + 10);
+    }
+    // MaskConsts of SphereIbmPlugin::build, crates/cfd_ibm/src/sphere.rs:277-279
+    const double ke = 0.5 * (fs[1] * fs[1] + fs[2] * fs[2] + fs[3] * fs[3]) / fs[0];
+    const double st5[5] = {fs[0], 0.0, 0.0, 0.0, fs[4] - ke};
+    std::memcpy(c->stagnant, st5, sizeof(st5));
+    std::memcpy(c->ambient, fs, 5 * sizeof(double));
+    if (c->sph_dev && c->sph_host.size() != h.size()) {
+        cudaFree(c->sph_dev);
+        c->sph_dev = nullptr;
+    }
+    if (!c->sph_dev) CUDA_TRY(c, cudaMalloc(&c->sph_dev, h.size() * sizeof(double)));
+    CUDA_TRY(c, cudaMemcpyAsync(c->sph_dev, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, S(c)));
+    CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+    c->sph_host = h;
+    c->sphere_markers = n_markers;
+    c->ibm = true;
+    c->geom_dirty = true;
+    c->graph_valid = false;
+    return EFVM_OK;
+}
+
 static int read_forces(efvm_ctx* c, double* out, int offset) {
     if (!c || !out) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     if (!c->ibm) {
@@ -1224,11 +1440,15 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
         CUDA_TRY(c, cudaEventRecord(ev[1], S(c)));
         float ms_stage = 0.f, ms_ibm = 0.f;
         for (int s = 0; s < 3; ++s) {
-            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s], c->st, -1, s, 0, false, S(c));
+            if (c->ibm)
+                c->launches += is_3d(c) ? launch_mirror3(c->g, c->ph, ib, bufs[s], false, S(c))
+                                        : launch_ibm(c->g, c->ph, ib, bufs[s], c->st, -1, s, 0, false, S(c));
             CUDA_TRY(c, cudaEventRecord(ev[2], S(c)));
             enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1], false);
             CUDA_TRY(c, cudaEventRecord(ev[3], S(c)));
-            if (c->ibm) c->launches += launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->st, s, -1, 0, false, S(c));
+            if (c->ibm)
+                c->launches += is_3d(c) ? launch_forces3(c->g, c->ph, ib, bufs[s + 1], c->st, false, S(c))
+                                        : launch_ibm(c->g, c->ph, ib, bufs[s + 1], c->st, s, -1, 0, false, S(c));
             CUDA_TRY(c, cudaEventRecord(ev[4], S(c)));
             CUDA_TRY(c, cudaEventSynchronize(ev[4]));
             float t_stage = 0.f, t_after = 0.f;

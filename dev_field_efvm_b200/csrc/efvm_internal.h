@@ -122,6 +122,29 @@ struct MarkerDev {
     int pad;
 };
 
+// 3-D immersed spheres: one solid cell of the ghost list, and one surface
+// marker, with their trilinear sample located when the lists are built.
+// fluid bits: 0..5 the +x, -x, +y, -y, +z, -z face neighbour; 8 + 4 di + 2 dj + dk
+// the trilinear corner (di, dj, dk).
+constexpr unsigned FLUID3_CORNER_SHIFT = 8;
+struct IbmGhost3Dev {
+    int i, j, k, valid;
+    int lo[3];
+    unsigned fluid;
+    double t[3];
+    double uw[3];           // wall velocity at the ghost's wall footprint
+};
+struct Marker3Dev {
+    double normal[3];
+    double area;
+    double uw[3];           // wall velocity at the marker
+    double t[3];
+    int lo[3];
+    int valid;
+    unsigned fluid;
+    int body;
+};
+
 struct Ibm {
     int enabled;
     int n_ghost;
@@ -139,6 +162,8 @@ struct Ibm {
     double* history;        // hist_cap x 6 (may be null)
     double* partials;       // 6 doubles per force block (deterministic reduction)
     unsigned int* counter;  // blocks finished in the current force launch
+    const IbmGhost3Dev* ghosts3;  // 3-D lists (spheres)
+    const Marker3Dev* markers3;
 };
 
 // Everything a stage kernel needs.
@@ -223,6 +248,15 @@ int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, 
                int force_stage, int mirror_stage, int setup, bool pdl, void* stream);
 int launch_pack(const Geometry& g, const double* host_like, int64_t si, int64_t sj, int64_t sv, double* q,
                  int to_device, void* stream);
+// 3-D spheres: the solid mask with the stagnant/ambient re-seed of flipped
+// cells (spheres: n x 10 doubles as efvm_sphere), the ghost mirror of q before
+// a stage, and the marker and staircase forces of q after one (one block,
+// fixed-order sums, the marker force appended to the history when it is set).
+int launch_geometry3(const Geometry& g, const Physics& ph, const double* spheres, int n, const double* stagnant,
+                     const double* ambient, double* q, uint8_t* mask, void* stream);
+int launch_mirror3(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, bool pdl, void* stream);
+int launch_forces3(const Geometry& g, const Physics& ph, const Ibm& ib, const double* q, DevState* st, bool pdl,
+                   void* stream);
 // The same for a 3-D state: element (i, j, k, v) at i si + j sj + k sk + v sv.
 int launch_pack3(const Geometry& g, double* host_like, int64_t si, int64_t sj, int64_t sk, int64_t sv, double* q,
                  int to_device, void* stream);

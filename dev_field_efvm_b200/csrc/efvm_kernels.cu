@@ -1447,4 +1447,25 @@ int launch_pack3(const Geometry& g, double* host_like, int64_t si, int64_t sj, i
     return 1;
 }
 
+int launch_geometry3(const Geometry& g, const Physics& ph, const double* spheres, int n, const double* stagnant,
+                     const double* ambient, double* q, uint8_t* mask, void* stream) {
+    const U5 sg{stagnant[0], stagnant[1], stagnant[2], stagnant[3], stagnant[4]};
+    const U5 am{ambient[0], ambient[1], ambient[2], ambient[3], ambient[4]};
+    geometry3_kernel<<<grid_for((long long)g.nx * g.ny * g.nz, 256), 256, 0, (cudaStream_t)stream>>>(
+        g, ph, spheres, n, sg, am, q, mask);
+    return 1;
+}
+
+int launch_mirror3(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, bool pdl, void* stream) {
+    const int nb = ib.n_ghost > 0 ? (ib.n_ghost + 127) / 128 : 1;
+    launch_k(mirror3_kernel, dim3(nb), dim3(128), (cudaStream_t)stream, pdl, g, ph, ib, q);
+    return 1;
+}
+
+int launch_forces3(const Geometry& g, const Physics& ph, const Ibm& ib, const double* q, DevState* st, bool pdl,
+                   void* stream) {
+    launch_k(forces3_kernel, dim3(1), dim3(FORCE3_THREADS), (cudaStream_t)stream, pdl, g, ph, ib, q, st);
+    return 1;
+}
+
 }  // namespace efvm

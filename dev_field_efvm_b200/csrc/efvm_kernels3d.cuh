@@ -350,22 +350,32 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                 double rhs[5];
 #pragma unroll
                 for (int v = 0; v < 5; ++v) rhs[v] = __dsub_rn(acc[v], __dmul_rn(yt[v], g.inv_y));
-                if (VISC) {
+                const bool ibm = a.mask != nullptr;
+                const bool solid = ibm && a.mask[o];
+                if (VISC && !solid) {
                     // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (7-point stencil),
-                    // one axis pair of neighbours at a time.  The seven reciprocal
-                    // densities come from one reciprocal of their product.
+                    // one axis pair of neighbours at a time; a solid neighbour enters as
+                    // (0, 0, 0, T of the cell).  The seven reciprocal densities come from
+                    // one reciprocal of their product.
                     const long long nbo[6] = {cidx3(g, i + 1, j, k), cidx3(g, i - 1, j, k), cidx3(g, i, j + 1, k),
                                               cidx3(g, i, j - 1, k), cidx3(g, i, j, k + 1), cidx3(g, i, j, k - 1)};
+                    bool sn[6];
+                    double rn[6];
+#pragma unroll
+                    for (int n = 0; n < 6; ++n) {
+                        sn[n] = ibm && a.mask[nbo[n]];
+                        rn[n] = sn[n] ? 1.0 : uin[nbo[n]];
+                    }
                     double pr[7];
                     pr[0] = ucd.r;
 #pragma unroll
-                    for (int n = 0; n < 6; ++n) pr[n + 1] = pr[n] * uin[nbo[n]];
+                    for (int n = 0; n < 6; ++n) pr[n + 1] = pr[n] * rn[n];
                     double w = rcp_(pr[6]);
                     double inv[7];
 #pragma unroll
                     for (int n = 6; n >= 1; --n) {
                         inv[n] = pr[n - 1] * w;
-                        w = w * uin[nbo[n - 1]];  // now 1 / pr[n - 1]
+                        w = w * rn[n - 1];  // now 1 / pr[n - 1]
                     }
                     inv[0] = w;
                     double us, vs, ws, ts;
@@ -375,9 +385,11 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                     double lu = 0.0, lv = 0.0, lw = 0.0, lt = 0.0;  // d2x + d2y + d2z of u, v, w, T
 #pragma unroll
                     for (int ax = 0; ax < 3; ++ax) {
-                        double pu, pv, pw, pt, mu_, mv, mw, mt;
-                        prim5(load5(uin, P, nbo[2 * ax]), inv[2 * ax + 1], gm1, ph.r_gas, pu, pv, pw, pt);
-                        prim5(load5(uin, P, nbo[2 * ax + 1]), inv[2 * ax + 2], gm1, ph.r_gas, mu_, mv, mw, mt);
+                        double pu = 0.0, pv = 0.0, pw = 0.0, pt = ts, mu_ = 0.0, mv = 0.0, mw = 0.0, mt = ts;
+                        if (!sn[2 * ax])
+                            prim5(load5(uin, P, nbo[2 * ax]), inv[2 * ax + 1], gm1, ph.r_gas, pu, pv, pw, pt);
+                        if (!sn[2 * ax + 1])
+                            prim5(load5(uin, P, nbo[2 * ax + 1]), inv[2 * ax + 2], gm1, ph.r_gas, mu_, mv, mw, mt);
                         double im = 0.0, ip = 0.0, is = 0.0;
                         if (ax == 1) {
                             im = a.yw[j];
@@ -403,6 +415,9 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                     rhs[3] += fzv;
                     rhs[4] += us * fxv + vs * fyv + ws * fzv + kappa * lt;
                 }
+                if (solid)  // zero_solid_rhs, crates/cfd_ibm/src/lib.rs:293-301
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) rhs[v] = 0.0;
                 if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
                     rhs[1] += ucd.r * ph.body_force_x;
                     rhs[4] += ph.body_force_x * ucd.mx;
@@ -505,6 +520,179 @@ __global__ void total_mass3_kernel(Geometry g, const double* __restrict__ q, dou
         __syncthreads();
     }
     if (threadIdx.x == 0) partial[blockIdx.x] = s1[0];
+}
+
+// ---- immersed spheres (3-D) -------------------------------------------------
+// refresh_sphere_mask, crates/cfd_ibm/src/sphere.rs:81-111: a cell whose centre
+// is inside any sphere is solid; a cell that flips is seeded with the stagnant
+// (fluid -> solid) or ambient (solid -> fluid) state.  The mask's ghost layers on
+// a periodic axis hold the images of the interior (the reference's halo copies
+// the mask with the state).  Every operation is rounded explicitly, as on the
+// host, so the mask and the host-built lists agree.
+__global__ void geometry3_kernel(Geometry g, Physics ph, const double* __restrict__ sph, int nb, U5 stagnant,
+                                 U5 ambient, double* q, uint8_t* mask) {
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ((long long)g.nx * g.ny));
+        const long long r = t - (long long)k * g.nx * g.ny;
+        const int j = (int)(r / g.nx), i = (int)(r - (long long)j * g.nx);
+        const double cc[3] = {centre(g.lo[0], g.h[0], i), centre(g.lo[1], g.h[1], j), centre(g.lo[2], g.h[2], k)};
+        bool inside = false;
+        for (int b = 0; b < nb && !inside; ++b) {
+            const double* s = sph + 10 * b;
+            const double d0 = __dsub_rn(cc[0], s[0]), d1 = __dsub_rn(cc[1], s[1]), d2 = __dsub_rn(cc[2], s[2]);
+            const double rr = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
+            inside = __dsub_rn(rr, s[3]) < 0.0;
+        }
+        const long long o = cidx3(g, i, j, k);
+        const bool was = mask[o] != 0;
+        if (inside && !was) store5(q, g.plane, o, stagnant);
+        else if (!inside && was) store5(q, g.plane, o, ambient);
+        const uint8_t m = inside ? 1 : 0;
+        mask[o] = m;
+        if (ph.periodic_x) {
+            if (i >= g.nx - NG) mask[cidx3(g, i - g.nx, j, k)] = m;
+            if (i < NG) mask[cidx3(g, i + g.nx, j, k)] = m;
+        }
+        if (ph.periodic_y) {
+            if (j >= g.ny - NG) mask[cidx3(g, i, j - g.ny, k)] = m;
+            if (j < NG) mask[cidx3(g, i, j + g.ny, k)] = m;
+        }
+        if (ph.periodic_z) {
+            if (k >= g.nz - NG) mask[cidx3(g, i, j, k - g.nz)] = m;
+            if (k < NG) mask[cidx3(g, i, j, k + g.nz)] = m;
+        }
+    }
+}
+
+// sample_trilinear, crates/cfd_ibm/src/lib.rs:106-149: primitive (rho, u, v, w,
+// p, T) at a located point from the fluid corners of its 2x2x2 block (clear
+// corner bits are solid), skipping non-positive or non-finite densities, the
+// weights renormalised; false when they sum below 1e-12.
+__device__ __forceinline__ bool sample_trilinear3(const Geometry& g, const Physics& ph, const double* q,
+                                                  unsigned fluid, const int lo[3], const double t[3], double out[6]) {
+    const double gm1 = ph.gamma - 1.0;
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double total = 0.0;
+#pragma unroll
+    for (int di = 0; di < 2; ++di) {
+        const double wx = di == 0 ? 1.0 - t[0] : t[0];
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj) {
+            const double wy = dj == 0 ? 1.0 - t[1] : t[1];
+#pragma unroll
+            for (int dk = 0; dk < 2; ++dk) {
+                const double wz = dk == 0 ? 1.0 - t[2] : t[2];
+                if (!(fluid & (1u << (FLUID3_CORNER_SHIFT + 4 * di + 2 * dj + dk)))) continue;
+                const U5 u = load5(q, g.plane, cidx3(g, lo[0] + di, lo[1] + dj, lo[2] + dk));
+                if (!isfinite(u.r) || u.r <= 0.0) continue;
+                const double w = wx * wy * wz;
+                const double inv = 1.0 / u.r;
+                const double vu = u.mx * inv, vv = u.my * inv, vw = u.mz * inv;
+                const double ke = 0.5 * u.r * (vu * vu + vv * vv + vw * vw);
+                const double p = gm1 * (u.E - ke);
+                const double tt = p * inv / ph.r_gas;
+                acc[0] += w * u.r;
+                acc[1] += w * vu;
+                acc[2] += w * vv;
+                acc[3] += w * vw;
+                acc[4] += w * p;
+                acc[5] += w * tt;
+                total += w;
+            }
+        }
+    }
+    if (total < 1e-12) return false;
+    const double inv = 1.0 / total;
+#pragma unroll
+    for (int v = 0; v < 6; ++v) out[v] = acc[v] * inv;
+    return true;
+}
+
+// apply_ibm_ghost_bc, crates/cfd_ibm/src/lib.rs:258-289: every ghost takes its
+// image point's density, pressure and temperature and the velocity mirrored
+// about the wall velocity, 2 u_w - u_image; a ghost whose sample fails keeps its
+// value.
+__global__ void mirror3_kernel(Geometry g, Physics ph, Ibm ib, double* q) {
+    pdl_wait_then_release();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ib.n_ghost) return;
+    const IbmGhost3Dev gh = ib.ghosts3[t];
+    if (!gh.valid) return;
+    double im[6];
+    if (!sample_trilinear3(g, ph, q, gh.fluid, gh.lo, gh.t, im)) return;
+    const double u = 2.0 * gh.uw[0] - im[1], v = 2.0 * gh.uw[1] - im[2], w = 2.0 * gh.uw[2] - im[3];
+    const double ke = 0.5 * im[0] * (u * u + v * v + w * w);
+    const U5 c{im[0], im[0] * u, im[0] * v, im[0] * w, im[4] / (ph.gamma - 1.0) + ke};
+    store5(q, g.plane, cidx3(g, gh.i, gh.j, gh.k), c);
+}
+
+// marker_force_system + compute_marker_loadings (crates/cfd_ibm/src/lib.rs:442-480,
+// 601-615) and wall_force_system (:309-395) over the state after a stage: one
+// block, each thread summing a strided share of the markers and of the solid
+// cells with fluid neighbours (the ghost list), then a fixed-order tree sum.
+constexpr int FORCE3_THREADS = 256;
+__global__ void __launch_bounds__(FORCE3_THREADS) forces3_kernel(Geometry g, Physics ph, Ibm ib, const double* q,
+                                                                  DevState* st) {
+    pdl_wait_then_release();
+    __shared__ double red[12][FORCE3_THREADS];
+    double f[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // marker p, v; wall p, v
+    const double gm1 = ph.gamma - 1.0;
+    for (int m = threadIdx.x; m < ib.n_markers; m += FORCE3_THREADS) {
+        const Marker3Dev mk = ib.markers3[m];
+        if (!mk.valid) continue;
+        double img[6];
+        if (!sample_trilinear3(g, ph, q, mk.fluid, mk.lo, mk.t, img)) continue;
+        if (!(isfinite(img[4]) && isfinite(img[5]) && isfinite(img[1]) && isfinite(img[2]) && isfinite(img[3])))
+            continue;
+        const double us[3] = {img[1] - mk.uw[0], img[2] - mk.uw[1], img[3] - mk.uw[2]};
+        const double udotn = us[0] * mk.normal[0] + us[1] * mk.normal[1] + us[2] * mk.normal[2];
+        const double mu = viscosity(ph, img[5]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double ut = us[d] - udotn * mk.normal[d];
+            f[d] += -img[4] * mk.normal[d] * mk.area;
+            f[3 + d] += mu * ut / ib.sample_offset * mk.area;
+        }
+    }
+    const double face_area[3] = {g.h[1] * g.h[2], g.h[0] * g.h[2], g.h[0] * g.h[1]};
+    for (int t = threadIdx.x; t < ib.n_ghost; t += FORCE3_THREADS) {
+        const IbmGhost3Dev gh = ib.ghosts3[t];
+#pragma unroll
+        for (int nbk = 0; nbk < 6; ++nbk) {
+            if (!(gh.fluid & (1u << nbk))) continue;
+            const int dim = nbk >> 1;
+            const double sign = (nbk & 1) ? -1.0 : 1.0;
+            const int di = dim == 0 ? (nbk & 1 ? -1 : 1) : 0, dj = dim == 1 ? (nbk & 1 ? -1 : 1) : 0,
+                      dk = dim == 2 ? (nbk & 1 ? -1 : 1) : 0;
+            const U5 uc = load5(q, g.plane, cidx3(g, gh.i + di, gh.j + dj, gh.k + dk));
+            f[6 + dim] -= pressure5(uc, gm1) * sign * face_area[dim];
+            const double inv = 1.0 / uc.r;
+            const double vel[3] = {uc.mx * inv, uc.my * inv, uc.mz * inv};
+            const double ke = 0.5 * uc.r * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+            const double tt = gm1 * (uc.E - ke) * inv / ph.r_gas;
+            const double mu = viscosity(ph, tt);
+#pragma unroll
+            for (int td = 0; td < 3; ++td)
+                if (td != dim) f[9 + td] += mu * vel[td] / (0.5 * g.h[dim]) * face_area[dim];
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 12; ++v) red[v][threadIdx.x] = f[v];
+    __syncthreads();
+    for (int s = FORCE3_THREADS / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+#pragma unroll
+            for (int v = 0; v < 12; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int v = 0; v < 12; ++v) ib.force_out[v] = red[v][0];
+        if (ib.history && st->hist_pos < st->hist_cap) {
+            for (int d = 0; d < 6; ++d) ib.history[6 * st->hist_pos + d] = red[d][0];
+            st->hist_pos += 1;
+        }
+    }
 }
 
 // ---- launches ---------------------------------------------------------------

@@ -20,7 +20,7 @@ _LIB = None
 # every entry point of include/efvm.h
 EXPORTS = (
     "efvm_abi_version", "efvm_create", "efvm_destroy", "efvm_last_error", "efvm_upload_state",
-    "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
+    "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_set_spheres", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
@@ -57,6 +57,7 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_upload_state.argtypes = [vp, dp, i64, i64, i64]
     L.efvm_download_state.argtypes = [vp, dp, i64, i64, i64]
     L.efvm_upload_state_3d.argtypes = [vp, dp, i64, i64, i64, i64]
+    L.efvm_set_spheres.argtypes = [vp, C.POINTER(abi.EfvmSphere), i32, i32, dp]
     L.efvm_download_state_3d.argtypes = [vp, dp, i64, i64, i64, i64]
     L.efvm_get_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.efvm_set_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
@@ -264,6 +265,14 @@ class Context:
         ca = arr_t(*[abi.EfvmCylinder(*c) for c in cyls])
         fs = np.ascontiguousarray(freestream, dtype=np.float64)
         self._check(self.L.efvm_set_cylinders(self.h, ca, len(cyls), _dp(fs)))
+
+    def set_spheres(self, spheres, freestream, n_markers: int = 2000) -> None:
+        """Immersed spheres (abi.make_sphere values) on a 3-D context; call again
+        between steps to move them."""
+        arr_t = abi.EfvmSphere * max(len(spheres), 1)
+        sa = arr_t(*spheres)
+        fs = np.ascontiguousarray(freestream, dtype=np.float64)
+        self._check(self.L.efvm_set_spheres(self.h, sa, len(spheres), int(n_markers), _dp(fs)))
 
     def marker_force(self) -> np.ndarray:
         out = np.zeros(6)

@@ -141,6 +141,15 @@ typedef struct {
     double cx, cy, radius;
 } efvm_cylinder;
 
+/* A rigid sphere with its kinematic state (SphereBody, crates/cfd_ibm/src/
+ * sphere.rs:26-72): centre, radius, translational velocity (vx, vy, vz) and
+ * angular velocity (wx, wy, wz); the wall moves at v + w x (p - centre). */
+typedef struct {
+    double cx, cy, cz, radius;
+    double vx, vy, vz;
+    double wx, wy, wz;
+} efvm_sphere;
+
 /* The Shu isentropic vortex used as exact solution (crates/cfd_solver/tests/
  * isentropic_vortex_muscl_convergence.rs:48-64): centre (cx0,cy0) at t=0,
  * translated by (mean_u,mean_v).  min_image != 0 measures the displacement
@@ -243,6 +252,18 @@ int efvm_cfl(efvm_ctx* ctx, double* dt_out);
  * seeds the cells that flip solid/fluid. */
 int efvm_set_cylinders(efvm_ctx* ctx, const efvm_cylinder* cylinders, int32_t n,
                        const double freestream[5]);
+/* SphereIbmPlugin::new(..).with_markers(n_markers) + GhostCellIbmPlugin
+ * (crates/cfd_ibm/src/sphere.rs:77-292) on a 3-D context: the solid mask
+ * (cell centres inside any sphere, flipped cells seeded as with cylinders), the
+ * ghost list (solid cells with a fluid face neighbour, image point mirrored
+ * across the nearest sphere, wall velocity of that body at the ghost's wall
+ * footprint) and max(n_markers, 12) Fibonacci markers per sphere of area
+ * 4 pi R^2 / n.  A moving body: call again between steps with the new centres
+ * and velocities; the lists are rebuilt before the next substep, as the
+ * reference's Setup systems do every substep.  Marker and staircase wall forces
+ * are then read with efvm_marker_force / efvm_wall_force. */
+int efvm_set_spheres(efvm_ctx* ctx, const efvm_sphere* spheres, int32_t n, int32_t n_markers,
+                     const double freestream[5]);
 /* MarkerForce{pressure,viscous} of the last Output phase
  * (crates/cfd_ibm/src/lib.rs:442-480,601-615). */
 int efvm_marker_force(efvm_ctx* ctx, double out[6]);

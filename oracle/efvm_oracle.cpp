@@ -788,6 +788,116 @@ void Case::compute_cylinder_markers() {
     }
 }
 
+// refresh_sphere_mask, crates/cfd_ibm/src/sphere.rs:81-111
+void Case::refresh_sphere_mask() {
+    for (int k = 0; k < mesh.n[2]; ++k)
+        for (int j = 0; j < mesh.n[1]; ++j)
+            for (int i = 0; i < mesh.n[0]; ++i) {
+                const size_t c = mesh.idx(i, j, k);
+                double cc[3];
+                mesh.cell_centroid(c, cc);
+                bool inside = false;
+                for (const Sphere& b : spheres)
+                    if (b.signed_distance(cc) < 0.0) { inside = true; break; }
+                const bool was = solid[c] != 0;
+                if (inside && !was) {
+                    solid[c] = 1;
+                    u[c] = stagnant;
+                    rhs[c] = ConsVar();
+                } else if (!inside && was) {
+                    solid[c] = 0;
+                    u[c] = ambient;
+                    rhs[c] = ConsVar();
+                }
+            }
+}
+
+// compute_sphere_ghosts, crates/cfd_ibm/src/sphere.rs:116-195
+void Case::compute_sphere_ghosts() {
+    ghosts.clear();
+    if (spheres.empty()) return;
+    const int ng = mesh.ng;
+    const size_t sx = 1, sy = (size_t)mesh.N[0], sz = (size_t)mesh.N[0] * mesh.N[1];
+    for (int k = 0; k < mesh.n[2]; ++k)
+        for (int j = 0; j < mesh.n[1]; ++j)
+            for (int i = 0; i < mesh.n[0]; ++i) {
+                const size_t c = mesh.idx_raw(i + ng, j + ng, k + ng);
+                if (!solid[c]) continue;
+                const size_t nbrs[6] = {c + sx, c - sx, c + sy, c - sy, c + sz, c - sz};
+                bool any_fluid = false;
+                for (size_t nbi : nbrs) any_fluid = any_fluid || !solid[nbi];
+                if (!any_fluid) continue;
+                IbmGhost gh;
+                gh.idx = c;
+                mesh.cell_centroid(c, gh.cell_center);
+                double best_abs = std::numeric_limits<double>::max(), best_signed = 0.0;
+                double best_normal[3] = {1.0, 0.0, 0.0}, best_wall[3] = {0.0, 0.0, 0.0};
+                uint32_t best_body = 0;
+                for (size_t bid = 0; bid < spheres.size(); ++bid) {
+                    const double sd = spheres[bid].signed_distance(gh.cell_center);
+                    if (std::fabs(sd) < best_abs) {
+                        best_abs = std::fabs(sd);
+                        best_signed = sd;
+                        spheres[bid].normal(gh.cell_center, best_normal);
+                        best_body = (uint32_t)bid;
+                        // the body's surface velocity at the cell's wall footprint
+                        const double foot[3] = {gh.cell_center[0] - sd * best_normal[0],
+                                                gh.cell_center[1] - sd * best_normal[1],
+                                                gh.cell_center[2] - sd * best_normal[2]};
+                        spheres[bid].wall_velocity(foot, best_wall);
+                    }
+                }
+                const double push = 2.0 * (-best_signed);
+                for (int d = 0; d < 3; ++d) {
+                    gh.image_point[d] = gh.cell_center[d] + push * best_normal[d];
+                    gh.normal[d] = best_normal[d];
+                    gh.wall_velocity[d] = best_wall[d];
+                }
+                gh.body_id = best_body;
+                ghosts.push_back(gh);
+            }
+}
+
+// compute_sphere_markers + sphere_markers, crates/cfd_ibm/src/sphere.rs:201-245:
+// the golden-angle spherical Fibonacci lattice, area 4 pi R^2 / n per marker.
+void Case::compute_sphere_markers() {
+    markers.clear();
+    if (spheres.empty()) return;
+    const int n = std::max(sphere_markers_n, 12);
+    const double golden = PI * (3.0 - std::sqrt(5.0));
+    for (size_t bid = 0; bid < spheres.size(); ++bid) {
+        const Sphere& b = spheres[bid];
+        const double area = 4.0 * PI * b.r * b.r / (double)n;
+        for (int m = 0; m < n; ++m) {
+            const double zr = 1.0 - 2.0 * ((double)m + 0.5) / (double)n;
+            const double rr = std::sqrt(std::max(1.0 - zr * zr, 0.0));
+            const double phi = golden * (double)m;
+            const double dir[3] = {rr * std::cos(phi), rr * std::sin(phi), zr};
+            IbmMarker mk;
+            mk.body_id = (uint32_t)bid;
+            for (int d = 0; d < 3; ++d) {
+                mk.position[d] = b.c[d] + b.r * dir[d];
+                mk.normal[d] = dir[d];
+            }
+            mk.area = area;
+            b.wall_velocity(mk.position, mk.wall_velocity);
+            markers.push_back(mk);
+        }
+    }
+}
+
+void Case::geometry_systems() {
+    if (!spheres.empty()) {
+        refresh_sphere_mask();
+        compute_sphere_ghosts();
+        compute_sphere_markers();
+    } else {
+        refresh_cylinder_mask();
+        compute_cylinder_ghosts();
+        compute_cylinder_markers();
+    }
+}
+
 // sample_trilinear, :106-149
 bool Case::sample_trilinear(const double point[3], PrimVar& out) const {
     size_t lo_idx;
@@ -903,11 +1013,7 @@ void Case::wall_force_system() {
 void Case::substep() {
     // Setup: cfl_system (SolverPlugin) then the cylinder geometry (CylinderIbmPlugin)
     cfl_system();
-    if (ibm) {
-        refresh_cylinder_mask();
-        compute_cylinder_ghosts();
-        compute_cylinder_markers();
-    }
+    if (ibm) geometry_systems();
     // Halo
     halo_system();
     // Boundary: the stock fill, then the case's parabolic inlet
@@ -1213,16 +1319,48 @@ int oracle_set_cylinders(void* hp, const efvm_cylinder* c, int32_t n, const doub
     return EFVM_OK;
 }
 
+// SphereIbmPlugin::new(bodies, freestream).with_markers(n_markers),
+// crates/cfd_ibm/src/sphere.rs:262-286: the bodies replace any earlier ones
+// (an FSI driver moves them between steps this way).
+int oracle_set_spheres(void* hp, const efvm_sphere* s, int32_t n, int32_t n_markers, const double fs[5]) {
+    Case& cs = ((OracleHandle*)hp)->cs;
+    cs.spheres.clear();
+    for (int i = 0; i < n; ++i)
+        cs.spheres.push_back(Sphere{{s[i].cx, s[i].cy, s[i].cz}, s[i].radius, {s[i].vx, s[i].vy, s[i].vz},
+                                    {s[i].wx, s[i].wy, s[i].wz}});
+    cs.sphere_markers_n = n_markers;
+    const ConsVar f(fs[0], fs[1], fs[2], fs[3], fs[4]);
+    cs.stagnant = ConsVar(f.rho, 0.0, 0.0, 0.0, f.rho_e - f.kinetic_energy());
+    cs.ambient = f;
+    cs.ibm = true;
+    return EFVM_OK;
+}
+
+// The markers compute_sphere_markers places for one sphere (test access to the
+// lattice): per marker position[3], normal[3], area, wall_velocity[3] (10 doubles).
+int oracle_sphere_markers(const efvm_sphere* s, int32_t n_markers, double* out) {
+    Case cs;
+    cs.spheres.push_back(Sphere{{s->cx, s->cy, s->cz}, s->radius, {s->vx, s->vy, s->vz}, {s->wx, s->wy, s->wz}});
+    cs.sphere_markers_n = n_markers;
+    cs.compute_sphere_markers();
+    for (size_t m = 0; m < cs.markers.size(); ++m) {
+        double* o = out + 10 * m;
+        for (int d = 0; d < 3; ++d) {
+            o[d] = cs.markers[m].position[d];
+            o[3 + d] = cs.markers[m].normal[d];
+            o[7 + d] = cs.markers[m].wall_velocity[d];
+        }
+        o[6] = cs.markers[m].area;
+    }
+    return (int)cs.markers.size();
+}
+
 // The Setup-phase geometry systems alone (refresh_cylinder_mask,
 // compute_cylinder_ghosts, compute_cylinder_markers; crates/cfd_ibm/src/lib.rs:155-254,566-598),
 // as a freshly prepared App runs them before a restore overwrites its fields.
 int oracle_apply_geometry(void* hp) {
     Case& cs = ((OracleHandle*)hp)->cs;
-    if (cs.ibm) {
-        cs.refresh_cylinder_mask();
-        cs.compute_cylinder_ghosts();
-        cs.compute_cylinder_markers();
-    }
+    if (cs.ibm) cs.geometry_systems();
     return EFVM_OK;
 }
 

@@ -253,6 +253,26 @@ struct Cylinder {
         else { n[0] = dx / rr; n[1] = dy / rr; n[2] = 0.0; }
     }
 };
+// SphereBody, crates/cfd_ibm/src/sphere.rs:26-72
+struct Sphere {
+    double c[3], r, v[3], w[3];
+    double signed_distance(const double p[3]) const {
+        const double d0 = p[0] - c[0], d1 = p[1] - c[1], d2 = p[2] - c[2];
+        return std::sqrt(d0 * d0 + d1 * d1 + d2 * d2) - r;
+    }
+    void normal(const double p[3], double n[3]) const {
+        const double d0 = p[0] - c[0], d1 = p[1] - c[1], d2 = p[2] - c[2];
+        const double rr = std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        if (rr < 1e-12) { n[0] = 1.0; n[1] = 0.0; n[2] = 0.0; }
+        else { n[0] = d0 / rr; n[1] = d1 / rr; n[2] = d2 / rr; }
+    }
+    void wall_velocity(const double p[3], double out[3]) const {
+        const double r0 = p[0] - c[0], r1 = p[1] - c[1], r2 = p[2] - c[2];
+        out[0] = v[0] + w[1] * r2 - w[2] * r1;
+        out[1] = v[1] + w[2] * r0 - w[0] * r2;
+        out[2] = v[2] + w[0] * r1 - w[1] * r0;
+    }
+};
 struct IbmGhost {
     size_t idx;
     double cell_center[3], image_point[3], normal[3];
@@ -284,6 +304,8 @@ struct Case {
     SolverState ss;
     bool ibm = false;
     std::vector<Cylinder> cyls;
+    std::vector<Sphere> spheres;                 // SphereBodies (3-D)
+    int sphere_markers_n = 2000;                 // SphereMarkerCfg
     ConsVar stagnant, ambient;                   // MaskConsts
     std::vector<IbmGhost> ghosts;
     std::vector<IbmMarker> markers;
@@ -314,6 +336,10 @@ struct Case {
     void refresh_cylinder_mask();
     void compute_cylinder_ghosts();
     void compute_cylinder_markers();
+    void refresh_sphere_mask();
+    void compute_sphere_ghosts();
+    void compute_sphere_markers();
+    void geometry_systems();  // the Setup-phase geometry of whichever bodies are set
     void apply_ibm_ghost_bc();
     void zero_solid_rhs();
     void marker_force_system();

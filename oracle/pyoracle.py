@@ -59,6 +59,8 @@ def lib(parallel: bool = False) -> C.CDLL:
     L.oracle_get_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.oracle_set_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.oracle_set_cylinders.argtypes = [vp, C.POINTER(abi.EfvmCylinder), i32, dp]
+    L.oracle_set_spheres.argtypes = [vp, C.POINTER(abi.EfvmSphere), i32, i32, dp]
+    L.oracle_sphere_markers.argtypes = [C.POINTER(abi.EfvmSphere), i32, dp]
     L.oracle_marker_force.argtypes = [vp, dp]
     L.oracle_wall_force.argtypes = [vp, dp]
     L.oracle_ibm_counts.argtypes = [vp, C.POINTER(i64), C.POINTER(i64)]
@@ -95,6 +97,14 @@ def _dp(a: np.ndarray):
 
 def arr(x) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def sphere_markers(sphere: abi.EfvmSphere, n_markers: int) -> np.ndarray:
+    """[n, 10]: position, normal, area, wall velocity of the Fibonacci markers."""
+    L = lib()
+    out = np.zeros((max(n_markers, 12), 10))
+    n = L.oracle_sphere_markers(C.byref(sphere), int(n_markers), _dp(out))
+    return out[:n]
 
 
 class OracleCase:
@@ -180,6 +190,13 @@ class OracleCase:
         ca = arr_t(*[abi.EfvmCylinder(*c) for c in cyls])
         fs = arr(freestream)
         self.L.oracle_set_cylinders(self.h, ca, len(cyls), _dp(fs))
+
+    def set_spheres(self, spheres, freestream, n_markers: int = 2000) -> None:
+        """spheres: abi.EfvmSphere values (abi.make_sphere)."""
+        arr_t = abi.EfvmSphere * max(len(spheres), 1)
+        sa = arr_t(*spheres)
+        fs = arr(freestream)
+        self.L.oracle_set_spheres(self.h, sa, len(spheres), int(n_markers), _dp(fs))
 
     def marker_force(self) -> np.ndarray:
         out = np.zeros(6)

@@ -1,0 +1,137 @@
+"""Immersed spheres on 3-D meshes (SphereIbmPlugin + GhostCellIbmPlugin,
+crates/cfd_ibm/src/sphere.rs): the CUDA path through the C-ABI against the CPU
+oracle's restatement of the reference's sphere systems.
+
+Compared exactly: the solid and ghost-cell counts.  Compared within the
+tolerances of test_gpu_parity.py: the state (solid cells included, so the
+ghost-cell mirror is checked) after one and several RK3 steps, for a fixed
+sphere, a translating and spinning one (wall velocity in the mirror and the
+marker traction), a body moved between steps (cells flip and are re-seeded),
+and a walled viscous channel.  The marker and staircase forces are sums over a
+few thousand terms in another order: they are compared to 1e-10 of the
+pressure-force scale p A (A = 4 pi R^2)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from dev_field_efvm_b200 import abi, cases
+from dev_field_efvm_b200.device import Context, EfvmError
+from oracle import pyoracle as po
+from test_gpu_3d import TOL_MANY_STEPS, TOL_ONE_STEP, rel_err3
+
+pytestmark = pytest.mark.gpu
+
+
+def box_flow(n=40, viscous=False, mean=(0.3, 0.1, 0.05)):
+    """A periodic box with a uniform flow and a small z-dependent density wave."""
+    grid, params, u, _ = cases.vortex_tube_case(n, n, beta=0.0, mean=mean, amp=0.02, viscous=viscous, mu=5e-3)
+    return grid, params, u
+
+
+def run_pair(grid, params, u, spheres, n_markers, steps, moves=None):
+    o, d = po.OracleCase(grid, params), Context(grid, params)
+    o.upload(u)
+    d.upload(u)
+    fs = u[0, 0, 0].copy()
+    o.set_spheres(spheres, fs, n_markers)
+    d.set_spheres(spheres, fs, n_markers)
+    return o, d, fs
+
+
+def forces_close(o, d, p_ref, radius):
+    scale = p_ref * 4.0 * math.pi * radius ** 2
+    for a, b in ((o.marker_force(), d.marker_force()), (o.wall_force(), d.wall_force())):
+        assert np.max(np.abs(np.asarray(a) - np.asarray(b))) <= 1e-10 * scale, (a, b)
+
+
+@pytest.mark.parametrize("muscl", [False, True])
+def test_fixed_sphere_in_a_periodic_box(muscl):
+    grid, params, u = box_flow()
+    params.reconstruction = abi.RECON_MUSCL if muscl else abi.RECON_FIRST_ORDER
+    sph = [abi.make_sphere((5.0, 5.1, 4.9), 1.6)]
+    o, d, fs = run_pair(grid, params, u, sph, 600, 0)
+    o.step(1)
+    d.step(1)
+    assert d.ibm_counts() == o.ibm_counts()
+    assert d.ibm_counts()[1] > 100
+    assert rel_err3(d.download(), o.download()) < TOL_ONE_STEP
+    p_ref = 1.0
+    forces_close(o, d, p_ref, 1.6)
+    o.step(9)
+    d.step(9)
+    assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
+    forces_close(o, d, p_ref, 1.6)
+
+
+def test_moving_spinning_viscous_sphere_and_a_move_between_steps():
+    grid, params, u = box_flow(viscous=True)
+    params.reconstruction = abi.RECON_MUSCL
+    body = dict(radius=1.4, velocity=(0.2, -0.1, 0.05), omega=(0.3, -0.2, 0.5))
+    sph = [abi.make_sphere((4.6, 5.0, 5.2), **body)]
+    o, d, fs = run_pair(grid, params, u, sph, 800, 0)
+    o.step(3)
+    d.step(3)
+    assert d.ibm_counts() == o.ibm_counts()
+    assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
+    forces_close(o, d, 1.0, 1.4)
+    # the FSI driver moves the body between steps: cells flip and are re-seeded
+    sph2 = [abi.make_sphere((4.6 + 0.6, 5.0 - 0.3, 5.2 + 0.2), **body)]
+    o.set_spheres(sph2, fs, 800)
+    d.set_spheres(sph2, fs, 800)
+    o.step(3)
+    d.step(3)
+    assert d.ibm_counts() == o.ibm_counts()
+    assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
+    forces_close(o, d, 1.0, 1.4)
+
+
+def test_two_spheres_in_a_walled_viscous_channel():
+    """Subsonic inflow, pressure outlet, no-slip y walls, slip z walls, Sutherland
+    air; two spheres, so every ghost takes its nearest body."""
+    bcs = {abi.XLO: abi.make_bc(abi.BC_SUBSONIC_INFLOW, rho=1.2, u=30.0, v=0.0, w=0.0, t=300.0),
+           abi.XHI: abi.make_bc(abi.BC_PRESSURE_OUTLET, p=1.0e5),
+           abi.YLO: abi.BC_NO_SLIP_WALL, abi.YHI: abi.BC_NO_SLIP_WALL,
+           abi.ZLO: abi.BC_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+    nx, ny, nz = 48, 24, 20
+    grid = abi.make_grid(nx, ny, hi=(0.04, 0.02, 0.0166667), bcs=bcs, nz=nz)
+    params = abi.make_params(cfl=0.4, viscous=1, viscosity_model=abi.VISC_SUTHERLAND,
+                             reconstruction=abi.RECON_MUSCL)
+    u = cases.prim_to_cons3(np.full((nz, ny, nx), 1.2), 30.0, 0.0, 0.0, np.full((nz, ny, nx), 1.0e5))
+    fs = u[0, 0, 0].copy()
+    sph = [abi.make_sphere((0.012, 0.0095, 0.008), 0.004), abi.make_sphere((0.026, 0.011, 0.0085), 0.0035)]
+    o, d = po.OracleCase(grid, params), Context(grid, params)
+    o.upload(u)
+    d.upload(u)
+    o.set_spheres(sph, fs, 500)
+    d.set_spheres(sph, fs, 500)
+    o.step(5)
+    d.step(5)
+    assert d.ibm_counts() == o.ibm_counts()
+    assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
+    forces_close(o, d, 1.0e5, 0.004)
+
+
+def test_force_history_and_substeps():
+    grid, params, u = box_flow(n=32)
+    sph = [abi.make_sphere((5.0, 5.0, 5.0), 1.7)]
+    o, d, fs = run_pair(grid, params, u, sph, 400, 0)
+    _, hist = d.step(2, history=True)
+    assert hist.shape == (6, 6)
+    for s in range(6):
+        o.substep()
+        np.testing.assert_allclose(hist[s], o.marker_force(), rtol=0, atol=1e-10 * 4.0 * math.pi * 1.7 ** 2)
+
+
+def test_sphere_arguments():
+    grid, params, u = box_flow(n=24)
+    d = Context(grid, params)
+    d.upload(u)
+    with pytest.raises(EfvmError):
+        d.set_spheres([abi.make_sphere((5.0, 5.0, 5.0), -1.0)], u[0, 0, 0])
+    g2, p2, u2, _ = cases.vortex_case(32, periodic=True)
+    c2 = Context(g2, p2)
+    with pytest.raises(EfvmError):
+        c2.set_spheres([abi.make_sphere((5.0, 5.0, 0.1), 1.0)], u2[0, 0])

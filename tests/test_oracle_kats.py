@@ -208,3 +208,25 @@ def test_half_periodic_axis_is_rejected():
     g = abi.make_grid(8, 1, bcs={abi.XLO: abi.BC_PERIODIC})
     with pytest.raises(ValueError, match="periodic"):
         po.OracleCase(g, abi.make_params())
+
+
+# ---- crates/cfd_ibm/src/sphere.rs:298-348 ---------------------------------
+def test_sphere_wall_velocity_and_fibonacci_markers():
+    # rigid wall velocity v + w x r at the +x surface point of the reference's example
+    b = abi.make_sphere((1.0, 2.0, 3.0), 0.5, velocity=(0.1, 0.0, 0.0), omega=(0.0, 0.0, 2.0))
+    m = po.sphere_markers(b, 12)
+    # the lattice's z-extreme markers are off the x axis; check the formula on all
+    for row in m:
+        r = row[0:3] - np.array([1.0, 2.0, 3.0])
+        want = np.array([0.1, 0.0, 0.0]) + np.cross([0.0, 0.0, 2.0], r)
+        assert np.allclose(row[7:10], want, atol=1e-12)
+    # areas sum to 4 pi R^2, markers on the surface with unit radial normals, lattice centred
+    b = abi.make_sphere((0.0, 0.0, 0.0), 0.75)
+    m = po.sphere_markers(b, 4000)
+    assert m.shape == (4000, 10)
+    assert abs(m[:, 6].sum() / (4.0 * np.pi * 0.75 ** 2) - 1.0) < 1e-12
+    assert np.all(np.abs(np.linalg.norm(m[:, 0:3], axis=1) - 0.75) < 1e-9)
+    assert np.all(np.abs(np.linalg.norm(m[:, 3:6], axis=1) - 1.0) < 1e-9)
+    assert np.all(np.abs(m[:, 0:3].mean(axis=0)) < 1e-2)
+    # at least 12 markers whatever is asked (SphereMarkerCfg: n.max(12))
+    assert po.sphere_markers(b, 3).shape[0] == 12
