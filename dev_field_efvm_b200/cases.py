@@ -118,6 +118,30 @@ def vortex_tube_case(n: int, nz: int | None = None, *, mean=(1.0, 1.0, 1.0), bet
     return grid, params, u, {"vortex": v}
 
 
+def sphere_drag_case(nx=144, ny=72, nz=72, *, rho=1.0, p=1.0e5, u_inf=56.1, reynolds=20.0, diameter=0.1,
+                     cfl=0.3, muscl=False, sponge_x_start=0.5, sponge_sigma=2.0e4, n_markers=2000):
+    """Resolved sphere drag at Re = 20 (examples/sphere_drag_validation/main.rs with
+    config.toml): box [-0.3,0.9] x [-0.3,0.3]^2, D = 0.1 at the origin (D/dx = 12
+    at 144x72x72), subsonic inflow, pressure outlet, symmetry sides, constant mu =
+    rho u D / Re, first-order HLLC, RK3, CFL 0.3, uniform-freestream sponge over
+    x in [0.5, 0.9] with sigma 2e4, 2000 Fibonacci markers."""
+    r_gas = 287.058
+    t_inf = p / (rho * r_gas)
+    bcs = {abi.XLO: abi.make_bc(abi.BC_SUBSONIC_INFLOW, rho=rho, u=u_inf, v=0.0, w=0.0, t=t_inf),
+           abi.XHI: abi.make_bc(abi.BC_PRESSURE_OUTLET, p=p),
+           abi.YLO: abi.BC_SYMMETRY, abi.YHI: abi.BC_SYMMETRY, abi.ZLO: abi.BC_SYMMETRY, abi.ZHI: abi.BC_SYMMETRY}
+    grid = abi.make_grid(nx, ny, lo=(-0.3, -0.3, -0.3), hi=(0.9, 0.3, 0.3), bcs=bcs, nz=nz)
+    mu = rho * u_inf * diameter / reynolds
+    params = abi.make_params(cfl=cfl, viscous=1, viscosity_model=abi.VISC_CONSTANT, mu=mu,
+                             reconstruction=abi.RECON_MUSCL if muscl else abi.RECON_FIRST_ORDER,
+                             sponge=1, sponge_x_start=sponge_x_start, sponge_x_end=0.9, sponge_sigma=sponge_sigma,
+                             sponge_u_max=u_inf, sponge_rho=rho, sponge_p=p)
+    u = prim_to_cons3(np.full((nz, ny, nx), rho), u_inf, 0.0, 0.0, np.full((nz, ny, nx), p))
+    sphere = abi.make_sphere((0.0, 0.0, 0.0), 0.5 * diameter)
+    q = 0.5 * rho * u_inf * u_inf * math.pi * (0.5 * diameter) ** 2
+    return grid, params, u, {"spheres": [sphere], "freestream": u[0, 0, 0].copy(), "n_markers": n_markers, "q": q}
+
+
 def cylinder_case(nx=440, ny=82, *, u_mean=50.0, rho=1.0, p=1.0e5, reynolds=20.0, cfl=0.3, muscl=False,
                   limiter=abi.LIMITER_MINMOD, sponge_sigma=1.0e4, sponge_x_start=1.4, precision=abi.PREC_FP64,
                   lz=0.041):

@@ -584,8 +584,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     if (d3) {
         if (slab) return bad(EFVM_ERR_UNSUPPORTED, "slabs are built for 2-D meshes (nz == 1)");
         if (p.precision != EFVM_PREC_FP64) return bad(EFVM_ERR_UNSUPPORTED, "3-D meshes run in FP64");
-        if (p.parabolic_inflow || p.sponge)
-            return bad(EFVM_ERR_UNSUPPORTED, "the parabolic inlet and the outlet sponge are 2-D case systems");
+        if (p.parabolic_inflow) return bad(EFVM_ERR_UNSUPPORTED, "the parabolic inlet is a 2-D case system");
     }
     if (gr.nx < 2 || gr.ny < 1) return bad(EFVM_ERR_INVALID_ARG, "nx must be >= 2 and ny >= 1");
     for (int a = 0; a < 3; ++a)

@@ -436,7 +436,23 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
 #pragma unroll
                     for (int v = 0; v < 5; ++v) nwv[v] = __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt));
                 }
-                const U5 nwu{nwv[0], nwv[1], nwv[2], nwv[3], nwv[4]};
+                U5 nwu{nwv[0], nwv[1], nwv[2], nwv[3], nwv[4]};
+                if (a.completes_step && ph.sponge) {
+                    // the sphere case's outlet sponge toward the uniform freestream
+                    // (rho, u_max, 0, 0, p), examples/sphere_drag_validation/main.rs:119-160
+                    const double cx = centre(g.lo[0], g.h[0], i);
+                    if (cx >= ph.sponge_x_start) {
+                        const double inv_w = 1.0 / (ph.sponge_x_end - ph.sponge_x_start);
+                        const double s = fmin(fmax((cx - ph.sponge_x_start) * inv_w, 0.0), 1.0);
+                        const double f = fmin(ph.sponge_sigma * s * s * dt, 1.0);
+                        const U5 tg = prim_to_cons5(ph.sponge_rho, ph.sponge_u_max, 0.0, 0.0, ph.sponge_p, gm1);
+                        nwu.r += f * (tg.r - nwu.r);
+                        nwu.mx += f * (tg.mx - nwu.mx);
+                        nwu.my += f * (tg.my - nwu.my);
+                        nwu.mz += f * (tg.mz - nwu.mz);
+                        nwu.E += f * (tg.E - nwu.E);
+                    }
+                }
                 store5(a.uout, P, o, nwu);
                 write_ghosts3(g, ph, a.uout, i, j, k, nwu);
                 int bad = 0;

@@ -116,7 +116,10 @@ typedef struct {
     int32_t parabolic_inflow;
     int32_t reserved0;
     double inflow_u_max, inflow_height, inflow_rho;
-    /* downstream sponge after each completed step, main.rs:186-229 */
+    /* downstream sponge after each completed step, main.rs:186-229: toward the
+     * parabolic profile of height sponge_height on a 2-D mesh; toward the uniform
+     * freestream (sponge_rho, sponge_u_max, 0, 0, sponge_p) on a 3-D mesh, the
+     * sphere case's sponge (examples/sphere_drag_validation/main.rs:119-160) */
     int32_t sponge;
     int32_t reserved1;
     double sponge_x_start, sponge_x_end, sponge_sigma;

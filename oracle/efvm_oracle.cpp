@@ -666,7 +666,10 @@ void Case::outlet_sponge_system() {
                 if (cx < x0) continue;
                 const double s = std::min(std::max((cx - x0) * inv_w, 0.0), 1.0);
                 const double f = std::fmin(sig * s * s * dt, 1.0);
-                const double uy = 4.0 * um * cy * (h - cy) / (h * h);
+                // a 3-D mesh relaxes toward the uniform freestream (rho, u_max, 0, 0, p),
+                // examples/sphere_drag_validation/main.rs:119-160; 2-D toward the parabolic
+                // inlet profile, examples/cylinder_drag_validation/main.rs:186-229
+                const double uy = mesh.n[2] > 1 ? um : 4.0 * um * cy * (h - cy) / (h * h);
                 const ConsVar target = eos.prim_to_cons(PrimVar{rho, uy, 0.0, 0.0, p, p / (rho * R_GAS_AIR)});
                 ConsVar& uu = u[idx];
                 uu.rho += f * (target.rho - uu.rho);
