@@ -126,6 +126,11 @@ class EfvmCylinder(C.Structure):
     _fields_ = [("cx", C.c_double), ("cy", C.c_double), ("radius", C.c_double)]
 
 
+class EfvmDisc(C.Structure):
+    """A moving 2-D disc: centre, radius, velocity, spin (efvm_disc)."""
+    _fields_ = [(n, C.c_double) for n in ("cx", "cy", "radius", "vx", "vy", "omega")]
+
+
 class EfvmSphere(C.Structure):
     """centre, radius, translational velocity, angular velocity (efvm_sphere)."""
     _fields_ = [(n, C.c_double) for n in ("cx", "cy", "cz", "radius", "vx", "vy", "vz", "wx", "wy", "wz")]

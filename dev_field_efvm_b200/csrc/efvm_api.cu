@@ -49,6 +49,10 @@ struct efvm_ctx {
     bool ibm = false;
     bool geom_dirty = false;
     std::vector<double> cyl_host;  // cx, cy, r per body
+    std::vector<double> disc_motion;  // vx, vy, omega per body (moving discs; zero for cylinders)
+    int cyl_markers = 64;             // markers per cylinder / disc
+    bool disc_rule = false;           // moving discs: mirror only cells with a fluid in-plane neighbour
+    int64_t n_mirror = 0;             // solid cells the mirror rewrites
     std::vector<double> sph_host;  // 3-D spheres: efvm_sphere's 10 doubles per body
     double* sph_dev = nullptr;
     int sphere_markers = 2000;     // Fibonacci markers per sphere
@@ -152,6 +156,19 @@ int sync_control(efvm_ctx* c, int stop_at_t, double t_stop, long long hist_cap) 
 }
 
 // Build the IBM ghost list and marker sample points after the device mask flip.
+// Rigid surface velocity v + omega z x (p - c) of disc b (Disc::wall_velocity,
+// examples/dkt_sedimentation/main.rs:94-102); zero for a cylinder at rest.
+void disc_wall_velocity(const efvm_ctx* c, int b, const double p[2], double out[2]) {
+    if (c->disc_motion.empty()) {
+        out[0] = out[1] = 0.0;
+        return;
+    }
+    const double rx = p[0] - c->cyl_host[3 * b], ry = p[1] - c->cyl_host[3 * b + 1];
+    const double* m = &c->disc_motion[3 * b];
+    out[0] = m[0] - m[2] * ry;
+    out[1] = m[1] + m[2] * rx;
+}
+
 int build_ibm_lists(efvm_ctx* c) {
     const Geometry& g = c->g;
     std::vector<uint8_t> m((size_t)g.nx * g.ny);
@@ -171,6 +188,7 @@ int build_ibm_lists(efvm_ctx* c) {
     };
     std::vector<IbmGhostDev> ghosts;
     c->n_solid = 0;
+    c->n_mirror = 0;
     for (int j = 0; j < g.ny; ++j)
         for (int i = 0; i < g.nx; ++i) {
             if (!m[(size_t)j * g.nx + i]) continue;
@@ -181,6 +199,7 @@ int build_ibm_lists(efvm_ctx* c) {
             const double cc[2] = {centre_h(g.lo[0], g.h[0], i), centre_h(g.lo[1], g.h[1], j)};
             double best_abs = std::numeric_limits<double>::max(), best_signed = 0.0;
             double nrm[2] = {1.0, 0.0};
+            int best_b = 0;
             for (int b = 0; b < ncyl; ++b) {
                 const double dx = cc[0] - c->cyl_host[3 * b], dy = cc[1] - c->cyl_host[3 * b + 1];
                 const double r = std::sqrt(dx * dx + dy * dy);
@@ -188,6 +207,7 @@ int build_ibm_lists(efvm_ctx* c) {
                 if (std::fabs(s) < best_abs) {
                     best_abs = std::fabs(s);
                     best_signed = s;
+                    best_b = b;
                     if (r < 1e-12) { nrm[0] = 1.0; nrm[1] = 0.0; }
                     else { nrm[0] = dx / r; nrm[1] = dy / r; }
                 }
@@ -197,10 +217,18 @@ int build_ibm_lists(efvm_ctx* c) {
             IbmGhostDev gh{};
             gh.i = i;
             gh.j = j;
+            // the nearest body's wall velocity at the cell's wall footprint
+            // (compute_disc_ghosts, examples/dkt_sedimentation/main.rs:175-249)
+            const double foot[2] = {cc[0] - best_signed * nrm[0], cc[1] - best_signed * nrm[1]};
+            disc_wall_velocity(c, best_b, foot, gh.uw);
             gh.valid = locate_h(g, ip[0], ip[1], gh.lo_i, gh.lo_j, gh.tx, gh.ty) ? 1 : 0;
             const int nbi[4] = {i + 1, i - 1, i, i}, nbj[4] = {j, j, j + 1, j - 1};
             for (int k = 0; k < 4; ++k)
                 if (!solid(nbi[k], nbj[k])) gh.fluid |= 1u << (FLUID_NB_SHIFT + k);
+            if (!c->disc_rule || (gh.fluid & (0xFu << FLUID_NB_SHIFT))) {
+                gh.fluid |= GHOST_MIRROR_BIT;
+                ++c->n_mirror;
+            }
             if (gh.valid) gh.fluid |= corner_bits(gh.lo_i, gh.lo_j);
             ghosts.push_back(gh);
         }
@@ -210,7 +238,7 @@ int build_ibm_lists(efvm_ctx* c) {
     const double z_lo = centre_h(g.lo[2], g.h[2], 0) - 0.5 * g.h[2];
     const double z_hi = centre_h(g.lo[2], g.h[2], 0) + 0.5 * g.h[2];
     const double lz = z_hi - z_lo;
-    const int n_theta = 64, n_z = 1;
+    const int n_theta = c->cyl_markers, n_z = 1;
     const double offset = g.h[0];  // marker_force_system: sample offset = spacing(0, 0)
     for (int b = 0; b < ncyl; ++b) {
         const double cx = c->cyl_host[3 * b], cy = c->cyl_host[3 * b + 1], r = c->cyl_host[3 * b + 2];
@@ -230,6 +258,12 @@ int build_ibm_lists(efvm_ctx* c) {
             mk.pos[0] = px;
             mk.pos[1] = py;
             mk.body = b;
+            const double pp[2] = {px, py};
+            double uw2[2];
+            disc_wall_velocity(c, b, pp, uw2);
+            mk.wall_velocity[0] = uw2[0];
+            mk.wall_velocity[1] = uw2[1];
+            mk.wall_velocity[2] = 0.0;
             markers.push_back(mk);
         }
     }
@@ -1275,6 +1309,9 @@ int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const d
     }
     if (has_halo(c)) return fail(c, EFVM_ERR_UNSUPPORTED, "IBM cylinders are not supported on a slab");
     c->cyl_host.clear();
+    c->disc_motion.clear();
+    c->cyl_markers = 64;
+    c->disc_rule = false;
     for (int b = 0; b < n; ++b) {
         if (!(cyl[b].radius > 0.0)) return fail(c, EFVM_ERR_INVALID_ARG, "cylinder radius must be > 0");
         c->cyl_host.push_back(cyl[b].cx);
@@ -1294,6 +1331,24 @@ int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const d
     c->ibm = true;
     c->geom_dirty = true;
     c->graph_valid = false;
+    return EFVM_OK;
+}
+
+int efvm_set_discs(efvm_ctx* c, const efvm_disc* d, int32_t n, int32_t n_theta, const double fs[5]) {
+    if (is_3d(c)) return refuse_3d(c, "efvm_set_discs");
+    if (!c || n < 0 || n_theta < 1 || (n > 0 && (!d || !fs))) return fail(c, EFVM_ERR_INVALID_ARG, "invalid disc arguments");
+    std::vector<efvm_cylinder> cyl((size_t)n);
+    for (int b = 0; b < n; ++b) cyl[b] = efvm_cylinder{d[b].cx, d[b].cy, d[b].radius};
+    const int rc = efvm_set_cylinders(c, n ? cyl.data() : nullptr, n, fs);
+    if (rc || n == 0) return rc;
+    c->disc_motion.clear();
+    for (int b = 0; b < n; ++b) {
+        c->disc_motion.push_back(d[b].vx);
+        c->disc_motion.push_back(d[b].vy);
+        c->disc_motion.push_back(d[b].omega);
+    }
+    c->cyl_markers = n_theta;
+    c->disc_rule = true;
     return EFVM_OK;
 }
 
@@ -1356,7 +1411,7 @@ int efvm_ibm_counts(efvm_ctx* c, int64_t* n_solid, int64_t* n_ghost) {
         if (rc) return rc;
     }
     *n_solid = c->ibm ? c->n_solid : 0;
-    *n_ghost = c->ibm ? c->ibm_desc.n_ghost : 0;
+    *n_ghost = c->ibm ? (is_3d(c) ? c->ibm_desc.n_ghost : c->n_mirror) : 0;
     return EFVM_OK;
 }
 

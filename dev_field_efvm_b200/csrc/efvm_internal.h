@@ -97,6 +97,12 @@ struct Physics {
 // fixed when the lists are built.
 constexpr unsigned FLUID_NB_SHIFT = 0;      // +x, -x, +y, -y face neighbour (ghosts only)
 constexpr unsigned FLUID_CORNER_SHIFT = 4;  // bilinear corner k = 2*di + dj
+// Set on the solid cells the mirror rewrites.  With cylinders that is every solid
+// cell (the 2-D mesh's z neighbours are fluid ghost layers); with the moving
+// discs only those with a fluid in-plane neighbour (compute_disc_ghosts,
+// examples/dkt_sedimentation/main.rs:175-249).  The list holds every solid cell
+// either way, for the staircase wall force.
+constexpr unsigned GHOST_MIRROR_BIT = 1u << 12;
 constexpr int IBM_THREADS = 128;            // threads per block of the IBM kernel
 
 // One solid cell that the IBM mirror refills every substage (IbmGhostCells).
@@ -106,6 +112,7 @@ struct IbmGhostDev {
     double tx, ty;           // bilinear fractions
     int valid;               // locate() succeeded
     unsigned fluid;          // FLUID_* bits
+    double uw[2];            // wall velocity at the cell's wall footprint (moving discs)
 };
 
 // One surface marker (IbmMarker) with its sample point already located.

@@ -790,16 +790,17 @@ __device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& p
     const long long o = cidx(g, gh.i, gh.j);
     const U4 pre = load4(q, g.plane, o);
     double img[5];
-    const bool ok = gh.valid && sample_bilinear(g, ph, q, gh.fluid, gh.lo_i, gh.lo_j, gh.tx, gh.ty, img);
+    const bool ok = gh.valid && (gh.fluid & GHOST_MIRROR_BIT) &&
+                    sample_bilinear(g, ph, q, gh.fluid, gh.lo_i, gh.lo_j, gh.tx, gh.ty, img);
     double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
     zf[0] = pre.r; zf[1] = pre.mx; zf[2] = pre.my; zf[3] = pre.E;
     if (stage == 0 || stage == 3) {
         double* z0 = ib.zg0 + 4LL * k;
         z0[0] = pre.r; z0[1] = pre.mx; z0[2] = pre.my; z0[3] = pre.E;
     }
-    if (!ok) return;
-    // u_ghost = 2 u_wall - u_image with u_wall = 0; rho, p, T from the image
-    const U4 m = prim_to_cons(img[0], 2.0 * 0.0 - img[1], 2.0 * 0.0 - img[2], img[3], ph.gamma - 1.0);
+    if (!ok || !(gh.fluid & GHOST_MIRROR_BIT)) return;
+    // u_ghost = 2 u_wall - u_image; rho, p, T from the image
+    const U4 m = prim_to_cons(img[0], 2.0 * gh.uw[0] - img[1], 2.0 * gh.uw[1] - img[2], img[3], ph.gamma - 1.0);
     store4(q, g.plane, o, m);
 }
 

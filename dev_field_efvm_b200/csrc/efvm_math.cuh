@@ -53,6 +53,14 @@ __device__ __forceinline__ double rsqrt_(double x) {
     return y * fma(-h * y, y, 1.5);
 }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+// The smallest normal value: the .ftz seeds above flush anything below it to
+// zero (and return infinity for it), so their callers keep inputs above it.
+template <class R>
+__device__ __forceinline__ R normal_min();
+template <>
+__device__ __forceinline__ double normal_min<double>() { return 2.2250738585072014e-308; }
+template <>
+__device__ __forceinline__ float normal_min<float>() { return 1.17549435e-38f; }
 
 // Gas-dynamic quantities of one face state, each computed once per face side:
 // 1/rho, normal and tangential velocity, |v|^2, pressure and sound speed
@@ -137,9 +145,14 @@ __device__ __forceinline__ Q4<R> hllc_flux(const Q4<R>& L, const Q4<R>& Rr, R ga
     if (THORNBER) {
         const R vmax2 = fmax_(l.q, r.q);
         const R amax = fmax_(l.a, r.a);
-        // z = min(|v|max / a_max, 1) as vmax2 / sqrt(vmax2 a_max^2): one reciprocal square root
+        // z = min(|v|max / a_max, 1) as vmax2 / sqrt(vmax2 a_max^2): one reciprocal square
+        // root.  Where vmax2 a_max^2 is below the normal range (round-off velocities
+        // near 1e-157 in still gas), z is taken as 0: the reference's z there is
+        // about 1e-160 and scales velocity differences of the same size, far below
+        // any representable change of the flux.
         const R amax2 = amax * amax;
-        const R z = (vmax2 >= amax2) ? R(1) : (vmax2 > R(0) ? vmax2 * rsqrt_(vmax2 * amax2) : R(0));
+        const R prod = vmax2 * amax2;
+        const R z = (vmax2 >= amax2) ? R(1) : (prod >= normal_min<R>() ? vmax2 * rsqrt_(prod) : R(0));
         const R avgn = R(0.5) * (l.un + r.un), avgt = R(0.5) * (l.ut + r.ut);
         const R hz = R(0.5) * z;
         const R dvn = hz * (l.un - r.un), dvt = hz * (l.ut - r.ut);
@@ -265,7 +278,8 @@ __device__ __forceinline__ Q5<R> hllc_flux5(const Q5<R>& L, const Q5<R>& Rr, R g
         const R vmax2 = fmax_(l.q, r.q);
         const R amax = fmax_(l.a, r.a);
         const R amax2 = amax * amax;
-        const R z = (vmax2 >= amax2) ? R(1) : (vmax2 > R(0) ? vmax2 * rsqrt_(vmax2 * amax2) : R(0));
+        const R prod = vmax2 * amax2;  // below the normal range: z = 0, as in hllc_flux
+        const R z = (vmax2 >= amax2) ? R(1) : (prod >= normal_min<R>() ? vmax2 * rsqrt_(prod) : R(0));
         const R avgn = R(0.5) * (l.un + r.un), avgt = R(0.5) * (l.ut + r.ut), avgs = R(0.5) * (l.us + r.us);
         const R hz = R(0.5) * z;
         const R dvn = hz * (l.un - r.un), dvt = hz * (l.ut - r.ut), dvs = hz * (l.us - r.us);

@@ -20,7 +20,7 @@ _LIB = None
 # every entry point of include/efvm.h
 EXPORTS = (
     "efvm_abi_version", "efvm_create", "efvm_destroy", "efvm_last_error", "efvm_upload_state",
-    "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_set_spheres", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
+    "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_set_spheres", "efvm_set_discs", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
     "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
@@ -58,6 +58,7 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_download_state.argtypes = [vp, dp, i64, i64, i64]
     L.efvm_upload_state_3d.argtypes = [vp, dp, i64, i64, i64, i64]
     L.efvm_set_spheres.argtypes = [vp, C.POINTER(abi.EfvmSphere), i32, i32, dp]
+    L.efvm_set_discs.argtypes = [vp, C.POINTER(abi.EfvmDisc), i32, i32, dp]
     L.efvm_download_state_3d.argtypes = [vp, dp, i64, i64, i64, i64]
     L.efvm_get_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.efvm_set_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
@@ -265,6 +266,13 @@ class Context:
         ca = arr_t(*[abi.EfvmCylinder(*c) for c in cyls])
         fs = np.ascontiguousarray(freestream, dtype=np.float64)
         self._check(self.L.efvm_set_cylinders(self.h, ca, len(cyls), _dp(fs)))
+
+    def set_discs(self, discs, freestream, n_theta: int = 64) -> None:
+        """Moving 2-D discs (abi.EfvmDisc values); call again between steps to move them."""
+        arr_t = abi.EfvmDisc * max(len(discs), 1)
+        da = arr_t(*discs)
+        fs = np.ascontiguousarray(freestream, dtype=np.float64)
+        self._check(self.L.efvm_set_discs(self.h, da, len(discs), int(n_theta), _dp(fs)))
 
     def set_spheres(self, spheres, freestream, n_markers: int = 2000) -> None:
         """Immersed spheres (abi.make_sphere values) on a 3-D context; call again

@@ -144,6 +144,14 @@ typedef struct {
     double cx, cy, radius;
 } efvm_cylinder;
 
+/* A moving disc (the 2-D rigid body of examples/dkt_sedimentation/main.rs:66-103):
+ * a z-aligned cylinder with translational velocity (vx, vy) and spin omega about
+ * z; the wall moves at (vx - omega ry, vy + omega rx). */
+typedef struct {
+    double cx, cy, radius;
+    double vx, vy, omega;
+} efvm_disc;
+
 /* A rigid sphere with its kinematic state (SphereBody, crates/cfd_ibm/src/
  * sphere.rs:26-72): centre, radius, translational velocity (vx, vy, vz) and
  * angular velocity (wx, wy, wz); the wall moves at v + w x (p - centre). */
@@ -255,6 +263,13 @@ int efvm_cfl(efvm_ctx* ctx, double* dt_out);
  * seeds the cells that flip solid/fluid. */
 int efvm_set_cylinders(efvm_ctx* ctx, const efvm_cylinder* cylinders, int32_t n,
                        const double freestream[5]);
+/* The moving-disc geometry of examples/dkt_sedimentation/main.rs:143-287 with
+ * GhostCellIbmPlugin on a 2-D context: the cylinder mask, ghosts and markers
+ * (n_theta per disc) with each disc's wall velocity in the ghost mirror and the
+ * marker traction.  An FSI driver calls it between steps with the new centres
+ * and velocities; efvm_body_loads then gives each disc's load and torque.
+ * efvm_set_cylinders is the same with bodies at rest and 64 markers. */
+int efvm_set_discs(efvm_ctx* ctx, const efvm_disc* discs, int32_t n, int32_t n_theta, const double freestream[5]);
 /* SphereIbmPlugin::new(..).with_markers(n_markers) + GhostCellIbmPlugin
  * (crates/cfd_ibm/src/sphere.rs:77-292) on a 3-D context: the solid mask
  * (cell centres inside any sphere, flipped cells seeded as with cylinders), the

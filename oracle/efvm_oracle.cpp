@@ -730,15 +730,18 @@ void Case::compute_cylinder_ghosts() {
             for (int i = 0; i < mesh.n[0]; ++i) {
                 const size_t c = mesh.idx_raw(i + ng, j + ng, k + ng);
                 if (!solid[c]) continue;
+                // CylinderIbmPlugin: the six face neighbours; the moving discs'
+                // compute_disc_ghosts (examples/dkt_sedimentation/main.rs:175-249): the
+                // four in-plane ones
                 const size_t nbrs[6] = {c + sx, c - sx, c + sy, c - sy, c + sz, c - sz};
                 bool any_fluid = false;
-                for (size_t nbi : nbrs) any_fluid = any_fluid || !solid[nbi];
+                for (int q = 0; q < (disc_ghost_rule ? 4 : 6); ++q) any_fluid = any_fluid || !solid[nbrs[q]];
                 if (!any_fluid) continue;
                 IbmGhost gh;
                 gh.idx = c;
                 mesh.cell_centroid(c, gh.cell_center);
                 double best_abs = std::numeric_limits<double>::max(), best_signed = 0.0;
-                double best_normal[3] = {1.0, 0.0, 0.0};
+                double best_normal[3] = {1.0, 0.0, 0.0}, best_wall[3] = {0.0, 0.0, 0.0};
                 uint32_t best_body = 0;
                 for (size_t bid = 0; bid < cyls.size(); ++bid) {
                     const double s = cyls[bid].signed_distance(gh.cell_center);
@@ -747,13 +750,18 @@ void Case::compute_cylinder_ghosts() {
                         best_signed = s;
                         cyls[bid].normal(gh.cell_center, best_normal);
                         best_body = (uint32_t)bid;
+                        // the wall velocity at the cell's wall footprint (compute_disc_ghosts,
+                        // examples/dkt_sedimentation/main.rs:175-249; zero for a body at rest)
+                        const double foot[3] = {gh.cell_center[0] - s * best_normal[0],
+                                                gh.cell_center[1] - s * best_normal[1], gh.cell_center[2]};
+                        cyls[bid].wall_velocity(foot, best_wall);
                     }
                 }
                 const double push = 2.0 * (-best_signed);
                 for (int d = 0; d < 3; ++d) {
                     gh.image_point[d] = gh.cell_center[d] + push * best_normal[d];
                     gh.normal[d] = best_normal[d];
-                    gh.wall_velocity[d] = 0.0;
+                    gh.wall_velocity[d] = best_wall[d];
                 }
                 gh.body_id = best_body;
                 ghosts.push_back(gh);
@@ -768,7 +776,7 @@ void Case::compute_cylinder_markers() {
     const double z_lo = mesh.centroid_axis(2, ng) - 0.5 * mesh.h[2];
     const double z_hi = mesh.centroid_axis(2, ng + nk - 1) + 0.5 * mesh.h[2];
     const double lz = z_hi - z_lo;
-    const int n_theta = 64, n_z = std::max(nk, 1);
+    const int n_theta = cylinder_markers_n, n_z = std::max(nk, 1);
     for (size_t bid = 0; bid < cyls.size(); ++bid) {
         const Cylinder& cy = cyls[bid];
         const double area = 2.0 * PI * cy.r * lz / (double)(n_theta * n_z);
@@ -784,7 +792,7 @@ void Case::compute_cylinder_markers() {
                 m.position[2] = z;
                 m.normal[0] = nx; m.normal[1] = ny; m.normal[2] = 0.0;
                 m.area = area;
-                m.wall_velocity[0] = m.wall_velocity[1] = m.wall_velocity[2] = 0.0;
+                cy.wall_velocity(m.position, m.wall_velocity);
                 markers.push_back(m);
             }
         }
@@ -1310,9 +1318,29 @@ int oracle_set_solver_state(void* hp, const efvm_solver_state* in) {
     return EFVM_OK;
 }
 
+int oracle_set_cylinders(void* hp, const efvm_cylinder* c, int32_t n, const double fs[5]);
+
+// The moving discs of examples/dkt_sedimentation/main.rs (n_theta markers per disc).
+int oracle_set_discs(void* hp, const efvm_disc* d, int32_t n, int32_t n_theta, const double fs[5]) {
+    std::vector<efvm_cylinder> c((size_t)n);
+    for (int i = 0; i < n; ++i) c[i] = efvm_cylinder{d[i].cx, d[i].cy, d[i].radius};
+    const int rc = oracle_set_cylinders(hp, c.data(), n, fs);
+    Case& cs = ((OracleHandle*)hp)->cs;
+    for (int i = 0; i < n; ++i) {
+        cs.cyls[i].vx = d[i].vx;
+        cs.cyls[i].vy = d[i].vy;
+        cs.cyls[i].omega = d[i].omega;
+    }
+    cs.cylinder_markers_n = n_theta;
+    cs.disc_ghost_rule = true;
+    return rc;
+}
+
 int oracle_set_cylinders(void* hp, const efvm_cylinder* c, int32_t n, const double fs[5]) {
     Case& cs = ((OracleHandle*)hp)->cs;
     cs.cyls.clear();
+    cs.cylinder_markers_n = 64;
+    cs.disc_ghost_rule = false;
     for (int i = 0; i < n; ++i) cs.cyls.push_back(Cylinder{c[i].cx, c[i].cy, c[i].radius});
     const ConsVar f(fs[0], fs[1], fs[2], fs[3], fs[4]);
     // CylinderIbmPlugin::build, crates/cfd_ibm/src/lib.rs:665-669

@@ -242,6 +242,14 @@ void Mesh::for_each_face(F&& f) const {
 // ---- IBM: crates/cfd_ibm/src/lib.rs ---------------------------------------
 struct Cylinder {
     double cx, cy, r;
+    double vx = 0.0, vy = 0.0, omega = 0.0;  // a moving disc (examples/dkt_sedimentation/main.rs:66-103)
+    // Disc::wall_velocity, :94-102: v + omega z x (p - c)
+    void wall_velocity(const double p[3], double out[3]) const {
+        const double rx = p[0] - cx, ry = p[1] - cy;
+        out[0] = vx - omega * ry;
+        out[1] = vy + omega * rx;
+        out[2] = 0.0;
+    }
     double signed_distance(const double p[3]) const {   // :70-74
         const double dx = p[0] - cx, dy = p[1] - cy;
         return std::sqrt(dx * dx + dy * dy) - r;
@@ -306,6 +314,8 @@ struct Case {
     std::vector<Cylinder> cyls;
     std::vector<Sphere> spheres;                 // SphereBodies (3-D)
     int sphere_markers_n = 2000;                 // SphereMarkerCfg
+    int cylinder_markers_n = 64;                 // n_theta of the cylinder / disc markers
+    bool disc_ghost_rule = false;                // compute_disc_ghosts: in-plane neighbours only
     ConsVar stagnant, ambient;                   // MaskConsts
     std::vector<IbmGhost> ghosts;
     std::vector<IbmMarker> markers;

@@ -60,6 +60,7 @@ def lib(parallel: bool = False) -> C.CDLL:
     L.oracle_set_solver_state.argtypes = [vp, C.POINTER(abi.EfvmSolverState)]
     L.oracle_set_cylinders.argtypes = [vp, C.POINTER(abi.EfvmCylinder), i32, dp]
     L.oracle_set_spheres.argtypes = [vp, C.POINTER(abi.EfvmSphere), i32, i32, dp]
+    L.oracle_set_discs.argtypes = [vp, C.POINTER(abi.EfvmDisc), i32, i32, dp]
     L.oracle_sphere_markers.argtypes = [C.POINTER(abi.EfvmSphere), i32, dp]
     L.oracle_marker_force.argtypes = [vp, dp]
     L.oracle_wall_force.argtypes = [vp, dp]
@@ -190,6 +191,13 @@ class OracleCase:
         ca = arr_t(*[abi.EfvmCylinder(*c) for c in cyls])
         fs = arr(freestream)
         self.L.oracle_set_cylinders(self.h, ca, len(cyls), _dp(fs))
+
+    def set_discs(self, discs, freestream, n_theta: int = 64) -> None:
+        """discs: abi.EfvmDisc values (moving 2-D bodies)."""
+        arr_t = abi.EfvmDisc * max(len(discs), 1)
+        da = arr_t(*discs)
+        fs = arr(freestream)
+        self.L.oracle_set_discs(self.h, da, len(discs), int(n_theta), _dp(fs))
 
     def set_spheres(self, spheres, freestream, n_markers: int = 2000) -> None:
         """spheres: abi.EfvmSphere values (abi.make_sphere)."""

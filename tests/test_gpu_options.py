@@ -86,3 +86,33 @@ def test_fp32_flux_on_the_viscous_channel():
     o.step(10)
     d.step(10)
     assert rel_err(d.download(), o.download()) < 2e-4
+
+
+@pytest.mark.parametrize("nz", [1, 4])
+def test_round_off_velocities_in_still_gas(nz):
+    """Still gas whose velocities are round-off sized (1e-157, squares below the
+    normal range): the low-Mach blend must stay finite and the state must match
+    the oracle (the flush-to-zero reciprocal square root once turned these into
+    NaN next to a resting immersed disc)."""
+    from oracle import pyoracle as po
+    from dev_field_efvm_b200.device import Context
+    rng = np.random.default_rng(11)
+    P = abi.BC_PERIODIC
+    grid = abi.make_grid(32, 24, hi=(1.0, 0.75, 0.125 if nz > 1 else 1.0 / 32),
+                         bcs={abi.XLO: P, abi.XHI: P, abi.YLO: P, abi.YHI: P,
+                              abi.ZLO: P if nz > 1 else abi.BC_SLIP_WALL, abi.ZHI: P if nz > 1 else abi.BC_SLIP_WALL},
+                         nz=nz)
+    params = abi.make_params(cfl=0.4, reconstruction=abi.RECON_MUSCL)
+    shape = (nz, 24, 32) if nz > 1 else (24, 32)
+    tiny = 1e-157 * rng.standard_normal((3,) + shape)
+    from dev_field_efvm_b200 import cases
+    u = cases.prim_to_cons3(np.ones(shape), tiny[0], tiny[1], tiny[2] if nz > 1 else 0.0, np.full(shape, 1.0e5))
+    o, d = po.OracleCase(grid, params), Context(grid, params)
+    o.upload(u)
+    d.upload(u)
+    o.step(4)
+    d.step(4)
+    got, want = d.download(), o.download()
+    assert np.isfinite(got).all()
+    assert np.max(np.abs(got[..., 0] - want[..., 0])) <= 1e-12
+    assert np.max(np.abs(got[..., 4] - want[..., 4])) <= 1e-12 * 2.5e5

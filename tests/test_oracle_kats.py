@@ -230,3 +230,24 @@ def test_sphere_wall_velocity_and_fibonacci_markers():
     assert np.all(np.abs(m[:, 0:3].mean(axis=0)) < 1e-2)
     # at least 12 markers whatever is asked (SphereMarkerCfg: n.max(12))
     assert po.sphere_markers(b, 3).shape[0] == 12
+
+
+# ---- examples/dkt_sedimentation/main.rs:289-402 (the driver's host arithmetic) ----
+def test_dkt_contact_and_rigid_body_update():
+    from dev_field_efvm_b200 import dkt
+    grid, params, u, discs, fsi, fs = dkt.setup()
+    # far apart and away from the walls: no contact force
+    assert dkt.contact_forces(discs, fsi) == [[0.0, 0.0], [0.0, 0.0]]
+    # inside the band: equal and opposite along the line of centres
+    a, b = discs
+    b.centre = [a.centre[0] + 2 * a.radius + 0.5 * fsi.contact_range, a.centre[1]]
+    f = dkt.contact_forces(discs, fsi)
+    assert f[0][0] < 0 < f[1][0] and f[0][0] == -f[1][0] and f[0][1] == f[1][1] == 0.0
+    assert abs(f[1][0] - fsi.k_n * 0.5 * fsi.contact_range) <= 1e-9 * abs(f[1][0])
+    # no fluid load and no contact: the buoyant weight accelerates at (1 - 1/s) g
+    grid, params, u, discs, fsi, fs = dkt.setup()
+    dt = 1e-5
+    dkt.fsi_update(discs, np.zeros((2, 9)), dt, fsi)
+    s = dkt.CONFIG["density_ratio"]
+    assert abs(discs[0].vel[1] + (1.0 - 1.0 / s) * fsi.g * dt) <= 1e-12 * fsi.g * dt
+    assert discs[0].vel[0] == 0.0 and discs[0].omega == 0.0
