@@ -71,7 +71,8 @@ def test_create_without_a_gpu_fails_loudly_or_rejects_bad_config(lib):
     p32 = abi.make_params(precision=abi.PREC_FP32_FLUX)
     assert lib.efvm_create(C.byref(g3), C.byref(p32), C.byref(h)) == abi.ERR_UNSUPPORTED
     assert b"FP64" in lib.efvm_last_error(None)
-    ps = abi.make_params(sponge=1, sponge_x_start=0.5, sponge_x_end=1.0)
-    assert lib.efvm_create(C.byref(g3), C.byref(ps), C.byref(h)) == abi.ERR_UNSUPPORTED
+    pi = abi.make_params(parabolic_inflow=1, inflow_u_max=1.0, inflow_height=1.0, inflow_rho=1.0)
+    assert lib.efvm_create(C.byref(g3), C.byref(pi), C.byref(h)) == abi.ERR_UNSUPPORTED
+    assert b"parabolic" in lib.efvm_last_error(None)
     g0 = abi.make_grid(8, 8, nz=0)
     assert lib.efvm_create(C.byref(g0), C.byref(abi.make_params()), C.byref(h)) == abi.ERR_INVALID_ARG
