@@ -271,7 +271,6 @@ int launch_init_vortex(const Geometry& g, const efvm_vortex& v, double* q, void*
 int launch_density_error(const Geometry& g, const efvm_vortex& v, const double* q, const DevState* st,
                           double* partial, int nblocks, void* stream);
 int launch_total_mass(const Geometry& g, const double* q, double* partial, int nblocks, void* stream);
-int launch_check_state(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream);
 // Rows j0, j0+1 (all four variables, interior columns) to buf (unpack = 0) or
 // from buf (unpack = 1); buf is [variable][row][i], 8*nx doubles.
 int launch_halo_rows(const Geometry& g, double* q, double* buf, int j0, int unpack, void* stream);

@@ -1061,20 +1061,6 @@ __global__ void total_mass_kernel(Geometry g, const double* __restrict__ q, doub
     if (threadIdx.x == 0) partial[blockIdx.x] = s1[0];
 }
 
-__global__ void check_state_kernel(Geometry g, Physics ph, const double* __restrict__ q, DevState* st) {
-    const long long n = (long long)g.nx * g.ny;
-    const double gm1 = ph.gamma - 1.0;
-    int bad = 0;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(k / g.nx), i = (int)(k - (long long)j * g.nx);
-        const U4 u = load4(q, g.plane, cidx(g, i, j));
-        if (!(u.r > 0.0)) bad |= 1;
-        if (!(pressure_d(u, gm1) > 0.0)) bad |= 2;
-        if (u.r != u.r || u.mx != u.mx || u.my != u.my || u.E != u.E) bad |= 4;
-    }
-    if (bad) atomicOr(&st->nonphysical, bad);
-}
-
 // ---------------------------------------------------------------------------
 // Host launch wrappers
 // ---------------------------------------------------------------------------
@@ -1436,10 +1422,6 @@ int launch_total_mass(const Geometry& g, const double* q, double* partial, int n
     return 1;
 }
 
-int launch_check_state(const Geometry& g, const Physics& ph, const double* q, DevState* st, void* stream) {
-    check_state_kernel<<<grid_for((long long)g.nx * g.ny, 256), 256, 0, (cudaStream_t)stream>>>(g, ph, q, st);
-    return 1;
-}
 
 int launch_pack3(const Geometry& g, double* host_like, int64_t si, int64_t sj, int64_t sk, int64_t sv, double* q,
                  int to_device, void* stream) {
