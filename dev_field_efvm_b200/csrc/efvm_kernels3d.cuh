@@ -179,10 +179,17 @@ constexpr int MINB3 = 4;  // resident blocks per SM of the 3-D stage kernel (128
 }  // namespace
 
 // ---------------------------------------------------------------------------
-// The 3-D stage kernel: one RK substage.  Warp w of block b works on the pair
-// (strip, layer) = ((b WPB + w) mod strips, (b WPB + w) div strips), so every
-// warp slot has work whatever the number of strips per layer; blockIdx.y is
-// the row block.
+// The 3-D stage kernel: one RK substage.  Block (b, by) covers strip b mod
+// strips and the WPB consecutive layers starting at WPB (b div strips); warp w
+// takes layer WPB (b div strips) + w, so the block's warps stack in z over the
+// same columns and rows.  Each warp forms the z face above its layer and hands
+// it to the warp above through shared memory; only warp 0 also forms the face
+// below its layer.  All z faces go through one non-unrolled loop body, so a
+// face formed at the top of one block and again at the bottom of the next is
+// bit-identical.  Every warp adds the face below and then the face above, in
+// the same order, so the step commutes with shifts in z.  A warp past the last
+// layer computes on the last layer (its loads stay in bounds) and stores
+// nothing; it only keeps the block's barriers.
 // ---------------------------------------------------------------------------
 template <int SCHEME, int RECON, bool VISC>
 __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, int rows) {
@@ -193,10 +200,14 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
     const long long P = g.plane;
     const int lane = threadIdx.x & 31;
     const int strips = (g.nx + STRIP - 1) / STRIP;
-    const int wid = blockIdx.x * WPB + (threadIdx.x >> 5);
-    const int k = wid / strips, strip = wid - k * strips;
+    const int warp = threadIdx.x >> 5;
+    const int kgroup = blockIdx.x / strips, strip = blockIdx.x - kgroup * strips;
+    const int k_raw = kgroup * WPB + warp;
+    const bool act = k_raw < g.nz;       // warp-uniform
+    const int k = act ? k_raw : g.nz - 1;
     const int by = blockIdx.y;
-    if (strip == 0 && by == 0 && k == 0 && lane == 0) {
+    __shared__ double zup[WPB][5][32];   // the face above each warp's layer, per lane
+    if (strip == 0 && by == 0 && k_raw == 0 && lane == 0) {
         // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
         DevState* st = a.st;
         if (a.stage >= 2) {
@@ -212,7 +223,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
     const int i0 = strip * STRIP;
     const int jb = by * rows;
     double lam = 0.0;
-    if (k < g.nz && jb < g.ny) {  // uniform across the warp
+    if (jb < g.ny) {  // uniform across the block (its barriers sit inside)
         constexpr bool MUSCL = RECON == EFVM_RECON_MUSCL;
         const int je = min(jb + rows, g.ny);
         const int i = i0 + lane;
@@ -299,11 +310,13 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                     acc[v] = __dsub_rn(t, __dmul_rn(fr[v], g.inv_x));
                 }
 
-                // ---- the two z faces of the cell through one code path: face s
-                // lies between layers k - 1 + s and k + s; its four cells are
-                // loaded here, so no z stencil stays live across the loop ----
+                // ---- the z faces of the cell through one code path: face s lies
+                // between layers k - 1 + s and k + s; its four cells are loaded
+                // here.  Warp 0 forms both, the others only the face above and
+                // take the one below from the warp under them. ----
+                V5 fzb, fza;
 #pragma unroll 1
-                for (int s = 0; s < 2; ++s) {
+                for (int s = warp == 0 ? 0 : 1; s < 2; ++s) {
                     const V5 A = ldz(j, s - 1), B = ldz(j, s);
                     V5 L = A, Rv = B;
                     if (MUSCL) {
@@ -318,10 +331,25 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                         }
                     }
                     const V5 f = zg5(face_flux5<SCHEME, double>(zq5(L), zq5(Rv), rg, gm1));
-                    const double fv[5] = {f.r, f.mx, f.my, f.mz, f.E};
-                    const double w = s ? -g.inv_z : g.inv_z;  // in through the face below, out through the one above
+                    if (s) fza = f;
+                    else fzb = f;
+                }
+                zup[warp][0][lane] = fza.r;
+                zup[warp][1][lane] = fza.mx;
+                zup[warp][2][lane] = fza.my;
+                zup[warp][3][lane] = fza.mz;
+                zup[warp][4][lane] = fza.E;
+                __syncthreads();
+                if (warp > 0)
+                    fzb = V5{zup[warp - 1][0][lane], zup[warp - 1][1][lane], zup[warp - 1][2][lane],
+                             zup[warp - 1][3][lane], zup[warp - 1][4][lane]};
+                __syncthreads();  // zup is rewritten on the next row
+                const double zb[5] = {fzb.r, fzb.mx, fzb.my, fzb.mz, fzb.E};
+                const double za[5] = {fza.r, fza.mx, fza.my, fza.mz, fza.E};
 #pragma unroll
-                    for (int v = 0; v < 5; ++v) acc[v] = __dadd_rn(acc[v], __dmul_rn(fv[v], w));
+                for (int v = 0; v < 5; ++v) {  // in through the face below, out through the one above
+                    acc[v] = __dadd_rn(acc[v], __dmul_rn(zb[v], g.inv_z));
+                    acc[v] = __dsub_rn(acc[v], __dmul_rn(za[v], g.inv_z));
                 }
             }
 
@@ -343,7 +371,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
             }
             const V5 gt = yg5(face_flux5<SCHEME, double>(yb_, yt_, rg, gm1));
 
-            if (row && owner) {
+            if (row && owner && act) {
                 const long long o = cidx3(g, i, j, k);
                 const U5 ucd = toU5(uc);
                 const double yt[5] = {gt.r, gt.mx, gt.my, gt.mz, gt.E};
@@ -728,8 +756,8 @@ static int rows_per_warp3(int nx, int ny, int nz) {
 template <int SCHEME, int RECON, bool VISC>
 static void launch_stage3_t(const StageArgs& a, bool pdl, cudaStream_t s) {
     const int rows = rows_per_warp3(a.g.nx, a.g.ny, a.g.nz);
-    const long long pairs = (long long)((a.g.nx + STRIP - 1) / STRIP) * a.g.nz;
-    dim3 grid((unsigned)((pairs + WPB - 1) / WPB), (a.g.ny + rows - 1) / rows);
+    const long long blocks = (long long)((a.g.nx + STRIP - 1) / STRIP) * ((a.g.nz + WPB - 1) / WPB);
+    dim3 grid((unsigned)blocks, (a.g.ny + rows - 1) / rows);
     launch_k(stage3_kernel<SCHEME, RECON, VISC>, grid, dim3(32 * WPB), s, pdl, a, rows);
 }
 
