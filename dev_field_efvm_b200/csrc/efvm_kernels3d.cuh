@@ -10,11 +10,12 @@
 //
 // The stage kernel keeps the 2-D kernel's organisation: a warp owns a strip of
 // 31 columns of one layer k and marches `rows` rows with the carried y window,
-// the x faces come from warp shuffles, and each lane also forms the two z
-// faces of its cell from the layers k-2..k+2 of its column.  A z face between
-// layers k and k+1 is formed by the warps of both layers; both go through the
-// same (non-unrolled) loop body, so the two results agree bit for bit and the
-// scheme stays conservative across layers.
+// and the x faces come from warp shuffles.  The warps of a block stack in z
+// over the same strip and rows and share the z direction through shared
+// memory: each limits the z slope of its own cell once and forms the z face
+// above its layer once.  A z face on the edge of two blocks is formed by both
+// through the same (non-unrolled) loop bodies, so the two results agree bit
+// for bit and the scheme stays conservative across layers.
 
 namespace {
 
@@ -174,25 +175,29 @@ __device__ __forceinline__ void prim5(const U5& u, double inv, double gm1, doubl
     t = gm1 * (u.E - ke) * inv / r_gas;
 }
 
+constexpr int WPB3 = 4;   // warps per block of the 3-D stage kernel, stacked in z
 constexpr int MINB3 = 4;  // resident blocks per SM of the 3-D stage kernel (128 registers)
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
 // The 3-D stage kernel: one RK substage.  Block (b, by) covers strip b mod
-// strips and the WPB consecutive layers starting at WPB (b div strips); warp w
-// takes layer WPB (b div strips) + w, so the block's warps stack in z over the
-// same columns and rows.  Each warp forms the z face above its layer and hands
-// it to the warp above through shared memory; only warp 0 also forms the face
-// below its layer.  All z faces go through one non-unrolled loop body, so a
-// face formed at the top of one block and again at the bottom of the next is
-// bit-identical.  Every warp adds the face below and then the face above, in
-// the same order, so the step commutes with shifts in z.  A warp past the last
-// layer computes on the last layer (its loads stay in bounds) and stores
-// nothing; it only keeps the block's barriers.
+// strips and the WPB3 consecutive layers starting at WPB3 (b div strips); warp
+// w takes layer WPB3 (b div strips) + w, so the block's warps stack in z over
+// the same columns and rows.  Per row, each warp limits the z slope of its own
+// cell (warp 0 also that of the cell below, the top warp that of the cell
+// above), hands the right state of the face below its cell to the warp under
+// it, forms the z face above its layer and hands that flux to the warp above;
+// only warp 0 also forms the face below its layer.  Slopes and faces each go
+// through one non-unrolled loop body, so a face formed at the top of one block
+// and again at the bottom of the next is bit-identical.  Every warp adds the
+// face below and then the face above, in the same order, so the step commutes
+// with shifts in z.  A warp past the last layer computes on the last layer
+// (its loads stay in bounds) and stores nothing; it only keeps the block's
+// barriers.
 // ---------------------------------------------------------------------------
 template <int SCHEME, int RECON, bool VISC>
-__global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, int rows) {
+__global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, int rows) {
     pdl_wait_then_release();
     if (!a.st->active) return;
     const Geometry& g = a.g;
@@ -202,11 +207,13 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
     const int strips = (g.nx + STRIP - 1) / STRIP;
     const int warp = threadIdx.x >> 5;
     const int kgroup = blockIdx.x / strips, strip = blockIdx.x - kgroup * strips;
-    const int k_raw = kgroup * WPB + warp;
+    const int k_raw = kgroup * WPB3 + warp;
     const bool act = k_raw < g.nz;       // warp-uniform
     const int k = act ? k_raw : g.nz - 1;
     const int by = blockIdx.y;
-    __shared__ double zup[WPB][5][32];   // the face above each warp's layer, per lane
+    __shared__ double zup[WPB3][5][32];     // the flux of the face above each warp's layer, per lane
+    // z face states of the block's column, face f lying below layer WPB3 (b div strips) + f
+    __shared__ double zst[2][WPB3 + 1][5][32];  // [left/right state][face][variable][lane]
     if (strip == 0 && by == 0 && k_raw == 0 && lane == 0) {
         // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
         DevState* st = a.st;
@@ -310,26 +317,53 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                     acc[v] = __dsub_rn(t, __dmul_rn(fr[v], g.inv_x));
                 }
 
-                // ---- the z faces of the cell through one code path: face s lies
-                // between layers k - 1 + s and k + s; its four cells are loaded
-                // here.  Warp 0 forms both, the others only the face above and
-                // take the one below from the warp under them. ----
+                // ---- z faces.  One non-unrolled loop marches the column up through
+                // the cells whose z slope this warp limits: its own, and for warp 0
+                // the one below, for the top warp (the last of the block, or of the
+                // mesh) the one above; so every slope comes from one code path.  Each
+                // slope gives the right state of the face below its cell and the left
+                // state of the face above; they meet in shared memory, every face
+                // state with one writer.  A second non-unrolled loop forms the face
+                // above the warp's layer (warp 0 also the one below), whose flux goes
+                // to the warp above.  A face on the edge of two blocks is formed from
+                // the same states through the same code by both. ----
+                const bool top = warp == WPB3 - 1 || k_raw + 1 >= g.nz;
+                const int lo = warp == 0 ? -1 : 0, hi = top ? 1 : 0;
+                auto put = [&](int side, int f, const V5& q) {
+                    zst[side][f][0][lane] = q.r;
+                    zst[side][f][1][lane] = q.mx;
+                    zst[side][f][2][lane] = q.my;
+                    zst[side][f][3][lane] = q.mz;
+                    zst[side][f][4][lane] = q.E;
+                };
+                auto get = [&](int side, int f) {
+                    return V5{zst[side][f][0][lane], zst[side][f][1][lane], zst[side][f][2][lane],
+                              zst[side][f][3][lane], zst[side][f][4][lane]};
+                };
+                {
+                    V5 m = ldz(j, lo - 1), c = ldz(j, lo);
+#pragma unroll 1
+                    for (int dk = lo; dk <= hi; ++dk) {
+                        const V5 p = ldz(j, dk + 1);
+                        V5 pl = c, mi = c;
+                        if (MUSCL) {
+                            V5 sp, sm;
+                            slope_faces5(ph.limiter, m, c, p, sp, sm);
+                            if (dk < 0 ? zrA[0] : zrA[1]) pl = sp;
+                            if (dk > 0 ? zrB[1] : zrB[0]) mi = sm;
+                        }
+                        // a warp past the last layer writes nothing: its faces belong to the top warp
+                        if (act && dk < 1) put(0, warp + dk + 1, pl);  // left state of the face above cell k + dk
+                        if (act && dk > -1) put(1, warp + dk, mi);     // right state of the face below it
+                        m = c;
+                        c = p;
+                    }
+                }
+                __syncthreads();
                 V5 fzb, fza;
 #pragma unroll 1
                 for (int s = warp == 0 ? 0 : 1; s < 2; ++s) {
-                    const V5 A = ldz(j, s - 1), B = ldz(j, s);
-                    V5 L = A, Rv = B;
-                    if (MUSCL) {
-                        V5 pl, mi;
-                        if (s ? zrA[1] : zrA[0]) {
-                            slope_faces5(ph.limiter, ldz(j, s - 2), A, B, pl, mi);
-                            L = pl;
-                        }
-                        if (s ? zrB[1] : zrB[0]) {
-                            slope_faces5(ph.limiter, A, B, ldz(j, s + 1), pl, mi);
-                            Rv = mi;
-                        }
-                    }
+                    const V5 L = get(0, warp + s), Rv = get(1, warp + s);
                     const V5 f = zg5(face_flux5<SCHEME, double>(zq5(L), zq5(Rv), rg, gm1));
                     if (s) fza = f;
                     else fzb = f;
@@ -339,11 +373,10 @@ __global__ void __launch_bounds__(32 * WPB, MINB3) stage3_kernel(StageArgs a, in
                 zup[warp][2][lane] = fza.my;
                 zup[warp][3][lane] = fza.mz;
                 zup[warp][4][lane] = fza.E;
-                __syncthreads();
+                __syncthreads();  // zst is rewritten on the next row only after this barrier
                 if (warp > 0)
                     fzb = V5{zup[warp - 1][0][lane], zup[warp - 1][1][lane], zup[warp - 1][2][lane],
                              zup[warp - 1][3][lane], zup[warp - 1][4][lane]};
-                __syncthreads();  // zup is rewritten on the next row
                 const double zb[5] = {fzb.r, fzb.mx, fzb.my, fzb.mz, fzb.E};
                 const double za[5] = {fza.r, fza.mx, fza.my, fza.mz, fza.E};
 #pragma unroll
@@ -746,7 +779,7 @@ __global__ void __launch_bounds__(FORCE3_THREADS) forces3_kernel(Geometry g, Phy
 // against 6.65 at 8 rows; 3 and 5 blocks 15 % and 10 % slower).
 static int rows_per_warp3(int nx, int ny, int nz) {
     const long long strips = (nx + STRIP - 1) / STRIP;
-    const long long slots = 148LL * MINB3 * WPB;
+    const long long slots = 148LL * MINB3 * WPB3;
     long long rows = (strips * ny * nz + slots - 1) / slots;
     if (rows < 2) rows = 2;
     if (rows > 12) rows = 12;
@@ -756,9 +789,9 @@ static int rows_per_warp3(int nx, int ny, int nz) {
 template <int SCHEME, int RECON, bool VISC>
 static void launch_stage3_t(const StageArgs& a, bool pdl, cudaStream_t s) {
     const int rows = rows_per_warp3(a.g.nx, a.g.ny, a.g.nz);
-    const long long blocks = (long long)((a.g.nx + STRIP - 1) / STRIP) * ((a.g.nz + WPB - 1) / WPB);
+    const long long blocks = (long long)((a.g.nx + STRIP - 1) / STRIP) * ((a.g.nz + WPB3 - 1) / WPB3);
     dim3 grid((unsigned)blocks, (a.g.ny + rows - 1) / rows);
-    launch_k(stage3_kernel<SCHEME, RECON, VISC>, grid, dim3(32 * WPB), s, pdl, a, rows);
+    launch_k(stage3_kernel<SCHEME, RECON, VISC>, grid, dim3(32 * WPB3), s, pdl, a, rows);
 }
 
 template <bool VISC>
