@@ -15,7 +15,9 @@ every step uploads the state from pinned host memory, steps, downloads it and
 reads the marker force, in three host threads with one context each so that one
 thread's copies overlap the other's kernels.  `roofline` relates the stage kernel's algorithmic
 bytes (the RK3 traffic of a cell-update, 256 B, plus the 1 B solid mask per
-stage) to its live CUDA-event duration and the measured HBM copy bandwidth.
+stage) to its live CUDA-event duration and the measured HBM copy bandwidth;
+`fp64` relates the same kernel's FP64 flops (counted by ncu, stored beside the
+traffic figures) to the FP64 peak, the bound this stencil actually meets.
 `cpu_baseline` times the CPU oracle (the reference's algorithm restated in
 C++, OpenMP over the host cores) on a bounded sample of the same workload.
 
@@ -76,6 +78,32 @@ def measured_peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def fp64_peaks():
+    """FP64 peaks of this GPU in TFLOP/s: measured (a cuBLAS FP64 GEMM, 8192^3,
+    2 N^3 flops, best of 5 after 2 warm-ups, CUDA events) and the issue peak at
+    the maximum SM clock (64 FP64 FMA lanes per SM x 148 SMs x 2 flops)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    mhz = 1965.0
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        mhz = float(json.load(open(p)).get("sm_max_mhz", mhz))
+    return 2.0 * n ** 3 / best / 1e12, 64 * 148 * 2 * mhz * 1e6 / 1e12
 
 
 class ClockSampler:
@@ -415,6 +443,7 @@ def main():
     achieved = bytes_per_launch / (stage_ms_per_launch * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = None
+    entry = None
     tf = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
     if os.path.exists(tf):
         entry = json.load(open(tf)).get(args.workload) if args.size is None else None
@@ -429,6 +458,18 @@ def main():
                 # (the per-kernel events of the profile pass wait on the host between
                 # stages, so its own whole-step time is not a step of the timed loop)
                 "share_of_step": 3 * stage_ms_per_launch / (ms / args.steps)}
+    # The same kernel against the FP64 peak: its FP64 flops per cell-update
+    # (dadd + dmul + 2 dfma thread instructions of one step's three launches,
+    # counted by ncu, per cell) over the same live launch time.
+    fp64 = None
+    if entry and entry.get("fp64_flops_per_cell_update"):
+        fpc = float(entry["fp64_flops_per_cell_update"])
+        dgemm, issue = fp64_peaks()
+        got = fpc * cells / 3.0 / (stage_ms_per_launch * 1e-3) / 1e12
+        fp64 = {"flops_per_cell_update": fpc, "achieved": got, "peak": dgemm, "unit": "TFLOP/s", "frac": got / dgemm,
+                "peak_source": "measured: cuBLAS FP64 GEMM 8192^3, best of 5", "issue_peak": issue,
+                "issue_frac": got / issue, "issue_peak_source": "64 FP64 FMA lanes/SM x 148 SMs x 2 x max SM clock",
+                "counted": entry.get("fp64_how", "")}
 
     # ---- chosen form: FP32 reconstruction/fluxes, FP64 accumulation -------
     if d3:  # 3-D meshes run in FP64 only
@@ -504,6 +545,7 @@ def main():
                            l2="flushed between timed steps (256 MB write)",
                            time=st.time, final_step=int(st.step)),
             "roofline": roofline,
+            "fp64": fp64,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
                     "d2h_bytes_per_step": cells * 5 * 8 + (C.sizeof(abi.EfvmSolverState) if d3 else 48),
