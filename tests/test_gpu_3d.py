@@ -121,8 +121,9 @@ def test_mass_conservation_true_periodic():
 
 def test_translation_invariance_true_periodic():
     """The step commutes with a shift by whole cells in x, y and z, bit for bit:
-    a z face is formed by the warps of both its layers through one code path, and
-    a y face on the edge of two warps' rows likewise."""
+    a z face on the edge of two blocks' layers is formed by both blocks from
+    slopes and states that went through one code path, and a y face on the edge
+    of two warps' rows likewise."""
     grid, params, u, _ = cases.vortex_tube_case(96, 40, seam=abi.SEAM_TRUE_PERIODIC)
     params.fixed_dt = 2.0e-3
     shift = (7, 13, 29)  # z, y, x
