@@ -89,6 +89,25 @@ def test_channel_walls_inflow_outlet_viscous(flux, muscl):
     assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
 
 
+@pytest.mark.parametrize("nz", [2, 3, 5])
+def test_thin_meshes_with_fewer_layers_than_a_block(nz):
+    """Meshes whose last (or only) block of stacked layers is partly empty: the
+    warps past the last layer keep the block's barriers and write nothing.
+    Periodic in z (the wrap then reaches across the whole mesh) and walled."""
+    grid, params, u, _ = cases.vortex_tube_case(24, nz, seam=abi.SEAM_TRUE_PERIODIC)
+    o, d = pair3(grid, params, u)
+    o.step(4)
+    d.step(4)
+    assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
+    bcs = {abi.XLO: abi.BC_PERIODIC, abi.XHI: abi.BC_PERIODIC, abi.YLO: abi.BC_PERIODIC,
+           abi.YHI: abi.BC_PERIODIC, abi.ZLO: abi.BC_NO_SLIP_WALL, abi.ZHI: abi.BC_SLIP_WALL}
+    grid = abi.make_grid(24, 24, lo=(0.0, 0.0, 0.0), hi=(10.0, 10.0, 10.0 * nz / 24), bcs=bcs, nz=nz)
+    o, d = pair3(grid, params, u)
+    o.step(4)
+    d.step(4)
+    assert rel_err3(d.download(), o.download()) < TOL_MANY_STEPS
+
+
 def test_channel_inviscid_euler_integrator_and_mc_limiter():
     grid, params, u = channel3(True, viscous=False, integrator=abi.INTEGRATOR_EULER)
     params.limiter = abi.LIMITER_MC

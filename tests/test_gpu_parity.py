@@ -112,6 +112,36 @@ def test_reference_vortex_gate_reproduces_published_l1_on_gpu():
         assert info.steps_done == oi.steps_done
 
 
+def test_vortex_muscl_mc_second_order_gate_on_gpu():
+    """The reference's MUSCL convergence gate (isentropic vortex, outflow, MC
+    limiter, N = 40/80/160 to t = 1; crates/cfd_solver/tests/
+    isentropic_vortex_muscl_convergence.rs:146-192) on the CUDA path: errors fall,
+    the fitted and finest-pair orders reach 1.8, the finest L1 stays under its
+    bound, and the two coarser errors agree with the oracle's."""
+    g = GOLD["vortex_muscl_mc_gate"]
+    errs = []
+    for n in g["n"]:
+        grid, params, u, ex = cases.vortex_case(n, periodic=False, muscl=True, limiter=abi.LIMITER_MC)
+        d = Context(grid, params)
+        d.upload(u)
+        info = d.run_until(1.0)
+        assert np.all(d.download()[..., 0] > 0)
+        errs.append(d.density_error(ex["vortex"])[0])
+        if n <= 80:
+            o = po.OracleCase(grid, params)
+            o.upload(u)
+            oi = o.run_until(1.0)
+            assert info.steps_done == oi.steps_done
+            assert abs(errs[-1] - o.density_error(ex["vortex"])[0]) <= 1e-9 * errs[-1]
+    x, y = np.log(np.array(g["n"], float)), np.log(np.array(errs))
+    m = len(x)
+    fitted = -(m * np.sum(x * y) - x.sum() * y.sum()) / (m * np.sum(x * x) - x.sum() ** 2)
+    assert all(errs[k + 1] < errs[k] for k in range(len(errs) - 1))
+    assert fitted >= g["min_fitted_order"]
+    assert math.log2(errs[-2] / errs[-1]) >= g["min_finest_pair_order"]
+    assert errs[-1] < g["max_finest_l1"]
+
+
 def test_sod_and_periodic_pulse_reproduce_published_numbers_on_gpu():
     gs = GOLD["sod_first_order_l1"]
     grid, params, u, ex = cases.sod_case(100)
