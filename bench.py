@@ -12,12 +12,14 @@ is cell-updates/s (interior cells advanced by one full RK3 step per second).
 `value` is device time with the state resident in HBM and L2 flushed between
 timed steps; `e2e` is the same metric through the C-ABI with host buffers:
 every step uploads the state from pinned host memory, steps, downloads it and
-reads the marker force, in three host threads with one context each so that one
-thread's copies overlap the other's kernels.  `roofline` relates the stage kernel's algorithmic
+reads the marker force, in several host threads with one context each so that
+one thread's copies overlap the others' kernels (the step is enqueued without a
+status read; the download waits for it).  `roofline` relates the stage kernel's algorithmic
 bytes (the RK3 traffic of a cell-update, 256 B, plus the 1 B solid mask per
 stage) to its live CUDA-event duration and the measured HBM copy bandwidth;
 `fp64` relates the same kernel's FP64 flops (counted by ncu, stored beside the
-traffic figures) to the FP64 peak, the bound this stencil actually meets.
+traffic figures) to a measured FP64 GEMM.  The kernel reaches neither peak: it
+is bound by instruction issue and FP64 dependency latency.
 `cpu_baseline` times the CPU oracle (the reference's algorithm restated in
 C++, OpenMP over the host cores) on a bounded sample of the same workload.
 
@@ -43,7 +45,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Cell-updates/s on 1 B200: plain FP64 vs chosen form at equal L1 density error"
-E2E_STREAMS = 3  # host threads (one context each) in the end-to-end leg (1, 2, 3, 4 measured: 3 is fastest)
+# Host threads (one context each) in the end-to-end leg.  Measured on the
+# cylinder (1100x205, 9 MB each way per step): 3 threads 8.7e8, 4 threads
+# 1.05e9, 6 threads 1.10e9 cell-updates/s; the large meshes are bound by the
+# host link whatever the count, so they keep 3 and their pinned buffers small.
+E2E_THREADS_SMALL, E2E_THREADS_LARGE = 6, 3
 UNIT = "cell-updates/s"
 
 
@@ -478,10 +484,11 @@ def main():
         value32, ms32 = fp32_leg(args, grid, params, u, ex, flush, world, cells)
 
     # ---- end to end through the C-ABI with pinned host buffers -----------
-    # E2E_STREAMS host threads, each with its own context and pinned buffer,
+    # n_threads host threads, each with its own context and pinned buffer,
     # run upload -> step -> download -> result read in a loop; the threads'
     # copies and kernels overlap on the GPU (ctypes releases the GIL in calls).
-    e2e_ctx = [ctx] + [Context(grid, params) for _ in range(E2E_STREAMS - 1)]
+    n_threads = E2E_THREADS_SMALL if cells < 2_000_000 else E2E_THREADS_LARGE
+    e2e_ctx = [ctx] + [Context(grid, params) for _ in range(n_threads - 1)]
     hosts = []
     shape = (grid.nz, grid.ny, grid.nx, 5) if d3 else (grid.ny, grid.nx, 5)
     for c in e2e_ctx:
@@ -498,12 +505,12 @@ def main():
         for _ in range(n):
             if d3:
                 c.upload_ptr3(ptr, 5, 5 * grid.nx, sk, 1)
-                c.step(1)
+                c.step_async(1)  # efvm_step without a status read; the download waits for it
                 c.download_ptr3(ptr, 5, 5 * grid.nx, sk, 1)
                 c.solver_state()  # the step's clock (dt, time, step): 48 B
             else:
                 c.upload_ptr(ptr, 5, 5 * grid.nx, 1)
-                c.step(1)
+                c.step_async(1)
                 c.download_ptr(ptr, 5, 5 * grid.nx, 1)
                 c.marker_force()
 
@@ -549,7 +556,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
                     "d2h_bytes_per_step": cells * 5 * 8 + (C.sizeof(abi.EfvmSolverState) if d3 else 48),
-                    "steps": n_e2e, "host_threads": E2E_STREAMS,
+                    "steps": n_e2e, "host_threads": n_threads,
                     "note": "each thread: its own context; per step upload from pinned memory, one RK3 step, "
                             "download, " + ("solver-state read" if d3 else "marker-force read")},
             "gpu_launches": int(launches),
