@@ -448,17 +448,19 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 const bool ibm = a.mask != nullptr;
                 const bool solid = ibm && a.mask[o];
                 if (VISC && !solid) {
-                    // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D)
-                    double nu[4], nv[4], nt[4];  // +x, -x, +y, -y
-                    const U4 nbs[4] = {ld(i + 1, j), ld(i - 1, j), FP64 ? toU4(un) : ld(i, j + 1), ld(i, j - 1)};
+                    // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D).
+                    // Neighbours +x, -x, +y, -y; a solid one takes (0, 0, T of the cell).  The
+                    // densities come first: the five reciprocals from one reciprocal of their
+                    // product (running products forward, then peeled off backward).  The other
+                    // components are loaded one axis pair at a time, which keeps the live
+                    // state small.
                     const long long no[4] = {o + 1, o - 1, o + g.pitch, o - g.pitch};
-                    bool sn[4];  // solid neighbours take (0, 0, T of the cell)
+                    bool sn[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) sn[k] = ibm && a.mask[no[k]];
-                    // the five reciprocal densities from one reciprocal of their
-                    // product (running products forward, then peeled off backward)
-                    const double r0 = ucd.r, r1 = sn[0] ? 1.0 : nbs[0].r, r2 = sn[1] ? 1.0 : nbs[1].r;
-                    const double r3 = sn[2] ? 1.0 : nbs[2].r, r4 = sn[3] ? 1.0 : nbs[3].r;
+                    const double r0 = ucd.r, r1 = sn[0] ? 1.0 : uin[no[0]], r2 = sn[1] ? 1.0 : uin[no[1]];
+                    const double r3 = sn[2] ? 1.0 : (FP64 ? (double)un.r : uin[no[2]]);
+                    const double r4 = sn[3] ? 1.0 : uin[no[3]];
                     const double p1 = r0 * r1, p2 = p1 * r2, p3 = p2 * r3;
                     double w = rcp_(p3 * r4);
                     const double i4 = p3 * w;
@@ -468,29 +470,54 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     const double i2 = p1 * w;
                     w = w * r2;
                     const double ninv[4] = {r0 * w, i2, i3, i4};
+                    const double rn[4] = {r1, r2, r3, r4};
                     const double i0 = r1 * w;
                     double us, vs, ts;
                     prim_uvt(ucd, i0, gm1, ph.r_gas, us, vs, ts);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
+                    auto nb = [&](int k, double& vu, double& vv, double& t) {
                         if (sn[k]) {
-                            nu[k] = 0.0; nv[k] = 0.0; nt[k] = ts;
-                        } else {
-                            prim_uvt(nbs[k], ninv[k], gm1, ph.r_gas, nu[k], nv[k], nt[k]);
+                            vu = 0.0; vv = 0.0; t = ts;
+                            return;
                         }
-                    }
+                        U4 q;
+                        if (FP64 && k == 2) {
+                            q = toU4(un);
+                        } else {
+                            q.r = rn[k];
+                            q.mx = uin[P + no[k]];
+                            q.my = uin[2 * P + no[k]];
+                            q.E = uin[3 * P + no[k]];
+                        }
+                        prim_uvt(q, ninv[k], gm1, ph.r_gas, vu, vv, t);
+                    };
                     const double y_im = a.yw[j], y_ip = a.yw[g.ny + j], y_is = a.yw[2 * g.ny + j];
                     const double dxi2 = ph.dx_inv2;
                     auto d2x = [&](double m, double p, double c) { return (p - 2.0 * c + m) * dxi2; };
                     auto d2y = [&](double m, double p, double c) { return ((p - c) * y_ip - (c - m) * y_im) * y_is; };
+                    double lu, lv, lt;  // d2x + d2y of u, v, T
+                    {
+                        double pu, pv, pt, mu_, mv, mt;
+                        nb(0, pu, pv, pt);
+                        nb(1, mu_, mv, mt);
+                        lu = d2x(mu_, pu, us);
+                        lv = d2x(mv, pv, vs);
+                        lt = d2x(mt, pt, ts);
+                    }
+                    {
+                        double pu, pv, pt, mu_, mv, mt;
+                        nb(2, pu, pv, pt);
+                        nb(3, mu_, mv, mt);
+                        lu = lu + d2y(mu_, pu, us);
+                        lv = lv + d2y(mv, pv, vs);
+                        lt = lt + d2y(mt, pt, ts);
+                    }
                     const double mu = viscosity(ph, ts);
                     const double kappa = mu * ph.cp / 0.72;  // thermal_conductivity, crates/cfd_eos/src/lib.rs:83-87
-                    const double fxv = mu * (d2x(nu[1], nu[0], us) + d2y(nu[3], nu[2], us));
-                    const double fyv = mu * (d2x(nv[1], nv[0], vs) + d2y(nv[3], nv[2], vs));
-                    const double d2t = d2x(nt[1], nt[0], ts) + d2y(nt[3], nt[2], ts);
+                    const double fxv = mu * lu;
+                    const double fyv = mu * lv;
                     rhs[1] += fxv;
                     rhs[2] += fyv;
-                    rhs[3] += us * fxv + vs * fyv + kappa * d2t;
+                    rhs[3] += us * fxv + vs * fyv + kappa * lt;
                 }
                 if (solid) rhs[0] = rhs[1] = rhs[2] = rhs[3] = 0.0;  // zero_solid_rhs, crates/cfd_ibm/src/lib.rs:293-301
                 if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
