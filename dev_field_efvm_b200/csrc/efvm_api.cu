@@ -667,6 +667,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     g.inv_x = (g.h[1] * g.h[2]) / g.cell_volume;
     g.inv_y = (g.h[0] * g.h[2]) / g.cell_volume;
     g.inv_z = (g.h[0] * g.h[1]) / g.cell_volume;
+    for (int a = 0; a < 3; ++a) g.inv_h[a] = 1.0 / g.h[a];
     ph.gamma = p.gamma;
     ph.r_gas = p.r_gas;
     ph.cfl = p.cfl;
@@ -717,6 +718,23 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     ph.dx_inv2 = 1.0 / (g.h[0] * g.h[0]);
     ph.cp = p.gamma * p.r_gas / (p.gamma - 1.0);
     ph.cfl_visc_sum = 1.0 / (g.h[0] * g.h[0]) + 1.0 / (g.h[1] * g.h[1]) + 1.0 / (g.h[2] * g.h[2]);
+    ph.inv_r_gas = 1.0 / p.r_gas;
+    // the sponge's constants with the operations the device would apply (this file
+    // is compiled without floating-point contraction): inv_w as in the 2-D and 3-D
+    // sponges, p / (gamma - 1) as in prim_to_cons, and the 3-D uniform target
+    // (rho, rho u_max, 0, 0, E) as prim_to_cons5 forms it
+    const double gm1 = p.gamma - 1.0;
+    ph.sponge_inv_w = 1.0 / (p.sponge_x_end - p.sponge_x_start);
+    ph.sponge_e0 = p.sponge_p / gm1;
+    {
+        const double rho = p.sponge_rho, u = p.sponge_u_max, v = 0.0, w = 0.0;
+        const double ke = (0.5 * rho) * ((u * u + v * v) + w * w);
+        ph.sponge_t[0] = rho;
+        ph.sponge_t[1] = rho * u;
+        ph.sponge_t[2] = rho * v;
+        ph.sponge_t[3] = rho * w;
+        ph.sponge_t[4] = p.sponge_p / gm1 + ke;
+    }
     return EFVM_OK;
 }
 

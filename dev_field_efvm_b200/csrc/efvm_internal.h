@@ -67,6 +67,7 @@ struct Geometry {
     double cell_volume;
     int j_off;            // global index of row 0 (slabs; 0 otherwise)
     int pad_;
+    double inv_h[3];      // 1 / dx, 1 / dy, 1 / dz (the CFL wave speed)
 };
 
 struct Physics {
@@ -90,6 +91,11 @@ struct Physics {
     double dx_inv2;       // 1/(dx*dx), viscous x weight
     double cp;            // gamma*R/(gamma-1), for kappa = mu*cp/0.72
     double cfl_visc_sum;  // 1/dx^2 + 1/dy^2 + 1/dz^2
+    double inv_r_gas;     // 1 / R (the CFL wave speed's temperature)
+    // Sponge constants, formed once on the host with the device's operations:
+    // 1 / (x_end - x_start), p / (gamma - 1), and the 3-D uniform target state.
+    double sponge_inv_w, sponge_e0;
+    double sponge_t[5];
 };
 
 // Bits of IbmGhostDev::fluid / MarkerDev::fluid.  The solid mask changes only

@@ -173,19 +173,24 @@ __device__ __forceinline__ unsigned long long* lam_slot(DevState* st) {
 }
 
 // Local max wave speed of cfl_system, crates/cfd_solver/src/lib.rs:647-669.
+// The divisions of the reference's formula (by rho, by dx/dy/dz, by R) are taken
+// as products with reciprocals (1 / rho once per cell, the others once per
+// mesh): the wave speed differs from the reference's by a few ulps, and so
+// does dt, far below the step's own error.  The stage epilogue and the
+// stand-alone CFL pass both call this function, so they agree bit for bit.
 __device__ __forceinline__ double wave_speed(const Geometry& g, const Physics& ph, const U4& u) {
     if (!(u.r > 0.0)) return 0.0;
     const double gm1 = ph.gamma - 1.0;
     const double inv = 1.0 / u.r;
     const double vx = mul_(u.mx, inv), vy = mul_(u.my, inv);
-    const double p = pressure_d(u, gm1);
-    const double a = sqrt(mul_(ph.gamma, p) / u.r);
-    double lam = add_(add_(add_(fabs(vx), a) / g.h[0], add_(fabs(vy), a) / g.h[1]), add_(0.0, a) / g.h[2]);
+    const double ke = mul_(mul_(0.5, u.r), add_(mul_(vx, vx), mul_(vy, vy)));
+    const double p = mul_(gm1, sub_(u.E, ke));
+    const double a = sqrt(mul_(mul_(ph.gamma, p), inv));
+    double lam = add_(add_(mul_(add_(fabs(vx), a), g.inv_h[0]), mul_(add_(fabs(vy), a), g.inv_h[1])),
+                      mul_(add_(0.0, a), g.inv_h[2]));
     if (ph.viscous) {
-        const double ke = mul_(mul_(0.5, u.r), add_(mul_(vx, vx), mul_(vy, vy)));
-        const double pp = mul_(gm1, sub_(u.E, ke));
-        const double t = mul_(pp, inv) / ph.r_gas;
-        const double nu = viscosity(ph, t) / u.r;
+        const double t = mul_(mul_(p, inv), ph.inv_r_gas);
+        const double nu = mul_(viscosity(ph, t), inv);
         lam = add_(lam, mul_(mul_(2.0, nu), ph.cfl_visc_sum));
     }
     return lam;
@@ -546,12 +551,14 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     const double cx = centre(g.lo[0], g.h[0], i);
                     if (cx >= ph.sponge_x_start) {
                         const double cy = centre(g.lo[1], g.h[1], j + g.j_off);
-                        const double inv_w = 1.0 / (ph.sponge_x_end - ph.sponge_x_start);
-                        const double s = fmin(fmax((cx - ph.sponge_x_start) * inv_w, 0.0), 1.0);
+                        const double s = fmin(fmax((cx - ph.sponge_x_start) * ph.sponge_inv_w, 0.0), 1.0);
                         const double f = fmin(ph.sponge_sigma * s * s * dt, 1.0);
                         const double hh = ph.sponge_height;
                         const double uy = 4.0 * ph.sponge_u_max * cy * (hh - cy) / (hh * hh);
-                        const U4 tg = prim_to_cons(ph.sponge_rho, uy, 0.0, ph.sponge_p, gm1);
+                        // prim_to_cons(rho, uy, 0, p) with p / (gamma - 1) formed on the host
+                        const double rho_s = ph.sponge_rho;
+                        const double ke = mul_(mul_(0.5, rho_s), add_(mul_(uy, uy), mul_(0.0, 0.0)));
+                        const U4 tg{rho_s, mul_(rho_s, uy), mul_(rho_s, 0.0), add_(ph.sponge_e0, ke)};
                         nw.r += f * (tg.r - nw.r);
                         nw.mx += f * (tg.mx - nw.mx);
                         nw.my += f * (tg.my - nw.my);

@@ -112,19 +112,22 @@ __device__ __forceinline__ void write_ghosts3(const Geometry& g, const Physics& 
 }
 
 // Local max wave speed of cfl_system, crates/cfd_solver/src/lib.rs:647-669.
+// As the 2-D wave_speed: the reference's divisions taken as products with
+// reciprocals (a few ulps from its value), one code for the stage epilogue and
+// the stand-alone CFL pass.
 __device__ __forceinline__ double wave_speed3(const Geometry& g, const Physics& ph, const U5& u) {
     if (!(u.r > 0.0)) return 0.0;
     const double gm1 = ph.gamma - 1.0;
     const double inv = 1.0 / u.r;
     const double vx = mul_(u.mx, inv), vy = mul_(u.my, inv), vz = mul_(u.mz, inv);
-    const double p = pressure5(u, gm1);
-    const double a = sqrt(mul_(ph.gamma, p) / u.r);
-    double lam = add_(add_(add_(fabs(vx), a) / g.h[0], add_(fabs(vy), a) / g.h[1]), add_(fabs(vz), a) / g.h[2]);
+    const double ke = mul_(mul_(0.5, u.r), add_(add_(mul_(vx, vx), mul_(vy, vy)), mul_(vz, vz)));
+    const double p = mul_(gm1, sub_(u.E, ke));
+    const double a = sqrt(mul_(mul_(ph.gamma, p), inv));
+    double lam = add_(add_(mul_(add_(fabs(vx), a), g.inv_h[0]), mul_(add_(fabs(vy), a), g.inv_h[1])),
+                      mul_(add_(fabs(vz), a), g.inv_h[2]));
     if (ph.viscous) {
-        const double ke = mul_(mul_(0.5, u.r), add_(add_(mul_(vx, vx), mul_(vy, vy)), mul_(vz, vz)));
-        const double pp = mul_(gm1, sub_(u.E, ke));
-        const double t = mul_(pp, inv) / ph.r_gas;
-        const double nu = viscosity(ph, t) / u.r;
+        const double t = mul_(mul_(p, inv), ph.inv_r_gas);
+        const double nu = mul_(viscosity(ph, t), inv);
         lam = add_(lam, mul_(mul_(2.0, nu), ph.cfl_visc_sum));
     }
     return lam;
@@ -503,10 +506,10 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
                     // (rho, u_max, 0, 0, p), examples/sphere_drag_validation/main.rs:119-160
                     const double cx = centre(g.lo[0], g.h[0], i);
                     if (cx >= ph.sponge_x_start) {
-                        const double inv_w = 1.0 / (ph.sponge_x_end - ph.sponge_x_start);
-                        const double s = fmin(fmax((cx - ph.sponge_x_start) * inv_w, 0.0), 1.0);
+                        const double s = fmin(fmax((cx - ph.sponge_x_start) * ph.sponge_inv_w, 0.0), 1.0);
                         const double f = fmin(ph.sponge_sigma * s * s * dt, 1.0);
-                        const U5 tg = prim_to_cons5(ph.sponge_rho, ph.sponge_u_max, 0.0, 0.0, ph.sponge_p, gm1);
+                        // prim_to_cons5(rho, u_max, 0, 0, p), formed on the host
+                        const U5 tg{ph.sponge_t[0], ph.sponge_t[1], ph.sponge_t[2], ph.sponge_t[3], ph.sponge_t[4]};
                         nwu.r += f * (tg.r - nwu.r);
                         nwu.mx += f * (tg.mx - nwu.mx);
                         nwu.my += f * (tg.my - nwu.my);

@@ -77,34 +77,35 @@ struct CflArgs {
     long long pitch;
     int nx, ny;
     double dx, dy, dz;
+    double idx, idy, idz, inv_r_gas;  // 1 / dx, 1 / dy, 1 / dz, 1 / R
     double gamma, r_gas, cfl, fixed_dt;
     int viscous, visc_model;
     double mu, visc_sum;
 };
 
 // Same wave speed as the context path's CFL (cfl_system's per-cell lambda with
-// the z term of the 2-D mesh and the optional viscous spectral radius).
-// Every operation is rounded explicitly (no FMA contraction), as in the
-// context path, so the two agree bit for bit.
+// the z term of the 2-D mesh and the optional viscous spectral radius), in the
+// context path's form: the reference's divisions by rho, dx, dy, dz and R taken
+// as products with reciprocals.  Every operation is rounded explicitly (no FMA
+// contraction), as in the context path, so the two agree bit for bit.
 __device__ double cell_lambda(const CflArgs& a, double r, double mx, double my, double E) {
     if (!(r > 0.0)) return 0.0;
     const double gm1 = a.gamma - 1.0;
     const double inv = 1.0 / r;
     const double vx = __dmul_rn(mx, inv), vy = __dmul_rn(my, inv);
-    const double m2 = __dadd_rn(__dmul_rn(mx, mx), __dmul_rn(my, my));
-    const double p = __dmul_rn(gm1, __dsub_rn(E, __dmul_rn(0.5, m2) / r));
-    const double c = sqrt(__dmul_rn(a.gamma, p) / r);
-    double lam = __dadd_rn(__dadd_rn(__dadd_rn(fabs(vx), c) / a.dx, __dadd_rn(fabs(vy), c) / a.dy),
-                           __dadd_rn(0.0, c) / a.dz);
+    const double ke = __dmul_rn(__dmul_rn(0.5, r), __dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)));
+    const double p = __dmul_rn(gm1, __dsub_rn(E, ke));
+    const double c = sqrt(__dmul_rn(__dmul_rn(a.gamma, p), inv));
+    double lam = __dadd_rn(__dadd_rn(__dmul_rn(__dadd_rn(fabs(vx), c), a.idx), __dmul_rn(__dadd_rn(fabs(vy), c), a.idy)),
+                           __dmul_rn(__dadd_rn(0.0, c), a.idz));
     if (a.viscous) {
-        const double ke = __dmul_rn(__dmul_rn(0.5, r), __dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)));
-        const double t = __dmul_rn(__dmul_rn(gm1, __dsub_rn(E, ke)), inv) / a.r_gas;
+        const double t = __dmul_rn(__dmul_rn(p, inv), a.inv_r_gas);
         double mu = a.mu;
         if (a.visc_model == EFVM_VISC_SUTHERLAND) {
             const double MU_REF = 1.827e-5, T_REF = 291.15, S = 120.0;
             mu = MU_REF * pow(t / T_REF, 1.5) * (T_REF + S) / (t + S);
         }
-        lam = __dadd_rn(lam, __dmul_rn(__dmul_rn(2.0, mu / r), a.visc_sum));
+        lam = __dadd_rn(lam, __dmul_rn(__dmul_rn(2.0, __dmul_rn(mu, inv)), a.visc_sum));
     }
     return lam;
 }
@@ -178,6 +179,10 @@ extern "C" int efvm_cfl_dt_noalloc(const double* rho, const double* rho_u, const
     a.dx = (grid->hi[0] - grid->lo[0]) / (double)grid->nx;
     a.dy = (grid->hi[1] - grid->lo[1]) / (double)grid->ny;
     a.dz = (grid->hi[2] - grid->lo[2]) / (double)(grid->nz > 0 ? grid->nz : 1);
+    a.idx = 1.0 / a.dx;
+    a.idy = 1.0 / a.dy;
+    a.idz = 1.0 / a.dz;
+    a.inv_r_gas = 1.0 / params->r_gas;
     a.gamma = params->gamma;
     a.r_gas = params->r_gas;
     a.cfl = params->cfl;
