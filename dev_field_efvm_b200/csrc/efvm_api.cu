@@ -717,6 +717,7 @@ int setup_case(const efvm_grid& gr, const efvm_params& p, int row0, int rows, bo
     ph.body_force_x = p.body_force_x;
     ph.dx_inv2 = 1.0 / (g.h[0] * g.h[0]);
     ph.cp = p.gamma * p.r_gas / (p.gamma - 1.0);
+    ph.cp_pr = ph.cp / 0.72;
     ph.cfl_visc_sum = 1.0 / (g.h[0] * g.h[0]) + 1.0 / (g.h[1] * g.h[1]) + 1.0 / (g.h[2] * g.h[2]);
     ph.inv_r_gas = 1.0 / p.r_gas;
     // the sponge's constants with the operations the device would apply (this file

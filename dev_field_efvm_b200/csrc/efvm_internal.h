@@ -89,7 +89,8 @@ struct Physics {
     double sponge_x_start, sponge_x_end, sponge_sigma, sponge_u_max, sponge_height, sponge_rho, sponge_p;
     double body_force_x;
     double dx_inv2;       // 1/(dx*dx), viscous x weight
-    double cp;            // gamma*R/(gamma-1), for kappa = mu*cp/0.72
+    double cp;            // gamma*R/(gamma-1)
+    double cp_pr;         // cp / 0.72 (Pr), for kappa = mu*cp/Pr
     double cfl_visc_sum;  // 1/dx^2 + 1/dy^2 + 1/dz^2
     double inv_r_gas;     // 1 / R (the CFL wave speed's temperature)
     // Sponge constants, formed once on the host with the device's operations:

@@ -272,12 +272,12 @@ __device__ __forceinline__ Q4<R> shfl_down_q(const Q4<R>& u, int d) {
 }
 
 // Primitive (u, v, T) of a state given 1/rho (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
-__device__ __forceinline__ void prim_uvt(const U4& u, double inv, double gm1, double r_gas, double& vu, double& vv,
+__device__ __forceinline__ void prim_uvt(const U4& u, double inv, double gm1, double inv_r_gas, double& vu, double& vv,
                                          double& t) {
     vu = u.mx * inv;
     vv = u.my * inv;
     const double ke = 0.5 * u.r * (vu * vu + vv * vv);
-    t = gm1 * (u.E - ke) * inv / r_gas;
+    t = gm1 * (u.E - ke) * inv * inv_r_gas;  // T = p / (rho R), the division by R as a product
 }
 
 constexpr int STRIP = 31;  // cells a warp owns per row (lane 31 supplies the right face)
@@ -478,7 +478,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     const double rn[4] = {r1, r2, r3, r4};
                     const double i0 = r1 * w;
                     double us, vs, ts;
-                    prim_uvt(ucd, i0, gm1, ph.r_gas, us, vs, ts);
+                    prim_uvt(ucd, i0, gm1, ph.inv_r_gas, us, vs, ts);
                     auto nb = [&](int k, double& vu, double& vv, double& t) {
                         if (sn[k]) {
                             vu = 0.0; vv = 0.0; t = ts;
@@ -493,7 +493,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                             q.my = uin[2 * P + no[k]];
                             q.E = uin[3 * P + no[k]];
                         }
-                        prim_uvt(q, ninv[k], gm1, ph.r_gas, vu, vv, t);
+                        prim_uvt(q, ninv[k], gm1, ph.inv_r_gas, vu, vv, t);
                     };
                     const double y_im = a.yw[j], y_ip = a.yw[g.ny + j], y_is = a.yw[2 * g.ny + j];
                     const double dxi2 = ph.dx_inv2;
@@ -517,7 +517,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                         lt = lt + d2y(mt, pt, ts);
                     }
                     const double mu = viscosity(ph, ts);
-                    const double kappa = mu * ph.cp / 0.72;  // thermal_conductivity, crates/cfd_eos/src/lib.rs:83-87
+                    const double kappa = mu * ph.cp_pr;  // thermal_conductivity mu cp / Pr, crates/cfd_eos/src/lib.rs:83-87
                     const double fxv = mu * lu;
                     const double fyv = mu * lv;
                     rhs[1] += fxv;

@@ -169,13 +169,13 @@ __device__ __forceinline__ V5 shfl_down5(const V5& u, int d) {
 }
 
 // Primitive (u, v, w, T) of a state given 1/rho (cons_to_prim, crates/cfd_eos/src/lib.rs:44-53).
-__device__ __forceinline__ void prim5(const U5& u, double inv, double gm1, double r_gas, double& vu, double& vv,
+__device__ __forceinline__ void prim5(const U5& u, double inv, double gm1, double inv_r_gas, double& vu, double& vv,
                                       double& vw, double& t) {
     vu = u.mx * inv;
     vv = u.my * inv;
     vw = u.mz * inv;
     const double ke = 0.5 * u.r * (vu * vu + vv * vv + vw * vw);
-    t = gm1 * (u.E - ke) * inv / r_gas;
+    t = gm1 * (u.E - ke) * inv * inv_r_gas;
 }
 
 constexpr int WPB3 = 4;   // warps per block of the 3-D stage kernel, stacked in z
@@ -443,17 +443,17 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
                     }
                     inv[0] = w;
                     double us, vs, ws, ts;
-                    prim5(ucd, inv[0], gm1, ph.r_gas, us, vs, ws, ts);
+                    prim5(ucd, inv[0], gm1, ph.inv_r_gas, us, vs, ws, ts);
                     const double mu = viscosity(ph, ts);
-                    const double kappa = mu * ph.cp / 0.72;  // thermal_conductivity, crates/cfd_eos/src/lib.rs:83-87
+                    const double kappa = mu * ph.cp_pr;  // thermal_conductivity mu cp / Pr, crates/cfd_eos/src/lib.rs:83-87
                     double lu = 0.0, lv = 0.0, lw = 0.0, lt = 0.0;  // d2x + d2y + d2z of u, v, w, T
 #pragma unroll
                     for (int ax = 0; ax < 3; ++ax) {
                         double pu = 0.0, pv = 0.0, pw = 0.0, pt = ts, mu_ = 0.0, mv = 0.0, mw = 0.0, mt = ts;
                         if (!sn[2 * ax])
-                            prim5(load5(uin, P, nbo[2 * ax]), inv[2 * ax + 1], gm1, ph.r_gas, pu, pv, pw, pt);
+                            prim5(load5(uin, P, nbo[2 * ax]), inv[2 * ax + 1], gm1, ph.inv_r_gas, pu, pv, pw, pt);
                         if (!sn[2 * ax + 1])
-                            prim5(load5(uin, P, nbo[2 * ax + 1]), inv[2 * ax + 2], gm1, ph.r_gas, mu_, mv, mw, mt);
+                            prim5(load5(uin, P, nbo[2 * ax + 1]), inv[2 * ax + 2], gm1, ph.inv_r_gas, mu_, mv, mw, mt);
                         double im = 0.0, ip = 0.0, is = 0.0;
                         if (ax == 1) {
                             im = a.yw[j];
