@@ -806,7 +806,7 @@ __device__ __forceinline__ bool sample_bilinear(const Geometry& g, const Physics
         const double vu = u.mx * inv, vv = u.my * inv;
         const double ke = 0.5 * u.r * (vu * vu + vv * vv);
         const double p = gm1 * (u.E - ke);
-        const double t = p * inv / ph.r_gas;
+        const double t = p * inv * ph.inv_r_gas;
         acc[0] += w * u.r;
         acc[1] += w * vu;
         acc[2] += w * vv;
@@ -858,6 +858,7 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
     const double gm1 = ph.gamma - 1.0;
     double f[6] = {0, 0, 0, 0, 0, 0};
     if (blk == 0) {
+        const double inv_off = 1.0 / ib.sample_offset;  // traction = mu * u_t / offset
         for (int m = tid; m < ib.n_markers; m += blockDim.x) {
             const MarkerDev mk = ib.markers[m];
             if (!mk.valid) continue;
@@ -871,7 +872,7 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
             for (int d = 0; d < 3; ++d) {
                 const double ut = usd[d] - udotn * mk.normal[d];
                 f[d] += -img[3] * mk.normal[d] * mk.area;
-                f[3 + d] += mu * ut / ib.sample_offset * mk.area;
+                f[3 + d] += mu * ut * inv_off * mk.area;
             }
         }
     } else {
@@ -881,7 +882,6 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
             const int i = gh.i, j = gh.j;
             const double dx = g.h[0], dy = g.h[1], dz = g.h[2];
             const double face_area[3] = {dy * dz, dx * dz, dx * dy};
-            const double dn[3] = {dx, dy, dz};
             const double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
             const double* z0 = ib.zg0 + 4LL * k;
             // all neighbour states first (in bounds: the ring of boundary ghosts)
@@ -909,17 +909,21 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
                 const U4 u = nbu[nb];
                 const int dim = nb >> 1;
                 const double sign = (nb & 1) ? -1.0 : 1.0;
-                const double p = pressure_d(u, gm1);
-                f[dim] -= p * sign * face_area[dim];
+                // one division per neighbour (1/rho); p, T and the wall-distance
+                // quotient u / (dn / 2) as products, a few ulps from the
+                // reference's divisions
                 const double inv = 1.0 / u.r;
                 const double vel0 = u.mx * inv, vel1 = u.my * inv;
                 const double ke = 0.5 * u.r * (vel0 * vel0 + vel1 * vel1);
-                const double t = gm1 * (u.E - ke) * inv / ph.r_gas;
+                const double p = gm1 * (u.E - ke);
+                f[dim] -= p * sign * face_area[dim];
+                const double t = p * inv * ph.inv_r_gas;
                 const double mu = viscosity(ph, t);
                 const double vel[3] = {vel0, vel1, 0.0};
+                const double inv_half_dn = 2.0 * g.inv_h[dim];
 #pragma unroll
                 for (int td = 0; td < 3; ++td)
-                    if (td != dim) f[3 + td] += mu * vel[td] / (0.5 * dn[dim]) * face_area[dim];
+                    if (td != dim) f[3 + td] += mu * vel[td] * inv_half_dn * face_area[dim];
             }
         }
     }
