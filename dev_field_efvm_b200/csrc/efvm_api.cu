@@ -281,9 +281,9 @@ int build_ibm_lists(efvm_ctx* c) {
     c->force_partials = nullptr;
     const size_t nblocks = 1 + (ghosts.size() + IBM_THREADS - 1) / IBM_THREADS;
     CUDA_TRY(c, cudaMalloc(&c->force_partials, nblocks * 6 * sizeof(double)));
-    CUDA_TRY(c, cudaMalloc(&c->zg0, ng * 4 * sizeof(double)));
+    CUDA_TRY(c, cudaMalloc(&c->zg0, 2 * ng * 4 * sizeof(double)));
     CUDA_TRY(c, cudaMalloc(&c->zfill, 3 * ng * 4 * sizeof(double)));
-    CUDA_TRY(c, cudaMemsetAsync(c->zg0, 0, ng * 4 * sizeof(double), S(c)));
+    CUDA_TRY(c, cudaMemsetAsync(c->zg0, 0, 2 * ng * 4 * sizeof(double), S(c)));
     CUDA_TRY(c, cudaMemsetAsync(c->zfill, 0, 3 * ng * 4 * sizeof(double), S(c)));
     if (!ghosts.empty())
         CUDA_TRY(c, cudaMemcpyAsync(c->ghosts_dev, ghosts.data(), ghosts.size() * sizeof(IbmGhostDev),
@@ -490,7 +490,7 @@ int prologue(efvm_ctx* c) {
     return EFVM_OK;
 }
 
-void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, bool pdl = true) {
+void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, bool pdl = true, bool defer = false) {
     if (c->nn)  // the learned corrections of this stage's input
         c->launches += nn_forward_padded(c->nn, uin, c->g.plane, c->g.pitch, c->g.nx, c->g.ny, c->corr, c->prims,
                                          c->sensor, c->fallbacks, S(c));
@@ -508,7 +508,19 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
     a.stage = stage;
     a.completes_step = (stage == 2 || stage == 3) ? 1 : 0;
     a.want_cfl = a.completes_step && c->ph.fixed_dt <= 0.0;
+    a.defer_forces = defer ? 1 : 0;
     c->launches += launch_stage(a, pdl, S(c));
+}
+
+// The IBM forces of the step graph's last stage run in the next step's first
+// launch (beside its set-up and mirror), so that the step ends with its last
+// stage.  Anything that reads the forces, or changes what they read (the state,
+// the bodies, the force history's control), first runs them here if a step
+// left them pending: the kernel does nothing otherwise.
+static int finish_forces(efvm_ctx* c) {
+    if (!c->ibm || is_3d(c)) return EFVM_OK;
+    c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, c->U[0], c->st, 2, -1, 0, false, S(c), 1);
+    return EFVM_OK;
 }
 
 // Launch the kernels of one substage at RK stage `stage` (0..2, or 3 = Euler):
@@ -527,30 +539,32 @@ void enqueue_substage(efvm_ctx* c, int stage, double* uin, double* uout, bool wi
     if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, uout, c->st, stage, -1, 0, true, S(c));
 }
 
-// One whole SSP-RK3 step.  With IBM the forces of a stage and the mirror of the
-// next run in one launch (7 launches a step instead of 10).
 // One whole SSP-RK3 step, as captured into the step graph.  With IBM the
-// forces of stage s run on a side branch that forks after stage s, in parallel
-// with the mirror and stage s + 1 (they read only fluid cells of the stage-s
-// output and the stage-s z-fill, which the next stage leaves alone); the
-// branch joins at the end of the step, before the next step's mirror rewrites
-// the z-ghost state the last forces read.
+// forces of stages 1 and 2 run on a side branch that forks after the stage, in
+// parallel with the mirror and the next stage (they read only fluid cells of
+// the stage's output and the stage's z-fill, which the next stage leaves
+// alone); the branch joins at the end of the step.  The forces of stage 3 run
+// in the next step's first launch (finish_forces runs them before anything
+// reads them): they read fluid cells of U0, which that launch's mirror leaves
+// alone, stage 3's z-fill, and this step's saved z-ghost state, which the next
+// step saves into the other parity's buffer.
 int enqueue_rk3_step(efvm_ctx* c) {
     double* bufs[4] = {c->U[0], c->U[1], c->U[2], c->U[0]};
     if (c->ibm && is_3d(c)) {
         for (int s = 0; s < 3; ++s) enqueue_substage(c, s, bufs[s], bufs[s + 1], s == 0);
         return EFVM_OK;
     }
-    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->st, -1, 0, 1, true, S(c));
+    // the first launch: the forces of the previous step's last stage (when pending),
+    // the set-up and the mirror of stage 1; bufs[0] is both their state and its input
+    if (c->ibm) c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[0], c->st, 2, 0, 1, true, S(c), 1);
     else c->launches += launch_step_setup(c->ph, c->st, true, S(c));
     for (int s = 0; s < 3; ++s) {
-        enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1]);
-        if (c->ibm) {
+        enqueue_stage_kernel(c, s, bufs[s], bufs[s + 1], true, c->ibm && s == 2);
+        if (c->ibm && s < 2) {
             CUDA_TRY(c, cudaEventRecord(c->ev_fork[s], S(c)));
             CUDA_TRY(c, cudaStreamWaitEvent(c->side, c->ev_fork[s], 0));
             c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, s, -1, 0, false, c->side);
-            if (s < 2)
-                c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, -1, s + 1, 0, true, S(c));
+            c->launches += launch_ibm(c->g, c->ph, c->ibm_desc, bufs[s + 1], c->st, -1, s + 1, 0, true, S(c));
         }
     }
     if (c->ibm) {
@@ -893,6 +907,10 @@ int efvm_destroy(efvm_ctx* c) {
 
 static int transfer_state(efvm_ctx* c, double* base, int64_t si, int64_t sj, int64_t sv, bool upload) {
     if (!c || !base) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (upload) {  // pending forces read the state this replaces
+        const int rcf = finish_forces(c);
+        if (rcf) return rcf;
+    }
     const Geometry& g = c->g;
     // the host span the strides address, [min offset, max offset]
     int64_t lo = 0, hi = 0;
@@ -992,6 +1010,10 @@ int efvm_get_solver_state(efvm_ctx* c, efvm_solver_state* out) {
 
 int efvm_set_solver_state(efvm_ctx* c, const efvm_solver_state* in) {
     if (!c || !in) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    {
+        const int rcf = finish_forces(c);
+        if (rcf) return rcf;
+    }
     if (in->rk_stage < 0 || in->rk_stage > 2) return fail(c, EFVM_ERR_INVALID_ARG, "rk_stage must be 0..2");
     DevState s;
     int rc = read_state(c, s);
@@ -1202,6 +1224,8 @@ int efvm_wave_speed_slot(efvm_ctx* c, uint64_t** dev_slot) {
 
 int efvm_substep(efvm_ctx* c) {
     if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    int rc0 = finish_forces(c);
+    if (rc0) return rc0;
     if (c->control_dirty) sync_control(c, 0, 0.0, 0);
     int rc = prologue(c);
     if (rc) return rc;
@@ -1249,7 +1273,12 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
     }
     if (c->graph_with_history != (cap != 0)) c->graph_valid = false;
     c->graph_with_history = cap != 0;
-    if (!async || c->control_dirty) sync_control(c, stop_at_t, t_stop, cap);
+    if (!async || c->control_dirty) {
+        // forces a previous call left pending go into that call's history, not this one's
+        rc = finish_forces(c);
+        if (rc) return rc;
+        sync_control(c, stop_at_t, t_stop, cap);
+    }
     rc = prologue(c);  // may rebuild the IBM descriptor (first step after set_cylinders)
     if (rc) return rc;
     c->ibm_desc.history = cap ? c->history : nullptr;
@@ -1280,6 +1309,8 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
     }
     CUDA_TRY(c, cudaGetLastError());
     if (async) return EFVM_OK;
+    rc = finish_forces(c);  // the last step's stage-3 forces, for the history and later reads
+    if (rc) return rc;
     DevState s;
     rc = read_state(c, s);
     if (rc) return rc;
@@ -1321,6 +1352,10 @@ int efvm_cfl(efvm_ctx* c, double* dt_out) {
 int efvm_set_cylinders(efvm_ctx* c, const efvm_cylinder* cyl, int32_t n, const double fs[5]) {
     if (is_3d(c)) return refuse_3d(c, "efvm_set_cylinders");
     if (!c || (n > 0 && (!cyl || !fs)) || n < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid cylinder arguments");
+    {  // pending forces belong to the bodies being replaced
+        const int rcf = finish_forces(c);
+        if (rcf) return rcf;
+    }
     if (n == 0) {
         c->ibm = false;
         c->graph_valid = false;
@@ -1415,6 +1450,8 @@ static int read_forces(efvm_ctx* c, double* out, int offset) {
         for (int d = 0; d < 6; ++d) out[d] = 0.0;
         return EFVM_OK;
     }
+    const int rc = finish_forces(c);
+    if (rc) return rc;
     CUDA_TRY(c, cudaMemcpyAsync(out, c->force_out + offset, 6 * sizeof(double), cudaMemcpyDeviceToHost, S(c)));
     CUDA_TRY(c, cudaStreamSynchronize(S(c)));
     return EFVM_OK;
@@ -1469,6 +1506,10 @@ int efvm_density_error(efvm_ctx* c, const efvm_vortex* v, double out[2]) {
 int efvm_init_vortex(efvm_ctx* c, const efvm_vortex* v) {
     if (is_3d(c)) return refuse_3d(c, "efvm_init_vortex");
     if (!c || !v) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    {
+        const int rcf = finish_forces(c);
+        if (rcf) return rcf;
+    }
     c->launches += launch_init_vortex(c->g, *v, cur_buf(c), S(c));
     c->lam_stale = true;
     c->ghosts_stale = true;
@@ -1498,6 +1539,10 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
     if (!c || !out_ms || n_steps < 0) return fail(c, EFVM_ERR_INVALID_ARG, "invalid argument");
     if (c->params.integrator == EFVM_INTEGRATOR_EULER || c->rk_stage != 0)
         return fail(c, EFVM_ERR_INVALID_ARG, "efvm_profile_steps needs an RK3 context at a step boundary");
+    {
+        const int rcf = finish_forces(c);
+        if (rcf) return rcf;
+    }
     if (c->control_dirty) sync_control(c, 0, 0.0, 0);
     int rc = prologue(c);
     if (rc) return rc;

@@ -42,7 +42,7 @@ struct DevState {
     long long hist_cap;
     unsigned long long lam_ext;  // external wave-speed slot (slabs), see efvm_wave_speed_slot
     int ext_lam;             // 1: accumulate into / read from lam_ext
-    int pad_;
+    int forces_pending;      // the last stage's IBM forces are still to run (step graph)
     unsigned long long done_ns;  // device global timer when the set-up stopped the run
 };
 
@@ -168,9 +168,11 @@ struct Ibm {
     const MarkerDev* markers;
     double sample_offset;   // dx
     // emulated z-ghost states of the solid cells (the 2-D mesh's z layers),
-    // used only by the staircase wall force: zg0 (saved at stage 1) and the
-    // pre-mirror fill of each RK stage (one buffer per stage)
-    double* zg0;            // n_ghost x 4
+    // used only by the staircase wall force: zg0 (saved at stage 1, one buffer
+    // per step parity, so that the last stage's forces of one step can run
+    // beside the next step's first mirror) and the pre-mirror fill of each RK
+    // stage (one buffer per stage)
+    double* zg0;            // 2 x n_ghost x 4
     double* zfill;          // 3 x n_ghost x 4
     double* force_out;      // 12 doubles: marker force (6) then wall force (6)
     double* history;        // hist_cap x 6 (may be null)
@@ -195,6 +197,7 @@ struct StageArgs {
     int completes_step;               // sponge + CFL + clock in the epilogue
     int want_cfl;
     const float* corr;                // learned face-flux corrections [2][4][ny][nx] or null
+    int defer_forces;                 // stage 2 of the step graph: its IBM forces run in the next launch
 };
 
 // ---- batches of independent cases (efvm_batch.cu) --------------------------
@@ -257,9 +260,11 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
                      double* q, uint8_t* mask, void* stream);
 // IBM work between stage kernels, one launch: the forces of the state q after
 // stage force_stage (-1: none), the ghost mirror of q for stage mirror_stage
-// (-1: none) and, with setup, the per-step set-up before the mirror.
+// (-1: none) and, with setup, the per-step set-up before the mirror.  With
+// deferred, the forces are those of the last stage of the previous step, run
+// only while DevState::forces_pending is set (and cleared by them).
 int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ibm, double* q, DevState* st,
-               int force_stage, int mirror_stage, int setup, bool pdl, void* stream);
+               int force_stage, int mirror_stage, int setup, bool pdl, void* stream, int deferred = 0);
 int launch_pack(const Geometry& g, const double* host_like, int64_t si, int64_t sj, int64_t sv, double* q,
                  int to_device, void* stream);
 // 3-D spheres: the solid mask with the stagnant/ambient re-seed of flipped

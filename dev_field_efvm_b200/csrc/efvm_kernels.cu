@@ -314,6 +314,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
             st->completed = 1;
             st->step += 1;
             st->time += st->dt;
+            if (a.defer_forces) st->forces_pending = 1;
         } else {
             st->rk_stage = a.stage + 1;
             st->completed = 0;
@@ -613,6 +614,7 @@ struct BatchView {
     DevState* st;
     int stage, completes_step, want_cfl;
     const float* corr;
+    int defer_forces;  // batches have no IBM: always 0
 };
 
 // The same stage over a batch of independent cases, one warp per tile: warp w
@@ -824,7 +826,7 @@ __device__ __forceinline__ bool sample_bilinear(const Geometry& g, const Physics
 // ghost cell, recording its pre-mirror value for the emulated z-ghost of the
 // staircase wall force.  One thread per ghost cell.
 __device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& ph, const Ibm& ib, double* q,
-                                             int stage, int k) {
+                                             int stage, int k, int par) {
     const IbmGhostDev gh = ib.ghosts[k];
     const long long o = cidx(g, gh.i, gh.j);
     const U4 pre = load4(q, g.plane, o);
@@ -834,7 +836,7 @@ __device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& p
     double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
     zf[0] = pre.r; zf[1] = pre.mx; zf[2] = pre.my; zf[3] = pre.E;
     if (stage == 0 || stage == 3) {
-        double* z0 = ib.zg0 + 4LL * k;
+        double* z0 = ib.zg0 + 4LL * ((long long)par * ib.n_ghost + k);
         z0[0] = pre.r; z0[1] = pre.mx; z0[2] = pre.my; z0[3] = pre.E;
     }
     if (!ok || !(gh.fluid & GHOST_MIRROR_BIT)) return;
@@ -851,7 +853,7 @@ __device__ __forceinline__ void mirror_ghost(const Geometry& g, const Physics& p
 // both forces and appends the marker force to the substage history.
 __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& ph, const Ibm& ib,
                                              const double* __restrict__ q, DevState* st, int stage, int blk,
-                                             int nblk) {
+                                             int nblk, int deferred) {
     __shared__ double red[IBM_THREADS / 32][6];
     __shared__ bool last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -883,7 +885,10 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
             const double dx = g.h[0], dy = g.h[1], dz = g.h[2];
             const double face_area[3] = {dy * dz, dx * dz, dx * dy};
             const double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
-            const double* z0 = ib.zg0 + 4LL * k;
+            // the step's saved z-ghost state: stage 3 runs after its stage kernel has
+            // counted the step, the others before
+            const int par = (int)((stage == 2 ? st->step - 1ull : st->step) & 1ull);
+            const double* z0 = ib.zg0 + 4LL * ((long long)par * ib.n_ghost + k);
             // all neighbour states first (in bounds: the ring of boundary ghosts)
             U4 nbu[6];
             nbu[0] = load4(q, g.plane, cidx(g, i + 1, j));
@@ -967,6 +972,9 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
                 st->hist_pos += 1;
             }
             *ib.counter = 0u;  // ready for the next launch
+            // only the deferred launch clears the flag: the stage that sets it starts
+            // while the previous stage's forces may still run on the side branch
+            if (deferred) st->forces_pending = 0;
         }
     }
 }
@@ -982,20 +990,24 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
 // there leaves the state untouched.
 __global__ void __launch_bounds__(IBM_THREADS) ibm_kernel(Geometry g, Physics ph, Ibm ib, double* q, DevState* st,
                                                           int force_stage, int n_force_blocks, int mirror_stage,
-                                                          int setup) {
+                                                          int setup, int deferred) {
     pdl_wait_then_release();
-    if (!st->active) return;
     const int b = blockIdx.x;
     if (b < n_force_blocks) {  // uniform per block
-        forces_block(g, ph, ib, q, st, force_stage, b, n_force_blocks);
+        // Deferred forces belong to a step that ran; they go ahead whatever this
+        // launch's set-up decides, and only while they are pending.  Every block
+        // reads the flag before it counts itself in, and only the last one clears it.
+        if (deferred ? !st->forces_pending : !st->active) return;
+        forces_block(g, ph, ib, q, st, force_stage, b, n_force_blocks, deferred);
         return;
     }
+    if (!st->active) return;
     if (setup) {
         if (b == n_force_blocks && threadIdx.x == 0) step_setup(ph, st);
         if (step_stops(st)) return;
     }
     const int k = (b - n_force_blocks) * blockDim.x + threadIdx.x;
-    if (mirror_stage >= 0 && k < ib.n_ghost) mirror_ghost(g, ph, ib, q, mirror_stage, k);
+    if (mirror_stage >= 0 && k < ib.n_ghost) mirror_ghost(g, ph, ib, q, mirror_stage, k, (int)(st->step & 1ull));
 }
 
 // ---------------------------------------------------------------------------
@@ -1428,13 +1440,13 @@ int launch_geometry(const Geometry& g, const double* cyl, int ncyl, const double
 }
 
 int launch_ibm(const Geometry& g, const Physics& ph, const Ibm& ib, double* q, DevState* st,
-               int force_stage, int mirror_stage, int setup, bool pdl, void* stream) {
+               int force_stage, int mirror_stage, int setup, bool pdl, void* stream, int deferred) {
     const int nf = force_stage >= 0 ? 1 + (ib.n_ghost + IBM_THREADS - 1) / IBM_THREADS : 0;
     int nm = mirror_stage >= 0 ? (ib.n_ghost + IBM_THREADS - 1) / IBM_THREADS : 0;
     if (setup && nm < 1) nm = 1;
     if (nf + nm == 0) return 0;
     launch_k(ibm_kernel, dim3(nf + nm), dim3(IBM_THREADS), (cudaStream_t)stream, pdl, g, ph, ib, q, st, force_stage,
-             nf, mirror_stage, setup);
+             nf, mirror_stage, setup, deferred);
     return 1;
 }
 
