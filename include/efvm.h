@@ -283,10 +283,14 @@ int efvm_set_discs(efvm_ctx* ctx, const efvm_disc* discs, int32_t n, int32_t n_t
 int efvm_set_spheres(efvm_ctx* ctx, const efvm_sphere* spheres, int32_t n, int32_t n_markers,
                      const double freestream[5]);
 /* MarkerForce{pressure,viscous} of the last Output phase
- * (crates/cfd_ibm/src/lib.rs:442-480,601-615). */
+ * (crates/cfd_ibm/src/lib.rs:442-480,601-615).  On a 2-D mesh, efvm_step
+ * computes the forces of a step's last substage in the next step's first
+ * launch; this call (and every call that replaces the state or the bodies, or
+ * steps with a history or a stop time) first runs them if they are still
+ * pending, so it always returns the last substage's forces. */
 int efvm_marker_force(efvm_ctx* ctx, double out[6]);
 /* WallForce{pressure,viscous}, the staircase estimate (crates/cfd_ibm/src/
- * lib.rs:309-395). */
+ * lib.rs:309-395); pending forces are run first, as for efvm_marker_force. */
 int efvm_wall_force(efvm_ctx* ctx, double out[6]);
 /* ---- output -------------------------------------------------------------- */
 /* The fields write_vtk_to writes (crates/cfd_output/src/lib.rs:36-125) for the
