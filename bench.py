@@ -1,32 +1,36 @@
 """Throughput of the B200 explicit finite-volume step (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload cylinder|vortex4096|vortex3d|batch512]
+                    [--workload vortex4096|cylinder|vortex3d|batch512]
 
 A step is one SSP-RK3 time step (three substages) of the whole case.  The
-default workload is the cylinder channel with the ghost-cell immersed boundary
-and viscous terms: 1100x205 cells, MUSCL (minmod) + HLLC-Thornber, FP64,
-parabolic inlet, sponge, marker-force Output phase every substage.  The metric
-is cell-updates/s (interior cells advanced by one full RK3 step per second).
+default workload is the metric's vortex family at its largest single-GPU size:
+the isentropic vortex on the periodic [0,10]^2 box at 4096x4096 cells,
+MUSCL (minmod) + HLLC-Thornber, SSP-RK3, CFL 0.4, FP64.  The metric is
+cell-updates/s (interior cells advanced by one full RK3 step per second).
 
-`value` is device time with the state resident in HBM and L2 flushed between
-timed steps; `e2e` is the same metric through the C-ABI with host buffers:
-every step uploads the state from pinned host memory, steps, downloads it and
-reads the marker force, in several host threads with one context each so that
-one thread's copies overlap the others' kernels (the step is enqueued without a
-status read; the download waits for it).  `roofline` relates the stage kernel's algorithmic
-bytes (the RK3 traffic of a cell-update, 256 B, plus the 1 B solid mask per
-stage) to its live CUDA-event duration and the measured HBM copy bandwidth;
-`fp64` relates the same kernel's FP64 flops (counted by ncu, stored beside the
-traffic figures) to a measured FP64 GEMM.  The kernel reaches neither peak: it
-is bound by instruction issue and FP64 dependency latency.
-`cpu_baseline` times the CPU oracle (the reference's algorithm restated in
-C++, OpenMP over the host cores) on a bounded sample of the same workload.
+`value` is the plain FP64 path: device time with the state resident in HBM
+(537 MB per state buffer, larger than L2; L2 is also flushed between timed
+steps).  `chosen_form` is the FP32-flux form (FP32 reconstruction and face
+fluxes, FP64 accumulation) timed the same way, with the L1 and max-norm
+density error of both forms against the exact vortex and against each other
+after the same number of steps with the same fixed dt, so the line says
+whether the two are at equal L1 error.  `e2e` is the same metric through the
+C-ABI with host buffers: every step uploads the state from pinned host memory,
+steps, and downloads it, on one context (`e2e.value`); `e2e.multi_context`
+adds the aggregate of several host threads with one context each, whose
+copies overlap one another's kernels.  `roofline` relates the stage kernel's
+algorithmic bytes (the RK3 traffic of a cell-update, 256 B, plus the 1 B
+solid mask per stage with an immersed body) to its live CUDA-event duration
+and the measured HBM copy bandwidth; `fp64` relates the same kernel's FP64
+flops (counted by ncu, stored beside the traffic figures) to a measured FP64
+GEMM.  `cpu_baseline` times the CPU oracle (the reference's algorithm
+restated in C++, OpenMP over the host cores) on a bounded sample of the same
+workload, and the serial oracle on one core.
 
 Under torchrun (N > 1) every rank advances its own replica of the case (weak
-scaling: the cylinder's immersed body is not split over row slabs, see
-dev_field_efvm_b200/slab.py), timing is the max over ranks, and `value` counts
-the cells of all ranks.
+scaling, no data-path collective), timing is the max over ranks, and `value`
+counts the cells of all ranks.
 """
 from __future__ import annotations
 
@@ -158,8 +162,12 @@ class ClockSampler:
                 "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
-def cpu_baseline(grid, params, u, ex, target_seconds=12.0):
-    """The CPU oracle (OpenMP, all host threads) on a bounded number of steps."""
+def cpu_baseline(grid, params, u, ex, target_seconds=12.0, one_core_sample=None):
+    """The CPU oracle (OpenMP, all host threads) on a bounded number of steps,
+    and the serial oracle on one core.  `one_core_sample` = (grid, u, what): a
+    smaller grid of the same case for the serial leg when one serial step of the
+    full case would take longer than the sample budget (the oracle's work per
+    cell does not depend on the grid size)."""
     from oracle import pyoracle
     c = pyoracle.OracleCase(grid, params, parallel=True)
     if "cylinders" in ex:
@@ -183,10 +191,12 @@ def cpu_baseline(grid, params, u, ex, target_seconds=12.0):
                "sample": f"{n} RK3 steps of the same case after 2 untimed steps ({dt:.1f} s)"}
     c.close()
     # the same oracle on one core (the reference itself is serial): a shorter sample
-    s1 = pyoracle.OracleCase(grid, params, parallel=False)
+    g1, u1, what = (grid, u, "the same case") if one_core_sample is None else one_core_sample
+    cells1 = g1.nx * g1.ny * g1.nz
+    s1 = pyoracle.OracleCase(g1, params, parallel=False)
     if "cylinders" in ex:
         s1.set_cylinders(ex["cylinders"], ex["freestream"])
-    s1.upload(u)
+    s1.upload(u1)
     s1.step(1)
     t0 = time.perf_counter()
     s1.step(1)
@@ -196,8 +206,9 @@ def cpu_baseline(grid, params, u, ex, target_seconds=12.0):
         t0 = time.perf_counter()
         s1.step(m)
         one1 = (time.perf_counter() - t0) / m
-    out["one_core"] = {"value": cells / one1, "unit": UNIT, "cores": 1,
-                       "sample": f"{max(m, 1)} RK3 step(s) of the same case after 2 untimed steps, serial oracle"}
+    out["one_core"] = {"value": cells1 / one1, "unit": UNIT, "cores": 1,
+                       "sample": f"{max(m, 1)} RK3 step(s) of {what} after {2 if m else 1} untimed step(s), "
+                                 "serial oracle"}
     s1.close()
     return out
 
@@ -334,15 +345,21 @@ def run_batch(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def with_params(params, **changes):
+    from dev_field_efvm_b200 import abi
+    p = abi.make_params(**{f: getattr(params, f) for f, _ in abi.EfvmParams._fields_})
+    for k, v in changes.items():
+        setattr(p, k, type(getattr(p, k))(v))
+    return p
+
+
 def fp32_leg(args, grid, params, u, ex, flush, world, cells):
     """The chosen form on the same case: FP32 reconstruction and fluxes, FP64
     accumulation, device-timed as the FP64 leg."""
     import torch
     from dev_field_efvm_b200 import abi
     from dev_field_efvm_b200.device import Context
-    p32 = abi.make_params(**{f: getattr(params, f) for f, _ in abi.EfvmParams._fields_})
-    p32.precision = abi.PREC_FP32_FLUX
-    ctx32 = Context(grid, p32)
+    ctx32 = Context(grid, with_params(params, precision=abi.PREC_FP32_FLUX))
     if "cylinders" in ex:
         ctx32.set_cylinders(ex["cylinders"], ex["freestream"])
     ctx32.upload(u)
@@ -359,18 +376,117 @@ def fp32_leg(args, grid, params, u, ex, flush, world, cells):
     torch.cuda.synchronize()
     ms32 = sum(a.elapsed_time(b) for a, b in ev32)
     value32 = world * cells * args.steps / (ms32 * 1e-3)
+    prof32 = ctx32.profile_steps(max(10, min(args.steps, 50)))
+    stage32 = prof32[0] / (3 * max(10, min(args.steps, 50)))
     ctx32.close()
-    return value32, ms32
+    return value32, ms32, stage32
+
+
+def accuracy_leg(grid, params, u, ex, t_end):
+    """Density error of both forms on the vortex: FP64 and FP32-flux contexts
+    from the same initial state, the same fixed dt (the CFL dt of the initial
+    state) and the same number of steps to t_end; L1 (volume-weighted) and
+    max-norm of rho - rho_exact for each, and of rho_fp32 - rho_fp64."""
+    from dev_field_efvm_b200 import abi
+    from dev_field_efvm_b200.device import Context
+    v = ex["vortex"]
+    with Context(grid, params) as c:
+        c.upload(u)
+        dt0 = c.cfl()
+    n = max(1, int(round(t_end / dt0)))
+    out, rho = {}, {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_flux", abi.PREC_FP32_FLUX)):
+        with Context(grid, with_params(params, precision=prec, fixed_dt=dt0)) as c:
+            c.upload(u)
+            c.step(n)
+            l1, linf = c.density_error(v)
+            out[name] = {"l1_vs_exact": l1, "linf_vs_exact": linf}
+            rho[name] = c.download()[..., 0]
+    d = np.abs(rho["fp32_flux"] - rho["fp64"])
+    ratio = out["fp32_flux"]["l1_vs_exact"] / out["fp64"]["l1_vs_exact"]
+    return {"t": n * dt0, "steps": n, "dt": dt0, "fp64": out["fp64"], "fp32_flux": out["fp32_flux"],
+            "fp32_minus_fp64": {"l1": float(d.mean()), "linf": float(d.max())},
+            "l1_ratio_fp32_over_fp64": ratio,
+            # equal when the FP32 form's error is within 10 % of the plain method's
+            "equal_l1": bool(abs(ratio - 1.0) <= 0.10)}
+
+
+def e2e_leg(grid, params, u, ex, ctx, n_steps, n_threads, dist):
+    """End to end through the C-ABI: per step the state goes up from pinned host
+    memory (efvm_upload_state), one RK3 step runs (efvm_step, enqueued without
+    a status read), and the state comes back (efvm_download_state, which waits
+    for the step) with the step's result (marker force with a body, else the
+    solver state).  Returns (single-context rate, multi-context rate, threads)."""
+    import torch
+    from dev_field_efvm_b200.device import Context
+    d3 = grid.nz > 1
+    cells = grid.nx * grid.ny * grid.nz
+    shape = (grid.nz, grid.ny, grid.nx, 5) if d3 else (grid.ny, grid.nx, 5)
+    sk = 5 * grid.nx * grid.ny
+
+    def make_host():
+        h = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        h.copy_(torch.from_numpy(u))
+        return h
+
+    def e2e_loop(c, h, n):
+        ptr = h.data_ptr()
+        for _ in range(n):
+            if d3:
+                c.upload_ptr3(ptr, 5, 5 * grid.nx, sk, 1)
+                c.step_async(1)
+                c.download_ptr3(ptr, 5, 5 * grid.nx, sk, 1)
+            else:
+                c.upload_ptr(ptr, 5, 5 * grid.nx, 1)
+                c.step_async(1)
+                c.download_ptr(ptr, 5, 5 * grid.nx, 1)
+            if "cylinders" in ex:
+                c.marker_force()
+            else:
+                c.solver_state()
+
+    def timed(ctxs, hosts, n):
+        for c, h in zip(ctxs, hosts):  # warm-up: graph capture, staging buffers
+            e2e_loop(c, h, 2)
+            h.copy_(torch.from_numpy(u))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        threads = [threading.Thread(target=e2e_loop, args=(c, h, n)) for c, h in zip(ctxs, hosts)]
+        t0 = time.perf_counter()
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            s = float(t.item())
+        return cells * n * len(ctxs) / s
+
+    h0 = make_host()
+    single = timed([ctx], [h0], n_steps)
+    extra = [Context(grid, params) for _ in range(n_threads - 1)]
+    for c in extra:
+        if "cylinders" in ex:
+            c.set_cylinders(ex["cylinders"], ex["freestream"])
+    hosts = [h0] + [make_host() for _ in extra]
+    multi = timed([ctx] + extra, hosts, n_steps)
+    for c in extra:
+        c.close()
+    return single, multi
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8000)
-    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cylinder", choices=["cylinder", "vortex4096", "vortex3d", "batch512"])
+    ap.add_argument("--workload", default="vortex4096", choices=["vortex4096", "cylinder", "vortex3d", "batch512"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the density-error leg (profiler captures)")
     ap.add_argument("--size", type=int, default=None,
                     help="vortex workloads only: a smaller n x n (x n) grid of the same case "
                          "(for profiler captures)")
@@ -440,12 +556,13 @@ def main():
     value = world * cells * args.steps / (ms * 1e-3)
 
     # ---- stage-kernel roofline (live CUDA events per kernel class) --------
-    prof = ctx.profile_steps(max(10, min(args.steps, 50)))
     n_prof = max(10, min(args.steps, 50))
+    prof = ctx.profile_steps(n_prof)
     stage_ms_per_launch = prof[0] / (3 * n_prof)
     mask_bytes = 1 if "cylinders" in ex else 0
     # the RK3 traffic of a cell-update: 8 state reads/writes of 32 B (2-D, 4 planes) or 40 B (3-D, 5 planes)
-    bytes_per_launch = cells * ((320 if d3 else 256) + 3 * mask_bytes) / 3.0
+    bytes_per_cell_update = (320 if d3 else 256) + 3 * mask_bytes
+    bytes_per_launch = cells * bytes_per_cell_update / 3.0
     achieved = bytes_per_launch / (stage_ms_per_launch * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = None
@@ -458,7 +575,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind,
                 "kernel": ("stage3_kernel (fused 3-D MUSCL/HLLC/RK3 substage, x/y/z faces)" if d3
-                           else "stage_kernel (fused MUSCL/HLLC/viscous/RK3 substage)"),
+                           else "stage_kernel (fused MUSCL/HLLC/RK3 substage)"),
+                "bytes_per_cell_update": bytes_per_cell_update, "cells_per_launch": cells,
                 "stage_ms_per_launch": stage_ms_per_launch,
                 # the three stage launches per step against the graph-timed step above
                 # (the per-kernel events of the profile pass wait on the host between
@@ -478,91 +596,62 @@ def main():
                 "counted": entry.get("fp64_how", "")}
 
     # ---- chosen form: FP32 reconstruction/fluxes, FP64 accumulation -------
-    if d3:  # 3-D meshes run in FP64 only
-        value32 = ms32 = None
-    else:
-        value32, ms32 = fp32_leg(args, grid, params, u, ex, flush, world, cells)
+    chosen = None
+    if not d3:  # 3-D meshes run in FP64 only
+        value32, ms32, stage32 = fp32_leg(args, grid, params, u, ex, flush, world, cells)
+        a32 = bytes_per_launch / (stage32 * 1e-3) / 1e9
+        chosen = {"precision": "fp32 reconstruction+flux, fp64 accumulation", "value": value32, "unit": UNIT,
+                  "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
+                  "roofline": {"achieved": a32, "peak": peak, "unit": "GB/s", "frac": a32 / peak,
+                               "stage_ms_per_launch": stage32}}
+        if "vortex" in ex and not args.no_accuracy:
+            # the same horizon in physical time at any grid size: t = 0.25
+            chosen["accuracy"] = accuracy_leg(grid, params, u, ex, t_end=0.25)
 
     # ---- end to end through the C-ABI with pinned host buffers -----------
-    # n_threads host threads, each with its own context and pinned buffer,
-    # run upload -> step -> download -> result read in a loop; the threads'
-    # copies and kernels overlap on the GPU (ctypes releases the GIL in calls).
     n_threads = E2E_THREADS_SMALL if cells < 2_000_000 else E2E_THREADS_LARGE
-    e2e_ctx = [ctx] + [Context(grid, params) for _ in range(n_threads - 1)]
-    hosts = []
-    shape = (grid.nz, grid.ny, grid.nx, 5) if d3 else (grid.ny, grid.nx, 5)
-    for c in e2e_ctx:
-        if "cylinders" in ex:
-            c.set_cylinders(ex["cylinders"], ex["freestream"])
-        h = torch.empty(shape, dtype=torch.float64, pin_memory=True)
-        h.copy_(torch.from_numpy(u))
-        hosts.append(h)
-    n_each = max(3, min(args.steps, 60))
-    sk = 5 * grid.nx * grid.ny
-
-    def e2e_loop(c, h, n):
-        ptr = h.data_ptr()
-        for _ in range(n):
-            if d3:
-                c.upload_ptr3(ptr, 5, 5 * grid.nx, sk, 1)
-                c.step_async(1)  # efvm_step without a status read; the download waits for it
-                c.download_ptr3(ptr, 5, 5 * grid.nx, sk, 1)
-                c.solver_state()  # the step's clock (dt, time, step): 48 B
-            else:
-                c.upload_ptr(ptr, 5, 5 * grid.nx, 1)
-                c.step_async(1)
-                c.download_ptr(ptr, 5, 5 * grid.nx, 1)
-                c.marker_force()
-
-    for c, h in zip(e2e_ctx, hosts):  # warm-up: graph capture, staging buffers
-        e2e_loop(c, h, 2)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    threads = [threading.Thread(target=e2e_loop, args=(c, h, n_each)) for c, h in zip(e2e_ctx, hosts)]
-    t0 = time.perf_counter()
-    for t in threads:
-        t.start()
-    for t in threads:
-        t.join()
-    e2e_s = time.perf_counter() - t0
-    n_e2e = n_each * len(e2e_ctx)
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * cells * n_e2e / e2e_s
-    for c in e2e_ctx[1:]:
-        c.close()
+    n_each = max(3, min(args.steps, 40 if cells < 2_000_000 else 10))
+    e2e_single, e2e_multi = e2e_leg(grid, params, u, ex, ctx, n_each, n_threads, dist)
+    e2e_single *= world
+    e2e_multi *= world
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(grid, params, u, ex)
+        sample = None
+        if args.workload == "vortex4096" and cells > 2_000_000:
+            g1, p1, u1, ex1, _ = workload(args.workload, 1024)
+            sample = (g1, u1, "the same vortex at 1024x1024 (the per-cell work does not depend on the size)")
+        cpu = cpu_baseline(grid, params, u, ex, one_core_sample=sample)
 
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
     if rank == 0:
+        res_bytes = C.sizeof(abi.EfvmSolverState) if "cylinders" not in ex else 48
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(desc, parallelism=f"replicas{world}" if world > 1 else "single",
-                           l2="flushed between timed steps (256 MB write)",
+                           l2=("inputs larger than L2 (537 MB per state buffer); L2 also flushed between timed steps "
+                               "(256 MB write)") if cells * 32 > 126e6 else
+                              "flushed between timed steps (256 MB write)",
                            time=st.time, final_step=int(st.step)),
             "roofline": roofline,
             "fp64": fp64,
+            "chosen_form": chosen,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
-                    "d2h_bytes_per_step": cells * 5 * 8 + (C.sizeof(abi.EfvmSolverState) if d3 else 48),
-                    "steps": n_e2e, "host_threads": n_threads,
-                    "note": "each thread: its own context; per step upload from pinned memory, one RK3 step, "
-                            "download, " + ("solver-state read" if d3 else "marker-force read")},
+            "e2e": {"value": e2e_single, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
+                    "d2h_bytes_per_step": cells * 5 * 8 + res_bytes, "steps": n_each,
+                    "note": "one context: per step upload from pinned memory, one RK3 step, download, "
+                            + ("marker-force read" if "cylinders" in ex else "solver-state read"),
+                    "multi_context": {"value": e2e_multi, "unit": UNIT, "host_threads": n_threads,
+                                      "steps_per_thread": n_each,
+                                      "note": "one context per host thread, each its own copy of the case; "
+                                              "copies of one thread overlap kernels of the others"}},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
-            "chosen_form": None if d3 else {"precision": "fp32 reconstruction+flux, fp64 accumulation",
-                                            "value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps},
         }
         print(json.dumps(line), flush=True)
 

@@ -42,6 +42,8 @@ INTEGRATOR_RK3, INTEGRATOR_EULER = 0, 1
 VISC_SUTHERLAND, VISC_CONSTANT = 0, 1
 PREC_FP64, PREC_FP32_FLUX = 0, 1
 SEAM_REFERENCE, SEAM_TRUE_PERIODIC = 0, 1
+# rows of static scratch behind efvm_cfl_dt_noalloc (EFVM_CFL_NOALLOC_MAX_ROWS)
+CFL_NOALLOC_MAX_ROWS = 16384
 
 
 class EfvmBC(C.Structure):

@@ -1021,6 +1021,7 @@ int efvm_set_solver_state(efvm_ctx* c, const efvm_solver_state* in) {
     s.dt = in->dt;
     s.time = in->time;
     s.step = in->step;
+    s.step_par = (int)(in->step & 1ull);
     s.rk_stage = in->rk_stage;
     s.completed = in->completed_full_step;
     CUDA_TRY(c, cudaMemcpyAsync(c->st, &s, sizeof(DevState), cudaMemcpyHostToDevice, S(c)));

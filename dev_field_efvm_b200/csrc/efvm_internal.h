@@ -44,6 +44,9 @@ struct DevState {
     int ext_lam;             // 1: accumulate into / read from lam_ext
     int forces_pending;      // the last stage's IBM forces are still to run (step graph)
     unsigned long long done_ns;  // device global timer when the set-up stopped the run
+    int step_par;            // parity of the step in progress (step & 1 at its set-up): the z-ghost
+                             // buffer that the forces of its first two stages read
+    int pad_par_;
 };
 
 // Boundary side description resolved for the device.

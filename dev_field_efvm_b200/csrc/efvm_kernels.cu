@@ -684,6 +684,7 @@ __device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
         dt = lam > 0.0 ? ph.cfl / lam : INFINITY;
     }
     st->dt = dt;
+    st->step_par = (int)(st->step & 1ull);
     if (st->ext_lam) {  // the slot starts this step's accumulation from zero
         st->lam_ext = 0ull;
         return;
@@ -885,9 +886,12 @@ __device__ __forceinline__ void forces_block(const Geometry& g, const Physics& p
             const double dx = g.h[0], dy = g.h[1], dz = g.h[2];
             const double face_area[3] = {dy * dz, dx * dz, dx * dy};
             const double* zf = ib.zfill + ((long long)stage % 3) * ib.n_ghost * 4 + 4LL * k;
-            // the step's saved z-ghost state: stage 3 runs after its stage kernel has
-            // counted the step, the others before
-            const int par = (int)((stage == 2 ? st->step - 1ull : st->step) & 1ull);
+            // the step's saved z-ghost state.  Stage 3's forces run after its stage
+            // kernel has counted the step, and the step counter is stable while they
+            // run (the next step's first launch, or the substep call).  The forces of
+            // stages 1 and 2 may run on a side branch while the next stage kernel
+            // counts the step, so they take the parity that the step's set-up recorded.
+            const int par = stage == 2 ? (int)((st->step - 1ull) & 1ull) : st->step_par;
             const double* z0 = ib.zg0 + 4LL * ((long long)par * ib.n_ghost + k);
             // all neighbour states first (in bounds: the ring of boundary ghosts)
             U4 nbu[6];

@@ -156,6 +156,19 @@ extern "C" int efvm_cfl_dt_noalloc(const double* rho, const double* rho_u, const
         efvm::set_global_error("efvm_cfl_dt_noalloc: need nx >= 1, ny >= 1 and pitch >= nx");
         return EFVM_ERR_INVALID_ARG;
     }
+    if (grid->nz > 1) {
+        // the entry point takes no rho_w plane and reads one layer: a 3-D mesh's
+        // wave speed needs |w| and every layer (efvm_cfl handles 3-D contexts)
+        efvm::set_global_error("efvm_cfl_dt_noalloc: nz = " + std::to_string(grid->nz) +
+                               ": only 2-D meshes (nz <= 1) are supported; use efvm_cfl");
+        return EFVM_ERR_UNSUPPORTED;
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (!(grid->hi[a] > grid->lo[a])) {  // also rejects NaN bounds
+            efvm::set_global_error("efvm_cfl_dt_noalloc: the mesh extent hi - lo must be positive on every axis");
+            return EFVM_ERR_INVALID_ARG;
+        }
+    }
     if (grid->ny > EFVM_CFL_NOALLOC_MAX_ROWS) {
         efvm::set_global_error("efvm_cfl_dt_noalloc: ny = " + std::to_string(grid->ny) + " exceeds the " +
                 std::to_string(EFVM_CFL_NOALLOC_MAX_ROWS) + "-row scratch of this entry point; use efvm_cfl");

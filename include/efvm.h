@@ -421,7 +421,7 @@ int efvm_batch_download_state(efvm_batch* batch, int32_t k, double* base, int64_
                               int64_t stride_var);
 int efvm_batch_get_solver_state(efvm_batch* batch, int32_t k, efvm_solver_state* out);
 /* Advance every case by whole RK3 steps until its clock reaches t_stop[k] (the
- * time loop of examples/*: while t < t_final, three app.run() per step) or
+ * time loop of the example drivers: while t < t_final, three app.run() per step) or
  * max_steps steps have run.  Finished cases leave the launch table every
  * `chunk` steps (<= 0: 16).  results (may be NULL) receives one entry per case.
  * Returns EFVM_ERR_NONPHYSICAL if any case went non-physical. */
@@ -511,7 +511,10 @@ int efvm_correction_stats(efvm_ctx* ctx, uint64_t* faces, uint64_t* fallbacks);
  * Its only scratch is file-scope device memory of the library: one double per
  * grid row (EFVM_CFL_NOALLOC_MAX_ROWS rows, 128 KB) and a counter, held on
  * every GPU that loads the library until the process exits.  Grids with more
- * rows are rejected with EFVM_ERR_INVALID_ARG (use efvm_cfl).  All calls on a
+ * rows are rejected with EFVM_ERR_INVALID_ARG (use efvm_cfl), and so are
+ * non-positive extents (hi <= lo on an axis).  Only 2-D meshes are accepted:
+ * nz > 1 returns EFVM_ERR_UNSUPPORTED, since a 3-D wave speed needs rho_w and
+ * every layer.  The result equals efvm_cfl's bit for bit.  All calls on a
  * device share that scratch and it keeps the last call's contents; calls whose
  * kernels overlap on the GPU race and may return a wrong dt, so order them on
  * one stream.  The first call on a device looks up the scratch's device
