@@ -246,15 +246,16 @@ def run_reference(args, rank, world, budget_s=90.0):
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, rank, world, local):
+def batch_measurement(args, local):
     """512 independent cases in one batch (n log-uniform in [32, 512]; half
     periodic vortices to t = 1, half four-quadrant Riemann problems to t = 0.05;
-    MUSCL-minmod + HLLC-Thornber, FP32 fluxes with FP64 accumulation).  `value`
-    is the batch's total cell-updates over its device time (CUDA events on the
-    batch stream around the whole run, host polling gaps included); the
+    MUSCL-minmod + HLLC-Thornber, FP32 fluxes with FP64 accumulation).  The
+    batch runs with the persistent kernel (one launch per chunk of 16 steps over
+    the packed tile queue) and, for comparison, with one launch per stage; the
+    rate is the batch's total cell-updates over its device time (CUDA events on
+    the batch stream around the whole run, host polling gaps included).  The
     sequential leg runs the same cases one context after another and gives the
-    per-case completion percentiles it is compared with.  Each rank runs its own
-    batch (weak scaling)."""
+    per-case completion percentiles the batch is compared with."""
     import torch
     torch.cuda.set_device(local)
     from dev_field_efvm_b200 import cases
@@ -262,30 +263,40 @@ def run_batch(args, rank, world, local):
 
     grids, params, states, t_stop, kinds = cases.batch_cases()
     cells = np.array([g.nx * g.ny for g in grids], dtype=np.float64)
-    warm = Batch(grids, params)
-    for k, u in enumerate(states):
-        warm.upload(k, u)
-    warm.run(t_stop, max_steps=args.warmup)
-    warm.close()
 
-    b = Batch(grids, params)
-    for k, u in enumerate(states):
-        b.upload(k, u)
-    stream = torch.cuda.ExternalStream(b.stream())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    n0 = b.launch_count()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        e0.record(stream)
-        res = b.run(t_stop)
-        e1.record(stream)
+    def timed_run(persistent):
+        warm = Batch(grids, params)
+        warm.set_persistent(persistent)
+        for k, u in enumerate(states):
+            warm.upload(k, u)
+        warm.run(t_stop, max_steps=args.warmup)  # also tunes (cached per process)
+        warm.close()
+        b = Batch(grids, params)
+        b.set_persistent(persistent)
+        for k, u in enumerate(states):
+            b.upload(k, u)
+        stream = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = b.launch_count()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    launches = b.launch_count() - n0
+        with ClockSampler(local) as clocks:
+            e0.record(stream)
+            res = b.run(t_stop)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out = {"ms": ms, "launches": b.launch_count() - n0, "res": res, "clocks": clocks.summary(),
+               "rows": b.rows(), "blocks_per_sm": b.blocks_per_sm() if persistent else None}
+        b.close()
+        return out
+
+    per = timed_run(True)
+    stg = timed_run(False)
+    res = per["res"]
     steps = np.array([r.steps for r in res], dtype=np.float64)
     work = float((cells * steps).sum())
-    value = work / (ms * 1e-3)
     comp = np.array([r.completion_ms for r in res])
+    comp_stage = np.array([r.completion_ms for r in stg["res"]])
 
     # end to end: host states in, the whole batch run, host states out
     t0 = time.perf_counter()
@@ -311,36 +322,54 @@ def run_batch(args, rank, world, local):
         seq_done[k] = (time.perf_counter() - t0) * 1e3
         c.close()
     seq_s = time.perf_counter() - t0
+    return {
+        "workload": "512 cases, n log-uniform in [32,512] (23.4 M cells): 256 periodic vortices to t=1, 256 "
+                    "four-quadrant Riemann problems to t=0.05; MUSCL-minmod + HLLC-Thornber, SSP-RK3, CFL 0.4, "
+                    "FP32 fluxes + FP64 state",
+        "cases": len(grids), "cells": int(cells.sum()), "cell_updates": work,
+        "value": work / (per["ms"] * 1e-3), "unit": UNIT, "batch_ms": per["ms"], "gpu_launches": int(per["launches"]),
+        "kernel": "persistent: one launch per chunk of 16 steps over the packed tile queue",
+        "tuned_rows_per_bucket": per["rows"], "tuned_blocks_per_sm": per["blocks_per_sm"],
+        "completion_ms_p50": float(np.percentile(comp, 50)), "completion_ms_p99": float(np.percentile(comp, 99)),
+        "per_stage_launches": {"value": work / (stg["ms"] * 1e-3), "batch_ms": stg["ms"],
+                               "gpu_launches": int(stg["launches"]),
+                               "completion_ms_p50": float(np.percentile(comp_stage, 50)),
+                               "completion_ms_p99": float(np.percentile(comp_stage, 99))},
+        "sequential": {"value": work / seq_s, "seconds": seq_s,
+                       "completion_ms_p50": float(np.percentile(seq_done, 50)),
+                       "completion_ms_p99": float(np.percentile(seq_done, 99))},
+        "e2e": {"value": work / e2e_s, "unit": UNIT, "h2d_bytes": h2d, "d2h_bytes": h2d,
+                "note": "host states in, the whole batch run, host states out"},
+        "all_finished": bool(all(r.finished for r in res)),
+        "clocks": per["clocks"], "steps_max": int(steps.max()),
+    }
 
+
+def run_batch(args, rank, world, local):
+    """The batch workload as its own line (each rank runs its own batch: weak
+    scaling)."""
+    m = batch_measurement(args, local)
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        achieved = value * 256.0 / 1e9
+        achieved = m["value"] * 256.0 / 1e9
         line = {
-            "metric": "total cell-updates/s of a 512-case batch on 1 B200", "value": world * value, "unit": UNIT,
-            "n_gpus": world, "steps": int(steps.max()), "warmup": args.warmup, "ms_per_step": ms / steps.max(),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32-flux/f64-state",
-            "data": "synthetic",
-            "config": {"workload": "512 cases, n log-uniform in [32,512] (23.4 M cells): 256 periodic vortices to "
-                                   "t=1, 256 four-quadrant Riemann problems to t=0.05; MUSCL-minmod + HLLC-Thornber, "
-                                   "SSP-RK3, CFL 0.4, FP32 fluxes + FP64 state",
-                       "cases": len(grids), "cells": int(cells.sum()), "cell_updates": work,
+            "metric": "total cell-updates/s of a 512-case batch on 1 B200", "value": world * m["value"], "unit": UNIT,
+            "n_gpus": world, "steps": m["steps_max"], "warmup": args.warmup,
+            "ms_per_step": m["batch_ms"] / m["steps_max"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-flux/f64-state", "data": "synthetic",
+            "config": {"workload": m["workload"], "cases": m["cases"], "cells": m["cells"],
+                       "cell_updates": m["cell_updates"],
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": "inputs larger than L2 (2.2 GB of state)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_source": peak_kind,
                          "kernel": "whole batch run (256 algorithmic B per cell-update over the run's device time)"},
             "cpu_baseline": None,
-            "e2e": {"value": world * work / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": h2d, "note": "one 'step' here is the whole batch run"},
-            "gpu_launches": int(launches),
-            "clocks": clocks.summary(),
-            "batch": {"completion_ms_p50": float(np.percentile(comp, 50)),
-                      "completion_ms_p99": float(np.percentile(comp, 99)),
-                      "batch_ms": ms,
-                      "sequential_completion_ms_p50": float(np.percentile(seq_done, 50)),
-                      "sequential_completion_ms_p99": float(np.percentile(seq_done, 99)),
-                      "sequential_s": seq_s, "sequential_value": work / seq_s,
-                      "all_finished": bool(all(r.finished for r in res))},
+            "e2e": {"value": world * m["e2e"]["value"], "unit": UNIT, "h2d_bytes_per_step": m["e2e"]["h2d_bytes"],
+                    "d2h_bytes_per_step": m["e2e"]["d2h_bytes"], "note": "one 'step' here is the whole batch run"},
+            "gpu_launches": m["gpu_launches"],
+            "clocks": m["clocks"],
+            "batch": m,
         }
         print(json.dumps(line), flush=True)
 
@@ -487,6 +516,7 @@ def main():
     ap.add_argument("--workload", default="vortex4096", choices=["vortex4096", "cylinder", "vortex3d", "batch512"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the density-error leg (profiler captures)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 512-case batch leg of the default line")
     ap.add_argument("--size", type=int, default=None,
                     help="vortex workloads only: a smaller n x n (x n) grid of the same case "
                          "(for profiler captures)")
@@ -615,6 +645,14 @@ def main():
     e2e_single *= world
     e2e_multi *= world
 
+    # ---- the batching configuration (512 cases, FP32 fluxes) --------------
+    batch = None
+    if world == 1 and args.workload == "vortex4096" and args.size is None and not args.no_batch:
+        m = batch_measurement(args, local)
+        batch = {k: m[k] for k in ("workload", "value", "unit", "batch_ms", "gpu_launches", "kernel",
+                                    "tuned_rows_per_bucket", "tuned_blocks_per_sm", "completion_ms_p50",
+                                    "completion_ms_p99", "per_stage_launches", "sequential", "e2e", "all_finished")}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = None
@@ -652,6 +690,7 @@ def main():
                                               "copies of one thread overlap kernels of the others"}},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
+            "batch512": batch,
         }
         print(json.dumps(line), flush=True)
 

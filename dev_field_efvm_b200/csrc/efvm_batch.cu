@@ -49,9 +49,21 @@ struct efvm_batch {
     bool tuned = false;
     std::array<int, 4> bucket_rows{{0, 0, 0, 0}};  // 0 = the default heuristic
     cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;               // steps one replay of `graph` runs
     unsigned long long* clock_d = nullptr;
     uint64_t launches = 0;
     std::string err;
+    // the persistent kernel (on by default): one launch per chunk of steps
+    bool persistent = true;
+    int n_sms = 0;
+    int blocks_per_sm = 0;             // resident blocks per SM of its grid (0 = the form's maximum)
+    unsigned int* ready_d = nullptr;   // per case (PersistArgs)
+    unsigned int* done_d = nullptr;
+    int* case_tiles_d = nullptr;
+    unsigned long long* ticket_d = nullptr;
+    int* status_d = nullptr;
+    double wait_s = 2.0;               // limit of one wait in the persistent kernel
+    int stall_case = -1;               // test hook: the next run's table claims one tile too many for this case
 };
 
 namespace {
@@ -84,9 +96,11 @@ int write_states(efvm_batch* b, const std::vector<DevState>& s) {
     return EFVM_OK;
 }
 
-// Tiles of the active cases, case by case: (case, strip, row block).
+// Tiles of the active cases, case by case: (case, strip, row block), and the
+// number of tiles of each case (the persistent kernel's completion counts).
 int build_tiles(efvm_batch* b) {
     std::vector<int4> t;
+    std::vector<int> per_case(b->n, 0);
     for (int k = 0; k < b->n; ++k) {
         if (!b->active[k]) continue;
         const int strips = stage_strips(b->g[k].nx);
@@ -94,7 +108,12 @@ int build_tiles(efvm_batch* b) {
         const int blocks_y = (b->g[k].ny + rows - 1) / rows;
         for (int by = 0; by < blocks_y; ++by)
             for (int sx = 0; sx < strips; ++sx) t.push_back(make_int4(k, sx, by, 0));
+        per_case[k] = strips * blocks_y;
     }
+    // fault injection for the bounded waits: the case's stages can never complete
+    if (b->stall_case >= 0 && b->stall_case < b->n && per_case[b->stall_case] > 0) per_case[b->stall_case] += 1;
+    BATCH_TRY(b, cudaMemcpyAsync(b->case_tiles_d, per_case.data(), b->n * sizeof(int), cudaMemcpyHostToDevice,
+                                 b->stream));
     if ((int)t.size() > b->tiles_cap) {
         if (b->tiles_d) cudaFree(b->tiles_d);
         b->tiles_d = nullptr;
@@ -109,45 +128,58 @@ int build_tiles(efvm_batch* b) {
     return EFVM_OK;
 }
 
-// ---- the autotuner -----------------------------------------------------------
-// Rows per warp is the one tiling choice of the stage kernel that depends on the
-// case size: more rows amortise each strip's first y face, fewer rows give more
-// warps.  Cases are grouped in size buckets (cells < 64^2, < 128^2, < 256^2,
-// larger); for each bucket present the tuner times one batch step with 2, 4 and
-// 8 rows and keeps the fastest, on a copy of the states (restored afterwards, so
-// tuning changes no result).  Choices are cached per process for the device, its
-// SM count, the numerical method and the set of buckets present.
-constexpr int N_BUCKETS = 4;
-constexpr int ROW_CHOICES[3] = {2, 4, 8};
-
-int size_bucket(const Geometry& g) {
-    const long long c = (long long)g.nx * g.ny;
-    return c < 64 * 64 ? 0 : c < 128 * 128 ? 1 : c < 256 * 256 ? 2 : 3;
+int resident_blocks(const efvm_batch* b) {
+    const int form = batch_form_blocks(b->params.precision == EFVM_PREC_FP32_FLUX, b->ph.viscous != 0);
+    return b->blocks_per_sm > 0 ? std::min(b->blocks_per_sm, form) : form;
 }
 
-using TuneKey = std::tuple<int, int, int, int, int, int>;
-std::mutex g_tune_mu;
-std::map<TuneKey, std::array<int, 4>> g_tune_cache;
-
-// One RK3 step of every active case: set-up, then the three stages.
-void enqueue_step(efvm_batch* b) {
-    b->launches += launch_batch_setup(b->ph, b->cases_d, b->n, true, b->stream);
-    const int in_buf[3] = {0, 1, 2}, out_buf[3] = {1, 2, 0};
-    for (int s = 0; s < 3; ++s) {
-        BatchStageArgs a{};
-        a.ph = b->ph;
-        a.cases = b->cases_d;
-        a.tiles = b->tiles_d;
-        a.stage = s;
-        a.completes_step = s == 2;
-        a.want_cfl = s == 2 && b->ph.fixed_dt <= 0.0;
-        a.in_buf = in_buf[s];
-        a.out_buf = out_buf[s];
-        b->launches += launch_batch_stage(a, b->n_tiles, true, b->stream);
+// `steps` RK3 steps of every active case.  Persistent: the first step's set-up,
+// then one launch for all 3 x steps stages (the later set-ups run inside it).
+// Otherwise per step a set-up launch and one launch per stage over the table.
+void enqueue_steps(efvm_batch* b, int steps) {
+    if (b->persistent) {
+        b->launches += launch_batch_setup(b->ph, b->cases_d, b->n, false, b->stream);
+        cudaMemsetAsync(b->ready_d, 0, b->n * sizeof(unsigned int), b->stream);
+        cudaMemsetAsync(b->done_d, 0, b->n * sizeof(unsigned int), b->stream);
+        cudaMemsetAsync(b->ticket_d, 0, sizeof(unsigned long long), b->stream);
+        PersistArgs p{};
+        p.ph = b->ph;
+        p.cases = b->cases_d;
+        p.tiles = b->tiles_d;
+        p.case_tiles = b->case_tiles_d;
+        p.ready = b->ready_d;
+        p.done = b->done_d;
+        p.ticket = b->ticket_d;
+        p.status = b->status_d;
+        p.n_tiles = b->n_tiles;
+        p.rounds = 3 * steps;
+        p.want_cfl = b->ph.fixed_dt <= 0.0;
+        p.wait_ns = (unsigned long long)(b->wait_s * 1e9);
+        b->launches += launch_batch_persistent(p, resident_blocks(b), b->n_sms, b->stream);
+        return;
+    }
+    for (int step = 0; step < steps; ++step) {
+        b->launches += launch_batch_setup(b->ph, b->cases_d, b->n, true, b->stream);
+        const int in_buf[3] = {0, 1, 2}, out_buf[3] = {1, 2, 0};
+        for (int s = 0; s < 3; ++s) {
+            BatchStageArgs a{};
+            a.ph = b->ph;
+            a.cases = b->cases_d;
+            a.tiles = b->tiles_d;
+            a.stage = s;
+            a.completes_step = s == 2;
+            a.want_cfl = s == 2 && b->ph.fixed_dt <= 0.0;
+            a.in_buf = in_buf[s];
+            a.out_buf = out_buf[s];
+            b->launches += launch_batch_stage(a, b->n_tiles, true, b->stream);
+        }
     }
 }
 
-int capture(efvm_batch* b) {
+// Launches per replay of the captured steps.
+uint64_t launches_per_replay(const efvm_batch* b, int steps) { return b->persistent ? 2 : 4ull * steps; }
+
+int capture(efvm_batch* b, int steps) {
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -155,15 +187,42 @@ int capture(efvm_batch* b) {
     const uint64_t before = b->launches;
     cudaGraph_t graph;
     BATCH_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(b);
+    enqueue_steps(b, steps);
     cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
     b->launches = before;
     if (e != cudaSuccess) return bfail(b, EFVM_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&b->graph, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return bfail(b, EFVM_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
+    b->graph_steps = steps;
     return EFVM_OK;
 }
+
+// ---- the autotuner -----------------------------------------------------------
+// Two tiling choices of the batch depend on the case sizes and the device: the
+// tile height (rows per warp; more rows amortise each strip's first y face,
+// fewer give more tiles) per case-size bucket (cells < 64^2, < 128^2, < 256^2,
+// larger), and, for the persistent kernel, its resident blocks per SM.  The
+// tuner times one batch step for each height per bucket present (greedily,
+// bucket by bucket), then each block count, on the live states (restored
+// afterwards, so tuning changes no result), and keeps the fastest.  Choices are
+// cached per process for the device, its SM count, the numerical method, the
+// kernel and the set of buckets present.
+constexpr int N_BUCKETS = 4;
+constexpr int ROW_CHOICES[4] = {2, 4, 8, 16};
+
+int size_bucket(const Geometry& g) {
+    const long long c = (long long)g.nx * g.ny;
+    return c < 64 * 64 ? 0 : c < 128 * 128 ? 1 : c < 256 * 256 ? 2 : 3;
+}
+
+using TuneKey = std::tuple<int, int, int, int, int, int, int>;
+struct TuneChoice {
+    std::array<int, 4> rows;
+    int blocks_per_sm;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune_cache;
 
 // Rows of every case from the per-bucket choice (0 = default), uploaded.
 int apply_rows(efvm_batch* b) {
@@ -181,15 +240,14 @@ int apply_rows(efvm_batch* b) {
 int tune(efvm_batch* b) {
     int present = 0;
     for (int k = 0; k < b->n; ++k) present |= 1 << size_bucket(b->g[k]);
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-    const TuneKey key{b->device, sms, b->params.precision, b->params.flux_scheme * 2 + b->params.reconstruction,
-                      b->params.limiter, present};
+    const TuneKey key{b->device, b->n_sms, b->params.precision, b->params.flux_scheme * 2 + b->params.reconstruction,
+                      b->params.limiter, present, b->persistent ? 1 : 0};
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end()) {
-            b->bucket_rows = it->second;
+            b->bucket_rows = it->second.rows;
+            b->blocks_per_sm = it->second.blocks_per_sm;
             return apply_rows(b);
         }
     }
@@ -200,35 +258,58 @@ int tune(efvm_batch* b) {
     BATCH_TRY(b, cudaMalloc(&backup, pool_bytes));
     std::vector<DevState> saved;
     int rc = read_states(b, saved);
-    if (rc) return rc;
+    if (rc) {
+        cudaFree(backup);
+        return rc;
+    }
     BATCH_TRY(b, cudaMemcpyAsync(backup, b->pool, pool_bytes, cudaMemcpyDeviceToDevice, b->stream));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    // one step with the current choices: warm-up replay, then two timed replays
+    auto trial = [&](float& ms) -> int {
+        int r = apply_rows(b);
+        if (!r) r = build_tiles(b);
+        if (!r) r = capture(b, 1);
+        if (r) return r;
+        cudaGraphLaunch(b->graph, b->stream);
+        cudaEventRecord(e0, b->stream);
+        for (int i = 0; i < 2; ++i) cudaGraphLaunch(b->graph, b->stream);
+        cudaEventRecord(e1, b->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return bfail(b, EFVM_ERR_CUDA, std::string("batch autotune: ") + cudaGetErrorString(e));
+        cudaEventElapsedTime(&ms, e0, e1);
+        return EFVM_OK;
+    };
     for (int bucket = 0; bucket < N_BUCKETS && rc == EFVM_OK; ++bucket) {
         if (!(present & (1 << bucket))) continue;
         float best_ms = 1e30f;
         int best = ROW_CHOICES[0];
         for (int r : ROW_CHOICES) {
             b->bucket_rows[bucket] = r;
-            if ((rc = apply_rows(b)) || (rc = build_tiles(b)) || (rc = capture(b))) break;
-            cudaGraphLaunch(b->graph, b->stream);  // warm-up
-            cudaEventRecord(e0, b->stream);
-            for (int i = 0; i < 2; ++i) cudaGraphLaunch(b->graph, b->stream);
-            cudaEventRecord(e1, b->stream);
-            cudaError_t e = cudaEventSynchronize(e1);
-            if (e != cudaSuccess) {
-                rc = bfail(b, EFVM_ERR_CUDA, std::string("batch autotune: ") + cudaGetErrorString(e));
-                break;
-            }
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
+            if ((rc = trial(ms))) break;
             if (ms < best_ms) {
                 best_ms = ms;
                 best = r;
             }
         }
         b->bucket_rows[bucket] = best;
+    }
+    if (b->persistent && rc == EFVM_OK) {
+        const int form = batch_form_blocks(b->params.precision == EFVM_PREC_FP32_FLUX, b->ph.viscous != 0);
+        float best_ms = 1e30f;
+        int best = form;
+        for (int blocks = form; blocks >= std::max(2, form - 3); --blocks) {
+            b->blocks_per_sm = blocks;
+            float ms = 0.f;
+            if ((rc = trial(ms))) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = blocks;
+            }
+        }
+        b->blocks_per_sm = best;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -237,9 +318,12 @@ int tune(efvm_batch* b) {
     cudaFree(backup);
     if (rc) return rc;
     if (rc2) return rc2;
+    int status = 0;
+    BATCH_TRY(b, cudaMemcpy(&status, b->status_d, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return bfail(b, EFVM_ERR_TIMEOUT, "batch autotune: a wait of the persistent kernel ran out");
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tune_cache[key] = b->bucket_rows;
+        g_tune_cache[key] = TuneChoice{b->bucket_rows, b->blocks_per_sm};
     }
     return apply_rows(b);
 }
@@ -302,6 +386,14 @@ int efvm_batch_create(const efvm_grid* grids, int32_t n_cases, const efvm_params
         return cleanup(bfail(nullptr, EFVM_ERR_OOM, "efvm_batch_create: cudaMalloc"));
     if (cudaMalloc(&b->clock_d, sizeof(unsigned long long)) != cudaSuccess)
         return cleanup(bfail(nullptr, EFVM_ERR_OOM, "efvm_batch_create: cudaMalloc"));
+    if (cudaMalloc(&b->ready_d, n_cases * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc(&b->done_d, n_cases * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc(&b->case_tiles_d, n_cases * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->ticket_d, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&b->status_d, sizeof(int)) != cudaSuccess)
+        return cleanup(bfail(nullptr, EFVM_ERR_OOM, "efvm_batch_create: cudaMalloc"));
+    cudaMemsetAsync(b->status_d, 0, sizeof(int), b->stream);
+    cudaDeviceGetAttribute(&b->n_sms, cudaDevAttrMultiProcessorCount, b->device);
     std::vector<double> yw_all;
     yw_all.reserve(yw_total);
     b->cases.resize(n_cases);
@@ -347,6 +439,11 @@ int efvm_batch_destroy(efvm_batch* b) {
     cudaFree(b->tiles_d);
     cudaFree(b->staging);
     cudaFree(b->clock_d);
+    cudaFree(b->ready_d);
+    cudaFree(b->done_d);
+    cudaFree(b->case_tiles_d);
+    cudaFree(b->ticket_d);
+    cudaFree(b->status_d);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return EFVM_OK;
@@ -441,25 +538,47 @@ int efvm_batch_run(efvm_batch* b, const double* t_stop, int64_t max_steps, int64
     rc = write_states(b, s);
     if (rc) return rc;
     if (b->autotune && !b->tuned) {
+        const int stall = b->stall_case;  // an injected stall is for the run, not the tuning steps
+        b->stall_case = -1;
         rc = tune(b);
+        b->stall_case = stall;
         if (rc) return rc;
         b->tuned = true;
     }
     b->launches += launch_clock(b->clock_d, b->stream);
     rc = build_tiles(b);
     if (rc) return rc;
-    rc = capture(b);
-    if (rc) return rc;
+    // the persistent kernel runs a chunk of steps per replay; otherwise one step
+    const int64_t per_replay_max = b->persistent ? chunk : 1;
     int64_t done = 0;
+    bool recapture = true;
     while (done < max_steps) {
         const int64_t m = std::min<int64_t>(chunk, max_steps - done);
-        for (int64_t i = 0; i < m; ++i) {
-            BATCH_TRY(b, cudaGraphLaunch(b->graph, b->stream));
-            b->launches += 4;
+        const int steps = (int)std::min<int64_t>(m, per_replay_max);
+        if (recapture || b->graph_steps != steps) {
+            rc = capture(b, steps);
+            if (rc) return rc;
+            recapture = false;
         }
-        done += m;
+        for (int64_t i = 0; i < m / steps; ++i) {
+            BATCH_TRY(b, cudaGraphLaunch(b->graph, b->stream));
+            b->launches += launches_per_replay(b, steps);
+        }
+        done += (m / steps) * steps;
         rc = read_states(b, s);
         if (rc) return rc;
+        if (b->persistent) {
+            int status = 0;
+            BATCH_TRY(b, cudaMemcpyAsync(&status, b->status_d, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+            BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+            if (status) {
+                b->stall_case = -1;
+                cudaMemsetAsync(b->status_d, 0, sizeof(int), b->stream);
+                cudaStreamSynchronize(b->stream);
+                return bfail(b, EFVM_ERR_TIMEOUT,
+                             "a wait of the persistent batch kernel ran out; the cases' states are partly advanced");
+            }
+        }
         bool changed = false, any = false;
         for (int k = 0; k < b->n; ++k) {
             const char a = s[k].active ? 1 : 0;
@@ -471,10 +590,10 @@ int efvm_batch_run(efvm_batch* b, const double* t_stop, int64_t max_steps, int64
         if (changed) {
             rc = build_tiles(b);
             if (rc) return rc;
-            rc = capture(b);
-            if (rc) return rc;
+            recapture = true;
         }
     }
+    b->stall_case = -1;
     unsigned long long start = 0;
     BATCH_TRY(b, cudaMemcpyAsync(&start, b->clock_d, sizeof(start), cudaMemcpyDeviceToHost, b->stream));
     BATCH_TRY(b, cudaStreamSynchronize(b->stream));
@@ -505,6 +624,7 @@ int efvm_batch_set_autotune(efvm_batch* b, int32_t enable) {
     b->autotune = enable != 0;
     if (!b->autotune) {
         b->bucket_rows = {{0, 0, 0, 0}};
+        b->blocks_per_sm = 0;
         b->tuned = false;
         return apply_rows(b);
     }
@@ -514,6 +634,41 @@ int efvm_batch_set_autotune(efvm_batch* b, int32_t enable) {
 int efvm_batch_get_rows(efvm_batch* b, int32_t rows[4]) {
     if (!b || !rows) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
     for (int i = 0; i < 4; ++i) rows[i] = b->bucket_rows[i];
+    return EFVM_OK;
+}
+
+int efvm_batch_set_persistent(efvm_batch* b, int32_t enable) {
+    if (!b) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
+    b->persistent = enable != 0;
+    b->tuned = false;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return EFVM_OK;
+}
+
+int efvm_batch_set_wait_limit(efvm_batch* b, double seconds) {
+    if (!b || !(seconds > 0.0) || seconds > 60.0)
+        return bfail(b, EFVM_ERR_INVALID_ARG, "efvm_batch_set_wait_limit: need 0 < seconds <= 60");
+    b->wait_s = seconds;
+    if (b->graph) {  // the limit is a kernel argument of the captured launch
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return EFVM_OK;
+}
+
+int efvm_batch_inject_stall(efvm_batch* b, int32_t k) {
+    if (!b) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
+    if (k < 0 || k >= b->n) return bfail(b, EFVM_ERR_INVALID_ARG, "case index out of range");
+    b->stall_case = k;
+    return EFVM_OK;
+}
+
+int efvm_batch_get_blocks_per_sm(efvm_batch* b, int32_t* out) {
+    if (!b || !out) return bfail(b, EFVM_ERR_INVALID_ARG, "null argument");
+    *out = resident_blocks(b);
     return EFVM_OK;
 }
 

@@ -225,6 +225,32 @@ struct BatchStageArgs {
     int in_buf, out_buf;    // U[in_buf] -> U[out_buf]; U[0] is u^n
 };
 
+// One launch of the persistent batch kernel: every warp takes work tickets in
+// order; ticket t is RK stage r = t / n_tiles (3 per step) of table tile
+// t % n_tiles.  A tile of stage r > 0 waits until its case's stage r - 1 is
+// complete (ready[k] >= r; no wait on any other case), the last tile of a
+// case's stage publishes it, and the last tile of a step's third stage runs
+// that case's next set-up first.  A case that stops publishes ~0u, so its later
+// tiles pass at once and skip.  Waits are bounded by wait_ns: a wait that runs
+// out sets status bit 0 and the launch winds down (EFVM_ERR_TIMEOUT).
+struct PersistArgs {
+    Physics ph;                      // the shared settings (scheme, precision, gas, CFL)
+    const BatchCase* __restrict__ cases;
+    const int4* tiles;               // (case, strip, row block, 0) of every case in the table
+    const int* case_tiles;           // per case: its tiles in the table
+    unsigned int* ready;             // per case: stages of this launch complete
+    unsigned int* done;              // per case: tiles completed in this launch
+    unsigned long long* ticket;      // the next work ticket
+    int* status;
+    long long n_tiles;
+    int rounds;                      // RK stages this launch runs (3 per step)
+    int want_cfl;
+    unsigned long long wait_ns;
+};
+int launch_batch_persistent(const PersistArgs& p, int blocks_per_sm, int n_sms, void* stream);
+// Resident blocks per SM of the batch stage forms (their register budget).
+int batch_form_blocks(bool fp32, bool viscous);
+
 // Stage-kernel tiling of one case: strips of columns, and rows per warp for a
 // case that runs alone (fp32: the FP32-flux form; viscous: with viscous terms).
 int stage_strips(int nx);

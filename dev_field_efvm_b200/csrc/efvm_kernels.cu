@@ -22,6 +22,7 @@
 // 15-25 % of their peak.  No tensor cores are involved.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -59,6 +60,18 @@ struct U4 {
 
 __device__ __forceinline__ U4 load4(const double* q, long long plane, long long o) {
     return U4{q[o], q[plane + o], q[2 * plane + o], q[3 * plane + o]};
+}
+// Loads of a stage's inputs.  CG: through L2 only (ld.global.cg), for the
+// persistent batch kernel, whose inputs were written earlier in the same launch
+// by other blocks (an L1 line of this SM could still hold an older value).
+template <bool CG>
+__device__ __forceinline__ double gld(const double* p) {
+    if constexpr (CG) return __ldcg(p);
+    else return *p;
+}
+template <bool CG>
+__device__ __forceinline__ U4 load4g(const double* q, long long plane, long long o) {
+    return U4{gld<CG>(q + o), gld<CG>(q + plane + o), gld<CG>(q + 2 * plane + o), gld<CG>(q + 3 * plane + o)};
 }
 __device__ __forceinline__ void store4(double* q, long long plane, long long o, const U4& u) {
     q[o] = u.r;
@@ -170,6 +183,11 @@ __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& p
 // buffer, or the external slot that slabs max-reduce across GPUs.
 __device__ __forceinline__ unsigned long long* lam_slot(DevState* st) {
     return st->ext_lam ? &st->lam_ext : &st->lam[st->lam_idx];
+}
+// The same slot, its selectors read coherently (the persistent batch kernel).
+__device__ __forceinline__ unsigned long long* lam_slot_v(DevState* st) {
+    const volatile DevState* v = st;
+    return v->ext_lam ? &st->lam_ext : &st->lam[v->lam_idx];
 }
 
 // Local max wave speed of cfl_system, crates/cfd_solver/src/lib.rs:647-669.
@@ -298,27 +316,32 @@ constexpr int WPB = 4;     // warps per block
 // on a step's last stage, the sponge, refills the boundary ghosts of the output
 // and takes the wave-speed max for the next step's CFL dt.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true>
+template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true, bool CG = false>
 __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
-    if (!a.st->active) return;
+    if (!(CG ? *(volatile const int*)&a.st->active : a.st->active)) return;
     const Geometry& g = a.g;
     const Physics& ph = a.ph;
     const long long P = g.plane;
     const int lane = threadIdx.x & 31;
     if (strip == 0 && by == 0 && lane == 0) {
         // RK state machine and clock of update_system, crates/cfd_solver/src/lib.rs:607-621
-        // (no other thread reads time/step/rk_stage during this kernel)
-        DevState* st = a.st;
-        if (a.stage >= 2) {
-            st->rk_stage = 0;
-            st->completed = 1;
-            st->step += 1;
-            st->time += st->dt;
-            if (a.defer_forces) st->forces_pending = 1;
-        } else {
-            st->rk_stage = a.stage + 1;
-            st->completed = 0;
-        }
+        // (no other thread reads time/step/rk_stage during this stage)
+        auto machine = [&](auto* st) {
+            if (a.stage >= 2) {
+                st->rk_stage = 0;
+                st->completed = 1;
+                st->step += 1;
+                st->time += st->dt;
+                if (a.defer_forces) st->forces_pending = 1;
+            } else {
+                st->rk_stage = a.stage + 1;
+                st->completed = 0;
+            }
+        };
+        // the persistent batch kernel's set-up writes the state from other blocks
+        // during the launch: coherent (volatile) accesses there
+        if constexpr (CG) machine((volatile DevState*)a.st);
+        else machine(a.st);
     }
     const int i0 = strip * STRIP;
     const int jb = by * rows;
@@ -334,9 +357,9 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
         const double gm1 = ph.gamma - 1.0;
         const R rg = R(ph.gamma), rgm1 = R(gm1);
         const double* __restrict__ uin = a.uin;
-        auto ld = [&](int ii, int jj) { return load4(uin, P, cidx(g, ii, jj)); };
+        auto ld = [&](int ii, int jj) { return load4g<CG>(uin, P, cidx(g, ii, jj)); };
         const double* __restrict__ colp = uin + cidx(g, ic, 0);  // this lane's column at row 0
-        auto ldrow = [&](int jj) { return toR<R>(load4(colp, P, (long long)jj * g.pitch)); };
+        auto ldrow = [&](int jj) { return toR<R>(load4g<CG>(colp, P, (long long)jj * g.pitch)); };
 
         // Reconstruction flags of the faces on the domain edge; every interior
         // face reconstructs both sides under MUSCL.  x: this lane's face, between
@@ -364,19 +387,21 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
             V4<R> unused;
             slope_faces(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
         }
-        const double dt = a.st->dt;  // set by the step's set-up, constant during the stage
-        Q4<R> gb;
+        const double dt = gld<CG>(&a.st->dt);  // set by the step's set-up, constant during the stage
+        Q4<R> gb{R(0), R(0), R(0), R(0)};
         for (int j = jb - 1; j < je; ++j) {
             const V4<R> un2 = ldrow(j + 2);
             const bool row = j >= jb;  // warp-uniform: the first pass only forms the face below row jb
 
             // ---- x-face on the left of column i, row j, and the divergence of
             // the faces below, left and right of the cell ----
-            // Flux divergence in the reference's accumulation order: the face
-            // below (scattered when row j-1 was visited), the face on the left,
-            // then the cell's own +x and +y faces (for_each_face order,
-            // crates/cfd_solver/src/lib.rs:333-337).  Only these four partial
-            // sums stay live through the y-face flux below.
+            // Flux divergence, (F_left - F_right) / dx + (G_below - G_above) / dy
+            // per conserved variable: the sum of the four face terms that
+            // muscl_flux_system scatters into the cell (crates/cfd_solver/src/lib.rs:
+            // 333-337), formed as two differences (exact for the nearly equal
+            // fluxes of neighbouring faces) and one multiply-add, a few ulps from
+            // the reference's sequential sum.  Only the x part stays live through
+            // the y-face flux below.
             double part[4];
             auto x_face = [&]() {
                 V4<R> ul = shfl_up_v(uc, 1), ur = shfl_down_v(uc, 1);
@@ -402,32 +427,29 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 const Q4<R> fxr = shfl_down_q(fx, 1);  // face on the right of column i
                 const double fl[4] = {(double)fx.r, (double)fx.mn, (double)fx.mt, (double)fx.E};
                 const double fr[4] = {(double)fxr.r, (double)fxr.mn, (double)fxr.mt, (double)fxr.E};
-                const double gbv[4] = {(double)gb.r, (double)gb.mt, (double)gb.mn, (double)gb.E};
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    double acc = __dmul_rn(gbv[v], g.inv_y);
-                    acc = __dadd_rn(acc, __dmul_rn(fl[v], g.inv_x));
-                    part[v] = __dsub_rn(acc, __dmul_rn(fr[v], g.inv_x));
-                }
+                for (int v = 0; v < 4; ++v) part[v] = (fl[v] - fr[v]) * g.inv_x;
             };
-            if (XFIRST && row) x_face();
-
-            // ---- y-face above row j ----
             Q4<R> gt;
             V4<R> pn = un;  // +y face state of row j+1
+            // faces on the domain's y edges; an edge between slabs is an interior face
+            auto y_edge_rec = [&](bool& rb, bool& rt) {
+                const bool lo_edge = j == -1 && (!ph.halo_ylo || ph.seam_ylo);
+                const bool hi_edge = j + 1 == g.ny && (!ph.halo_yhi || ph.seam_yhi);
+                rb = lo_edge ? seam_rec : (hi_edge ? edge_rec : true);
+                rt = lo_edge ? edge_rec : (hi_edge ? seam_rec : true);
+            };
+            if (XFIRST && row) x_face();
+            // ---- y-face above row j ----
             if (MUSCL) {
                 V4<R> mn;
                 slope_faces(ph.limiter, uc, un, un2, pn, mn);
-                // faces on the domain's y edges; an edge between slabs is an interior face
-                const bool lo_edge = j == -1 && (!ph.halo_ylo || ph.seam_ylo);
-                const bool hi_edge = j + 1 == g.ny && (!ph.halo_yhi || ph.seam_yhi);
-                const bool rb = lo_edge ? seam_rec : (hi_edge ? edge_rec : true);
-                const bool rt = lo_edge ? edge_rec : (hi_edge ? seam_rec : true);
+                bool rb, rt;
+                y_edge_rec(rb, rt);
                 gt = face_flux<SCHEME, R>(yq(rb ? pc : uc), yq(rt ? mn : un), rg, rgm1);
             } else {
                 gt = face_flux<SCHEME, R>(yq(uc), yq(un), rg, rgm1);
             }
-
             if (!XFIRST && row) x_face();
 
             if (row && owner) {
@@ -435,9 +457,10 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                 // the cell's state in FP64 (the FP32 path reads it again)
                 const U4 ucd = FP64 ? toU4(uc) : ld(i, j);
                 const double gtv[4] = {(double)gt.r, (double)gt.mt, (double)gt.mn, (double)gt.E};
+                const double gbd[4] = {(double)gb.r, (double)gb.mt, (double)gb.mn, (double)gb.E};
                 double rhs[4];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) rhs[v] = __dsub_rn(part[v], __dmul_rn(gtv[v], g.inv_y));
+                for (int v = 0; v < 4; ++v) rhs[v] = fma(gbd[v] - gtv[v], g.inv_y, part[v]);
                 if constexpr (CORR) {
                     // learned corrections of the four faces (periodic grid): the
                     // x face on the left of a cell, the y face below it
@@ -464,9 +487,10 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     bool sn[4];
 #pragma unroll
                     for (int k = 0; k < 4; ++k) sn[k] = ibm && a.mask[no[k]];
-                    const double r0 = ucd.r, r1 = sn[0] ? 1.0 : uin[no[0]], r2 = sn[1] ? 1.0 : uin[no[1]];
-                    const double r3 = sn[2] ? 1.0 : (FP64 ? (double)un.r : uin[no[2]]);
-                    const double r4 = sn[3] ? 1.0 : uin[no[3]];
+                    const double r0 = ucd.r, r1 = sn[0] ? 1.0 : gld<CG>(uin + no[0]),
+                                 r2 = sn[1] ? 1.0 : gld<CG>(uin + no[1]);
+                    const double r3 = sn[2] ? 1.0 : (FP64 ? (double)un.r : gld<CG>(uin + no[2]));
+                    const double r4 = sn[3] ? 1.0 : gld<CG>(uin + no[3]);
                     const double p1 = r0 * r1, p2 = p1 * r2, p3 = p2 * r3;
                     double w = rcp_(p3 * r4);
                     const double i4 = p3 * w;
@@ -490,9 +514,9 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                             q = toU4(un);
                         } else {
                             q.r = rn[k];
-                            q.mx = uin[P + no[k]];
-                            q.my = uin[2 * P + no[k]];
-                            q.E = uin[3 * P + no[k]];
+                            q.mx = gld<CG>(uin + P + no[k]);
+                            q.my = gld<CG>(uin + 2 * P + no[k]);
+                            q.E = gld<CG>(uin + 3 * P + no[k]);
                         }
                         prim_uvt(q, ninv[k], gm1, ph.inv_r_gas, vu, vv, t);
                     };
@@ -531,19 +555,18 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     rhs[3] += ph.body_force_x * ucd.mx;
                 }
 
-                // Rk3Integrator / EulerIntegrator::substep, crates/cfd_solver/src/integrate.rs:48-101
+                // Rk3Integrator / EulerIntegrator::substep, crates/cfd_solver/src/integrate.rs:48-101,
+                // with multiply-adds: u + dt r, then w0 u0 + w1 (u + dt r)
                 const double ucv[4] = {ucd.r, ucd.mx, ucd.my, ucd.E};
                 double un_[4];
                 if (a.stage == 1 || a.stage == 2) {
                     const double w0 = a.stage == 1 ? 0.75 : (1.0 / 3.0);
                     const double w1 = a.stage == 1 ? 0.25 : (2.0 / 3.0);
 #pragma unroll
-                    for (int v = 0; v < 4; ++v)
-                        un_[v] = __dadd_rn(__dmul_rn(w0, a.u0[v * P + o]),
-                                           __dmul_rn(w1, __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt))));
+                    for (int v = 0; v < 4; ++v) un_[v] = fma(w1, fma(rhs[v], dt, ucv[v]), w0 * gld<CG>(a.u0 + v * P + o));
                 } else {
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) un_[v] = __dadd_rn(ucv[v], __dmul_rn(rhs[v], dt));
+                    for (int v = 0; v < 4; ++v) un_[v] = fma(rhs[v], dt, ucv[v]);
                 }
                 U4 nw{un_[0], un_[1], un_[2], un_[3]};
 
@@ -572,11 +595,15 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
 
                 // non-physical state flag (rho<=0, p<=0, NaN)
                 // p > 0 with rho > 0 is 2 E rho > m^2 (no division)
+                // (a NaN in any component fails one of the two tests, so the NaN
+                // bit is only looked at once a test has failed)
                 int bad = 0;
                 if (!(nw.r > 0.0)) bad |= 1;
                 if (!(2.0 * nw.E * nw.r > nw.mx * nw.mx + nw.my * nw.my)) bad |= 2;
-                if (nw.r != nw.r || nw.mx != nw.mx || nw.my != nw.my || nw.E != nw.E) bad |= 4;
-                if (bad) atomicOr(&a.st->nonphysical, bad);
+                if (bad) {
+                    if (nw.r != nw.r || nw.mx != nw.mx || nw.my != nw.my || nw.E != nw.E) bad |= 4;
+                    atomicOr(&a.st->nonphysical, bad);
+                }
 
                 if (a.completes_step && a.want_cfl) lam = fmax(lam, wave_speed(g, ph, nw));
             }
@@ -590,7 +617,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
     if (a.completes_step && a.want_cfl) {
         for (int o = 16; o > 0; o >>= 1) lam = fmax(lam, __shfl_xor_sync(0xffffffffu, lam, o));
         if (lane == 0 && lam > 0.0 && lam == lam)
-            atomicMax(lam_slot(a.st), (unsigned long long)__double_as_longlong(lam));
+            atomicMax(CG ? lam_slot_v(a.st) : lam_slot(a.st), (unsigned long long)__double_as_longlong(lam));
     }
 }
 
@@ -657,7 +684,8 @@ __global__ void reset_lam_kernel(DevState* st) {
 // crates/cfd_solver/src/lib.rs:671-676) or fixed_dt, and the stop test of the
 // case drivers' `if t >= T_FINAL break`.
 // The stop rule of step_setup: a non-physical state or t >= t_stop ends the run.
-__device__ __forceinline__ bool step_stops(const DevState* st) {
+template <class S>
+__device__ __forceinline__ bool step_stops(S* st) {
     return st->nonphysical || (st->stop_at_t && st->time >= st->t_stop);
 }
 
@@ -670,7 +698,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-__device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
+// S = DevState, or volatile DevState where other blocks of the same launch
+// write the state (the persistent batch kernel).
+template <class S>
+__device__ __forceinline__ void step_setup(const Physics& ph, S* st) {
     if (step_stops(st)) {
         st->active = 0;
         st->done_ns = global_ns();
@@ -680,7 +711,8 @@ __device__ __forceinline__ void step_setup(const Physics& ph, DevState* st) {
     if (ph.fixed_dt > 0.0) {
         dt = ph.fixed_dt;
     } else {
-        const double lam = __longlong_as_double((long long)*lam_slot(st));
+        const unsigned long long bits = st->ext_lam ? st->lam_ext : st->lam[st->lam_idx];
+        const double lam = __longlong_as_double((long long)bits);
         dt = lam > 0.0 ? ph.cfl / lam : INFINITY;
     }
     st->dt = dt;
@@ -709,6 +741,85 @@ __global__ void batch_setup_kernel(Physics ph, const BatchCase* cases, int n) {
 }
 
 __global__ void clock_kernel(unsigned long long* out) { *out = global_ns(); }
+
+
+// ---- the persistent batch kernel -------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Spin (one lane) until *flag >= target.  Bounded: the device global timer
+// limits the wait to limit_ns, and a wait that sees another warp's give-up in
+// *status stops too.  Returns false when it gave up.
+__device__ __forceinline__ bool wait_at_least(const unsigned* flag, unsigned target, unsigned long long limit_ns,
+                                              int* status) {
+    if (ld_acquire_u32(flag) >= target) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned n = 1;; ++n) {
+        __nanosleep(64);
+        if (ld_acquire_u32(flag) >= target) return true;
+        if ((n & 15u) == 0u) {
+            if (*(volatile int*)status) return false;
+            if (global_ns() - t0 > limit_ns || n > (1u << 30)) {
+                atomicOr(status, 1);
+                return false;
+            }
+        }
+    }
+}
+
+// Every warp runs tiles of the table in ticket order until the launch's stages
+// are used up (PersistArgs).  Tickets are taken only by running warps and a
+// tile waits only for tiles of lower tickets (its case's previous stage), so
+// the waits end whatever the number of resident blocks; the kernel has no block
+// barrier.  The stage inputs were written earlier in the same launch by other
+// blocks, so they are loaded through L2 (stage_strip with CG).
+template <int SCHEME, int RECON, class R, int MINB, bool VISC, bool XFIRST>
+__global__ void __launch_bounds__(32 * WPB, MINB) batch_persistent_kernel(PersistArgs p) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long total = (unsigned long long)p.rounds * (unsigned long long)p.n_tiles;
+    for (;;) {
+        unsigned long long t = total;
+        if (lane == 0 && !*(volatile int*)p.status) t = atomicAdd(p.ticket, 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) return;
+        const int r = (int)(t / (unsigned long long)p.n_tiles);
+        const int4 tile = p.tiles[t - (unsigned long long)r * (unsigned long long)p.n_tiles];
+        const int k = tile.x;
+        if (r > 0) {
+            int ok = 1;
+            if (lane == 0) ok = wait_at_least(p.ready + k, (unsigned)r, p.wait_ns, p.status);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) return;
+            (void)ld_acquire_u32(p.ready + k);  // each lane orders its own loads after the publication
+        }
+        const BatchCase& c = p.cases[k];
+        const int stage = r % 3;
+        const BatchView v{c.g, c.ph, c.U[stage], c.U[0], c.U[stage == 2 ? 0 : stage + 1], nullptr, c.yw, c.st,
+                          stage, stage == 2, stage == 2 && p.want_cfl, nullptr, 0};
+        stage_strip<SCHEME, RECON, R, VISC, BatchView, false, XFIRST, true>(v, c.rows, tile.y, tile.z);
+        __threadfence();  // this lane's results before the count below
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) last = atomicAdd(p.done + k, 1u) + 1u == (unsigned)(r + 1) * (unsigned)p.case_tiles[k];
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && lane == 0) {
+            __threadfence();
+            unsigned next = (unsigned)(r + 1);
+            // the case's next step: its set-up, or its end (the set-up of the step
+            // after the launch's last stage is the next launch's first work)
+            if (stage == 2 && r + 1 < p.rounds) {
+                volatile DevState* st = c.st;
+                if (st->active) step_setup(c.ph, st);
+                if (!st->active) next = ~0u;
+                __threadfence();
+            }
+            atomicMax(p.ready + k, next);
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Halo + Boundary for a whole state (after upload / geometry changes)
@@ -1284,6 +1395,46 @@ int launch_batch_stage(const BatchStageArgs& b, int n_tiles, bool pdl, void* str
     cudaStream_t s = (cudaStream_t)stream;
     if (b.ph.precision == EFVM_PREC_FP32_FLUX) launch_batch_r<float>(b, n_tiles, pdl, s);
     else launch_batch_r<double>(b, n_tiles, pdl, s);
+    return 1;
+}
+
+template <int SCHEME, int RECON, class R, bool VISC>
+static void launch_persist_f(const PersistArgs& p, int blocks, cudaStream_t s) {
+    using F = StageForm<R, VISC>;
+    launch_k(batch_persistent_kernel<SCHEME, RECON, R, F::MINB, VISC, F::XFIRST>, dim3(blocks), dim3(32 * WPB), s,
+             false, p);
+}
+
+template <class R>
+static void launch_persist_r(const PersistArgs& p, int blocks, cudaStream_t s) {
+    const bool muscl = p.ph.reconstruction == EFVM_RECON_MUSCL;
+    const bool visc = p.ph.viscous != 0;
+#define EFVM_PERSIST_V(S, RC)                                                   \
+    (visc ? launch_persist_f<S, RC, R, true>(p, blocks, s) : launch_persist_f<S, RC, R, false>(p, blocks, s))
+    switch (p.ph.flux_scheme) {
+        case EFVM_FLUX_RUSANOV:
+            muscl ? EFVM_PERSIST_V(EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL) : EFVM_PERSIST_V(EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER);
+            break;
+        case EFVM_FLUX_HLLC_TEXTBOOK:
+            muscl ? EFVM_PERSIST_V(EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL)
+                  : EFVM_PERSIST_V(EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER);
+            break;
+        default:
+            muscl ? EFVM_PERSIST_V(EFVM_FLUX_HLLC, EFVM_RECON_MUSCL) : EFVM_PERSIST_V(EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER);
+    }
+#undef EFVM_PERSIST_V
+}
+
+int batch_form_blocks(bool fp32, bool viscous) { return form_minb(fp32, viscous); }
+
+// One block per resident slot (blocks_per_sm on every SM): the warps take their
+// work from the ticket counter, so the grid does not depend on the table.
+int launch_batch_persistent(const PersistArgs& p, int blocks_per_sm, int n_sms, void* stream) {
+    if (p.n_tiles <= 0 || p.rounds <= 0) return 0;
+    const int blocks = std::max(1, blocks_per_sm) * std::max(1, n_sms);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (p.ph.precision == EFVM_PREC_FP32_FLUX) launch_persist_r<float>(p, blocks, s);
+    else launch_persist_r<double>(p, blocks, s);
     return 1;
 }
 

@@ -29,28 +29,28 @@ __device__ __forceinline__ float fmin_(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ double fabs_(double a) { return fabs(a); }
 __device__ __forceinline__ float fabs_(float a) { return fabsf(a); }
 
-// Reciprocal by Newton-Raphson iteration on f(r) = 1/r - b, r <- r + r (1 - b r),
-// seeded with the PTX approximate reciprocal rcp.approx.ftz.f64 (about 20
-// correct bits): two iterations square the relative error twice, to within an
-// ulp or two of 1/b.  Branch-free; denormals flush to zero (the flow states
-// here are far from that range).
+// Reciprocal from the PTX approximate reciprocal rcp.approx.ftz.f64 (a seed r0
+// with relative error e = 1 - b r0 of about 2^-22) and one third-order step of
+// the series 1/b = r0 / (1 - e) = r0 (1 + e + e^2 + ...): r0 + r0 (e + e^2)
+// leaves a relative error of e^3 (about 2^-66) before the final rounding, the
+// accuracy of two Newton steps at one operation less.  Branch-free; denormals
+// flush to zero (the flow states here are far from that range).
 __device__ __forceinline__ double rcp_(double b) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
-    double e = fma(-b, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-b, r, 1.0);
-    return fma(r, e, r);
+    const double e = fma(-b, r, 1.0);
+    return fma(r, fma(e, e, e), r);
 }
 __device__ __forceinline__ float rcp_(float b) { return __fdividef(1.0f, b); }
-// 1/sqrt(x) by Newton-Raphson on f(y) = 1/y^2 - x, y <- y (3/2 - x y^2 / 2),
-// seeded with the PTX approximate rsqrt.approx.ftz.f64; two iterations.
+// 1/sqrt(x) from the PTX approximate rsqrt.approx.ftz.f64 seed y0 and one
+// third-order step of the binomial series 1/sqrt(x) = y0 (1 - e)^(-1/2) with
+// e = 1 - x y0^2: y0 + y0 e (1/2 + 3e/8), relative error about 5e^3/16 before
+// rounding (the seed's e is about 2^-21), as accurate as two Newton steps.
 __device__ __forceinline__ double rsqrt_(double x) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double h = 0.5 * x;
-    y = y * fma(-h * y, y, 1.5);
-    return y * fma(-h * y, y, 1.5);
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y * e, fma(e, 0.375, 0.5), y);
 }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 // The smallest normal value: the .ftz seeds above flush anything below it to

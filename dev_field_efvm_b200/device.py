@@ -27,6 +27,7 @@ EXPORTS = (
     "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
     "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
+    "efvm_batch_set_persistent", "efvm_batch_set_wait_limit", "efvm_batch_inject_stall", "efvm_batch_get_blocks_per_sm",
     "efvm_nn_gemm_bf16", "efvm_body_loads", "efvm_output_fields", "efvm_synchronize", "efvm_write_vtk", "efvm_nn_param_count", "efvm_nn_create",
     "efvm_nn_destroy", "efvm_nn_get_params", "efvm_nn_set_params", "efvm_nn_get_scale", "efvm_nn_forward",
     "efvm_nn_loss_grad", "efvm_nn_adam", "efvm_set_flux_correction", "efvm_correction_stats", "efvm_cfl_dt_noalloc",
@@ -93,6 +94,10 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_batch_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_batch_set_autotune.argtypes = [vp, i32]
     L.efvm_batch_get_rows.argtypes = [vp, C.POINTER(C.c_int32)]
+    L.efvm_batch_set_persistent.argtypes = [vp, i32]
+    L.efvm_batch_set_wait_limit.argtypes = [vp, C.c_double]
+    L.efvm_batch_inject_stall.argtypes = [vp, i32]
+    L.efvm_batch_get_blocks_per_sm.argtypes = [vp, C.POINTER(C.c_int32)]
     L.efvm_nn_gemm_bf16.argtypes = [vp, vp, vp, i32, i32, i32, vp]
     L.efvm_body_loads.argtypes = [vp, i32, dp]
     L.efvm_output_fields.argtypes = [vp, dp, i32]
@@ -424,6 +429,20 @@ class Batch:
         r = (C.c_int32 * 4)()
         self._check(self.L.efvm_batch_get_rows(self.h, r))
         return list(r)
+
+    def set_persistent(self, enable: bool) -> None:
+        self._check(self.L.efvm_batch_set_persistent(self.h, int(enable)))
+
+    def set_wait_limit(self, seconds: float) -> None:
+        self._check(self.L.efvm_batch_set_wait_limit(self.h, float(seconds)))
+
+    def inject_stall(self, k: int) -> None:
+        self._check(self.L.efvm_batch_inject_stall(self.h, int(k)))
+
+    def blocks_per_sm(self) -> int:
+        v = C.c_int32()
+        self._check(self.L.efvm_batch_get_blocks_per_sm(self.h, C.byref(v)))
+        return v.value
 
 
 class FluxNet:

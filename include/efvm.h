@@ -393,11 +393,17 @@ int efvm_wave_speed_slot(efvm_ctx* ctx, uint64_t** dev_slot);
 /* ---- batches of independent cases ---------------------------------------- */
 
 /* A batch advances many independent cases (an ensemble or a parameter sweep;
- * the reference runs one App per case) together: per RK3 step one set-up
- * launch for all cases and one launch per stage over the strips of every
- * running case, each case with its own grid, boundary conditions, CFL dt,
- * clock and stop time.  All cases share one efvm_params (RK3 only); IBM
- * cylinders are not supported in a batch. */
+ * the reference runs one App per case) together, each case with its own grid,
+ * boundary conditions, CFL dt, clock and stop time.  By default one persistent
+ * kernel launch runs a whole chunk of RK3 steps of every running case: its
+ * warps take the tiles of all cases from one packed queue, a tile waits only
+ * for its own case's previous stage, and the last tile of a case's step runs
+ * that case's next set-up, so small cases run ahead of large ones.  The waits
+ * are bounded (efvm_batch_set_wait_limit); a wait that runs out ends the run
+ * with EFVM_ERR_TIMEOUT.  The other form (efvm_batch_set_persistent(b, 0))
+ * launches one set-up per step and one kernel per stage over the table.  Each
+ * chunk is a captured CUDA graph.  All cases share one efvm_params (RK3 only);
+ * IBM cylinders are not supported in a batch. */
 typedef struct efvm_batch efvm_batch;
 
 typedef struct {
@@ -431,13 +437,29 @@ int efvm_batch_launch_count(efvm_batch* batch, uint64_t* out);
 /* The CUDA stream the batch launches on (a cudaStream_t). */
 int efvm_batch_get_stream(efvm_batch* batch, void** stream);
 /* Autotuning (on by default): on the first efvm_batch_run the batch times one
- * step with 2, 4 and 8 rows per warp for each case-size bucket present (cells
- * < 64^2, < 128^2, < 256^2, larger) on a copy of the states, keeps the fastest,
- * and caches the choice per process for the device, the method and the buckets.
- * Tuning changes no result.  enable = 0 returns to the built-in heuristic. */
+ * step with tiles of 2, 4, 8 and 16 rows per warp for each case-size bucket
+ * present (cells < 64^2, < 128^2, < 256^2, larger) and then, for the persistent
+ * kernel, its grid at the form's maximum resident blocks per SM and up to three
+ * fewer, on a copy of the states; it keeps the fastest and caches the choice per
+ * process for the device, the method, the kernel and the buckets.  Tuning
+ * changes no result.  enable = 0 returns to the built-in heuristic. */
 int efvm_batch_set_autotune(efvm_batch* batch, int32_t enable);
 /* Rows per warp chosen for the four buckets (0 = heuristic / not tuned yet). */
 int efvm_batch_get_rows(efvm_batch* batch, int32_t rows[4]);
+/* Resident blocks per SM of the persistent kernel's grid (tuned or default). */
+int efvm_batch_get_blocks_per_sm(efvm_batch* batch, int32_t* out);
+/* enable != 0: one persistent launch per chunk of steps (the default); 0: one
+ * launch per stage.  Both give the same results bit for bit. */
+int efvm_batch_set_persistent(efvm_batch* batch, int32_t enable);
+/* Limit of one wait of the persistent kernel for a case's previous stage, in
+ * seconds (default 2, at most 60). */
+int efvm_batch_set_wait_limit(efvm_batch* batch, double seconds);
+/* Fault injection for the bounded waits (host side, no device fault): the next
+ * efvm_batch_run counts one tile more for case k than its table holds, so that
+ * case's first stage never completes, its next stage's waits run out and the
+ * run returns EFVM_ERR_TIMEOUT with the states partly advanced.  No counterpart
+ * in the reference. */
+int efvm_batch_inject_stall(efvm_batch* batch, int32_t k);
 
 /* ---- learned flux correction: BF16 tensor-core kernels -------------------- */
 

@@ -107,3 +107,65 @@ def test_autotuned_rows_change_no_result():
     for k in range(len(grids)):
         assert np.array_equal(ua[k], ub[k])
     assert any(r in (2, 4, 8) for r in rows_tuned) and rows_plain == [0, 0, 0, 0]
+
+
+def test_persistent_launch_equals_per_stage_launches_bit_for_bit():
+    """One persistent launch per chunk of steps (packed tile queue, per-case
+    waits, set-ups inside the launch) against one launch per stage over the same
+    table: the same step counts, and the same states and clocks within the
+    tolerances of the single-context comparison above (the two kernels are
+    separate compilations of the same strip code); the persistent form makes
+    fewer launches."""
+    from dev_field_efvm_b200.device import Batch
+
+    for precision, tol, ttol in ((abi.PREC_FP64, 1e-12, 1e-12), (abi.PREC_FP32_FLUX, 1e-5, 1e-6)):
+        grids, params, states, t_stop, kinds = small_batch(precision)
+        out = []
+        for persistent in (True, False):
+            b = Batch(grids, params)
+            b.set_persistent(persistent)
+            b.set_autotune(False)
+            for k, u in enumerate(states):
+                b.upload(k, u)
+            n0 = b.launch_count()
+            res = b.run(t_stop, chunk=5)
+            out.append(([b.download(k) for k in range(len(grids))], [(r.steps, r.time) for r in res],
+                        b.launch_count() - n0, max(r.steps for r in res)))
+            b.close()
+        (ua, ra, la, sa), (ub, rb, lb, sb) = out
+        exact = 0
+        for k in range(len(grids)):
+            assert ra[k][0] == rb[k][0], (precision, k, kinds[k], ra[k], rb[k])
+            assert abs(ra[k][1] - rb[k][1]) <= ttol * rb[k][1]
+            assert rel(ua[k], ub[k]) <= tol, (precision, k, kinds[k], rel(ua[k], ub[k]))
+            exact += int(np.array_equal(ua[k], ub[k]))
+        print(f"precision {precision}: {exact} of {len(grids)} cases bit-identical")
+        assert la < lb  # the per-stage form launches 4 kernels per step
+
+
+def test_bounded_wait_runs_out_on_an_injected_stall():
+    """Failure detection of the persistent kernel without a device fault: the
+    host counts one tile more for one case than the table holds, so that case's
+    first stage never completes and the waits of its next stage run out after
+    the limit.  The run returns EFVM_ERR_TIMEOUT within a few limits, and the
+    batch and the GPU stay usable: the next run completes normally."""
+    import time
+    from dev_field_efvm_b200.device import Batch, EfvmError
+
+    grids, params, states, t_stop, kinds = small_batch(abi.PREC_FP64)
+    b = Batch(grids, params)
+    b.set_autotune(False)
+    b.set_wait_limit(0.2)
+    for k, u in enumerate(states):
+        b.upload(k, u)
+    b.inject_stall(3)
+    t0 = time.perf_counter()
+    with pytest.raises(EfvmError) as e:
+        b.run(t_stop, max_steps=4, chunk=4)
+    assert e.value.code == abi.ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 10.0
+    for k, u in enumerate(states):
+        b.upload(k, u)
+    res = b.run(t_stop, chunk=4)
+    assert all(r.finished == 1 and r.nonphysical == 0 for r in res)
+    b.close()
