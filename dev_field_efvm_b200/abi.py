@@ -41,6 +41,8 @@ LIMITER_MINMOD, LIMITER_MC = 0, 1
 INTEGRATOR_RK3, INTEGRATOR_EULER = 0, 1
 VISC_SUTHERLAND, VISC_CONSTANT = 0, 1
 PREC_FP64, PREC_FP32_FLUX = 0, 1
+# efvm_stage_form: the stage kernel's form (efvm_set_stage_tiling)
+STAGE_AUTO, STAGE_STRIP, STAGE_TMA = 0, 1, 2
 SEAM_REFERENCE, SEAM_TRUE_PERIODIC = 0, 1
 # rows of static scratch behind efvm_cfl_dt_noalloc (EFVM_CFL_NOALLOC_MAX_ROWS)
 CFL_NOALLOC_MAX_ROWS = 16384

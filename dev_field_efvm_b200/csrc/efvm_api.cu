@@ -7,6 +7,7 @@
 // for a fixed body, so it is built once per efvm_set_cylinders: the solid mask
 // on the device, the ghost list and marker sample points on the host with the
 // same one-rounding-per-operation arithmetic as the reference's Rust.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -86,6 +87,13 @@ struct efvm_ctx {
     bool graph_with_history = false;
     int graph_kernels = 0;
     uint64_t launches = 0;
+    // The TMA-fed stage kernel (2-D contexts): tensor maps of U0, U1, U2 as the
+    // stage input and of U0 as U^n, and the stage tiling (efvm_set_stage_tiling)
+    CUtensorMap tmap[3];
+    CUtensorMap tmap_u0;
+    bool tmaps = false;
+    int stage_form = EFVM_STAGE_AUTO;
+    int stage_rows = 0;
     std::string err;
 };
 
@@ -490,6 +498,15 @@ int prologue(efvm_ctx* c) {
     return EFVM_OK;
 }
 
+// The stage-kernel form a context runs: EFVM_STAGE_AUTO resolves to the strip
+// kernel; the TMA-fed kernel runs where it is selected and the case allows it
+// (2-D, inviscid, no bodies, no learned correction).
+int resolved_form(const efvm_ctx* c) {
+    if (c->stage_form == EFVM_STAGE_TMA && c->tmaps && stage_tma_eligible(c->g, c->ph, c->ibm, c->nn != nullptr))
+        return EFVM_STAGE_TMA;
+    return EFVM_STAGE_STRIP;
+}
+
 void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, bool pdl = true, bool defer = false) {
     if (c->nn)  // the learned corrections of this stage's input
         c->launches += nn_forward_padded(c->nn, uin, c->g.plane, c->g.pitch, c->g.nx, c->g.ny, c->corr, c->prims,
@@ -509,6 +526,12 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
     a.completes_step = (stage == 2 || stage == 3) ? 1 : 0;
     a.want_cfl = a.completes_step && c->ph.fixed_dt <= 0.0;
     a.defer_forces = defer ? 1 : 0;
+    if (c->tmaps && resolved_form(c) == EFVM_STAGE_TMA) {
+        for (int k = 0; k < 3; ++k)
+            if (uin == c->U[k]) a.tmap_in = &c->tmap[k];
+        a.tmap_u0 = &c->tmap_u0;
+    }
+    a.rows = c->stage_rows;
     c->launches += launch_stage(a, pdl, S(c));
 }
 
@@ -829,6 +852,12 @@ static int create_impl(const efvm_grid* grid, const efvm_params* params, int32_t
         }
         cudaMemsetAsync(c->U[k], 0, state_bytes, c->stream);
     }
+    if (g.nz <= 1) {  // tensor maps of the TMA-fed stage kernel (none: the strip kernel only)
+        bool ok = true;
+        for (int k = 0; k < 3 && ok; ++k) ok = encode_state_map(g, c->U[k], false, &c->tmap[k]) == 0;
+        ok = ok && encode_state_map(g, c->U[0], true, &c->tmap_u0) == 0;
+        c->tmaps = ok;
+    }
     e = cudaMalloc(&c->mask, (size_t)g.plane);
     if (e != cudaSuccess) return cleanup_fail(fail(nullptr, EFVM_ERR_OOM, "cudaMalloc mask"));
     cudaMemsetAsync(c->mask, 0, (size_t)g.plane, c->stream);
@@ -1004,6 +1033,8 @@ int efvm_get_solver_state(efvm_ctx* c, efvm_solver_state* out) {
     out->step = s.step;
     out->rk_stage = c->rk_stage;
     out->completed_full_step = s.completed;
+    if (s.nonphysical & 8)
+        return fail(c, EFVM_ERR_TIMEOUT, "a stage kernel's wait for a row of its shared-memory ring ran out");
     if (s.nonphysical) return fail(c, EFVM_ERR_NONPHYSICAL, "the state went non-physical (rho<=0, p<=0 or NaN)");
     return EFVM_OK;
 }
@@ -1328,6 +1359,8 @@ int efvm_step(efvm_ctx* c, int64_t n_steps, int32_t stop_at_t, double t_stop, do
         info->stopped_at_t_stop = (stop_at_t && s.time >= t_stop) ? 1 : 0;
     }
     c->control_dirty = stop_at_t != 0 || cap != 0;
+    if (s.nonphysical & 8)
+        return fail(c, EFVM_ERR_TIMEOUT, "a stage kernel's wait for a row of its shared-memory ring ran out");
     if (s.nonphysical) return fail(c, EFVM_ERR_NONPHYSICAL, "the state went non-physical (rho<=0, p<=0 or NaN)");
     return EFVM_OK;
 }
@@ -1591,6 +1624,122 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
     for (auto& e : ev) cudaEventDestroy(e);
     for (int k = 0; k < 4; ++k) out_ms[k] = acc[k];
     CUDA_TRY(c, cudaGetLastError());
+    return EFVM_OK;
+}
+
+int efvm_set_stage_tiling(efvm_ctx* c, int32_t form, int32_t rows_per_warp) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (form < EFVM_STAGE_AUTO || form > EFVM_STAGE_TMA)
+        return fail(c, EFVM_ERR_INVALID_ARG, "form must be EFVM_STAGE_AUTO, EFVM_STAGE_STRIP or EFVM_STAGE_TMA");
+    if (rows_per_warp < 0 || rows_per_warp > 65536)
+        return fail(c, EFVM_ERR_INVALID_ARG, "rows_per_warp must be in [0, 65536]");
+    if (form == EFVM_STAGE_TMA && !c->tmaps)
+        return fail(c, EFVM_ERR_UNSUPPORTED, "the TMA-fed stage kernel needs a 2-D context with tensor maps");
+    c->stage_form = form;
+    c->stage_rows = rows_per_warp;
+    c->graph_valid = false;
+    return EFVM_OK;
+}
+
+int efvm_get_stage_tiling(efvm_ctx* c, int32_t* form, int32_t* rows_per_warp) {
+    if (!c || !form || !rows_per_warp) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    *form = resolved_form(c);
+    *rows_per_warp = c->stage_rows > 0 ? c->stage_rows
+                                       : stage_rows(c->g.nx, c->g.ny, c->ph.precision == EFVM_PREC_FP32_FLUX,
+                                                    c->ph.viscous != 0, *form == EFVM_STAGE_TMA);
+    return EFVM_OK;
+}
+
+// Times whole steps of every candidate tiling on the live state and keeps the
+// fastest: the strip kernel and (where the case allows it) the TMA-fed kernel,
+// each with 4, 8, 16 and 32 rows per warp and with the rows that fit the whole
+// grid into one wave of resident blocks.  The state, the clock and the force
+// outputs are saved first and restored after every candidate, so tuning
+// changes no result.
+int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (is_3d(c) || has_halo(c) || c->nn || c->params.integrator == EFVM_INTEGRATOR_EULER)
+        return fail(c, EFVM_ERR_UNSUPPORTED, "stage tuning covers 2-D RK3 contexts without slabs or a flux correction");
+    if (c->rk_stage != 0) return fail(c, EFVM_ERR_INVALID_ARG, "efvm_autotune_stage needs a step boundary");
+    if (n_steps <= 0) n_steps = 3;
+    int rc = finish_forces(c);
+    if (rc) return rc;
+    if (c->control_dirty) sync_control(c, 0, 0.0, 0);
+    rc = prologue(c);
+    if (rc) return rc;
+    DevState s0;
+    rc = read_state(c, s0);
+    if (rc) return rc;
+    const size_t state_bytes = (size_t)4 * c->g.plane * sizeof(double);
+    double* backup = nullptr;
+    CUDA_TRY(c, cudaMalloc(&backup, state_bytes));
+    double f0[12] = {0};
+    if (c->ibm) CUDA_TRY(c, cudaMemcpy(f0, c->force_out, sizeof(f0), cudaMemcpyDeviceToHost));
+    CUDA_TRY(c, cudaMemcpyAsync(backup, c->U[0], state_bytes, cudaMemcpyDeviceToDevice, S(c)));
+    auto restore = [&]() -> int {
+        CUDA_TRY(c, cudaMemcpyAsync(c->U[0], backup, state_bytes, cudaMemcpyDeviceToDevice, S(c)));
+        CUDA_TRY(c, cudaMemcpyAsync(c->st, &s0, sizeof(DevState), cudaMemcpyHostToDevice, S(c)));
+        if (c->ibm) CUDA_TRY(c, cudaMemcpyAsync(c->force_out, f0, sizeof(f0), cudaMemcpyHostToDevice, S(c)));
+        CUDA_TRY(c, cudaStreamSynchronize(S(c)));
+        return EFVM_OK;
+    };
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const bool fp32 = c->ph.precision == EFVM_PREC_FP32_FLUX;
+    std::vector<int> forms{EFVM_STAGE_STRIP};
+    if (c->tmaps && stage_tma_eligible(c->g, c->ph, c->ibm, false)) forms.push_back(EFVM_STAGE_TMA);
+    cudaEvent_t e0, e1;
+    CUDA_TRY(c, cudaEventCreate(&e0));
+    CUDA_TRY(c, cudaEventCreate(&e1));
+    const int saved_form = c->stage_form, saved_rows = c->stage_rows;
+    float best = 1e30f;
+    int best_form = saved_form, best_rows = saved_rows;
+    for (int form : forms) {
+        // one wave: the rows that spread the grid's strips over every resident block once
+        const int minb = stage_blocks_per_sm(fp32, c->ph.viscous != 0, form == EFVM_STAGE_TMA);
+        const int bx = (stage_strips(c->g.nx) + 3) / 4;
+        const int by = std::max(1, sms * minb / std::max(bx, 1));
+        std::vector<int> rows{4, 8, 16, 32, (c->g.ny + by - 1) / by};
+        std::sort(rows.begin(), rows.end());
+        rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+        for (int r : rows) {
+            if (r > c->g.ny && r != rows.front()) continue;
+            c->stage_form = form;
+            c->stage_rows = r;
+            rc = capture_step_graph(c);
+            if (rc) break;
+            CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, S(c)));  // warm-up
+            CUDA_TRY(c, cudaEventRecord(e0, S(c)));
+            for (int k = 0; k < n_steps; ++k) CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, S(c)));
+            CUDA_TRY(c, cudaEventRecord(e1, S(c)));
+            CUDA_TRY(c, cudaEventSynchronize(e1));
+            c->launches += (uint64_t)(n_steps + 1) * c->graph_kernels;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            DevState s;
+            rc = read_state(c, s);
+            if (!rc && (s.nonphysical & 8))
+                rc = fail(c, EFVM_ERR_TIMEOUT, "a stage kernel's wait for a row of its shared-memory ring ran out");
+            if (!rc) rc = restore();
+            if (rc) break;
+            if (ms < best) {
+                best = ms;
+                best_form = form;
+                best_rows = r;
+            }
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int rc2 = restore();
+    cudaFree(backup);
+    c->stage_form = rc ? saved_form : best_form;
+    c->stage_rows = rc ? saved_rows : best_rows;
+    c->graph_valid = false;
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (best_ms_per_step) *best_ms_per_step = best / n_steps;
     return EFVM_OK;
 }
 

@@ -36,7 +36,7 @@ struct DevState {
     int lam_idx;             // lam[lam_idx] is being accumulated / is current
     int active;              // 0 once t_stop was reached (kernels become no-ops)
     int stop_at_t;
-    int nonphysical;         // bit 0: rho<=0, bit 1: p<=0, bit 2: NaN
+    int nonphysical;         // bit 0: rho<=0, bit 1: p<=0, bit 2: NaN, bit 3: a TMA row wait ran out
     double t_stop;
     long long hist_pos;      // next MarkerForce history slot
     long long hist_cap;
@@ -201,6 +201,12 @@ struct StageArgs {
     int want_cfl;
     const float* corr;                // learned face-flux corrections [2][4][ny][nx] or null
     int defer_forces;                 // stage 2 of the step graph: its IBM forces run in the next launch
+    // The TMA-fed stage kernel (2-D, inviscid, no bodies, no correction): host
+    // copies of the tensor maps (CUtensorMap, 128 bytes) of the stage input and
+    // of U^n, copied into the launch's parameters; null selects the strip kernel.
+    const void* tmap_in;
+    const void* tmap_u0;
+    int rows;                         // rows per warp; 0 = the built-in choice
 };
 
 // ---- batches of independent cases (efvm_batch.cu) --------------------------
@@ -254,7 +260,15 @@ int batch_form_blocks(bool fp32, bool viscous);
 // Stage-kernel tiling of one case: strips of columns, and rows per warp for a
 // case that runs alone (fp32: the FP32-flux form; viscous: with viscous terms).
 int stage_strips(int nx);
-int stage_rows(int nx, int ny, bool fp32, bool viscous);
+int stage_rows(int nx, int ny, bool fp32, bool viscous, bool tma = false);
+// Resident blocks per SM of the stage-kernel form (tma: the TMA-fed kernel).
+int stage_blocks_per_sm(bool fp32, bool viscous, bool tma);
+// Whether a stage of this case can run the TMA-fed kernel (2-D, inviscid, no
+// immersed bodies, no learned correction), and the tensor map of a state
+// buffer of the case's layout as a 3-D tensor (columns, rows, planes) with the
+// box of the stage input (u0 = false) or of U^n (u0 = true); 0 on success.
+bool stage_tma_eligible(const Geometry& g, const Physics& ph, bool ibm, bool corr);
+int encode_state_map(const Geometry& g, const double* buf, bool u0, void* map_out);
 int launch_batch_stage(const BatchStageArgs& b, int n_tiles, bool pdl, void* stream);
 // Per-step set-up of every case (one thread each).
 int launch_batch_setup(const Physics& ph, const BatchCase* cases, int n_cases, bool pdl, void* stream);

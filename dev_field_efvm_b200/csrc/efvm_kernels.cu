@@ -21,6 +21,7 @@
 // latency: HBM runs at 10-25 % of its copy bandwidth and the FP64 units at
 // 15-25 % of their peak.  No tensor cores are involved.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -28,6 +29,7 @@
 
 #include "efvm_internal.h"
 #include "efvm_math.cuh"
+#include "efvm_tma.cuh"
 
 namespace efvm {
 
@@ -301,6 +303,113 @@ __device__ __forceinline__ void prim_uvt(const U4& u, double inv, double gm1, do
 constexpr int STRIP = 31;  // cells a warp owns per row (lane 31 supplies the right face)
 constexpr int WPB = 4;     // warps per block
 
+// Where a stage reads its rows, the halo cells of a row and U^n.
+//
+// GlobalSrc reads them from the state buffers in global memory (through L1 and
+// L2); its hooks around each row are empty.
+template <bool CG>
+struct GlobalSrc {
+    const double* uin;
+    const double* u0;
+    const double* colp = nullptr;  // this lane's column at row 0
+    long long P = 0;
+    int pitch = 0;
+    __device__ __forceinline__ void bind(const Geometry& g, int /*i*/, int ic) {
+        P = g.plane;
+        pitch = g.pitch;
+        colp = uin + cidx(g, ic, 0);
+    }
+    __device__ __forceinline__ U4 col(int jj) const { return load4g<CG>(colp, P, (long long)jj * pitch); }
+    __device__ __forceinline__ U4 at(const Geometry& g, int ii, int jj) const {
+        return load4g<CG>(uin, P, cidx(g, ii, jj));
+    }
+    __device__ __forceinline__ double u0v(int v, long long o, int /*i*/, int /*j*/) const {
+        return gld<CG>(u0 + v * P + o);
+    }
+    __device__ __forceinline__ bool wait_row(int) { return true; }
+    __device__ __forceinline__ void refill(int) {}
+    __device__ __forceinline__ void release(int) {}
+};
+
+// TmaSrc reads them from the block's shared-memory row ring (efvm_tma.cuh),
+// which TMA fills one iteration ahead: before the first read of row r the warp
+// waits for its slot (wait_row), at the start of iteration j thread 0 loads row
+// j + 3 into the slot that row j - 1 held (refill), and at the end of iteration
+// j every warp releases row j (release).
+struct TmaSrc {
+    double* ring;
+    uint64_t* full;
+    uint64_t* empty;
+    const CUtensorMap* map_in;
+    const CUtensorMap* map_u0;  // null: this stage reads no U^n
+    DevState* st;
+    int first, last;            // the block's row stream
+    int u0_lo, u0_hi;           // rows [u0_lo, u0_hi) carry a U^n copy
+    int x_in, x_u0;             // tensor-map x of slot column 0 (input, U^n)
+    int col0;                   // interior column of input slot column 0
+    int scol;                   // this lane's input slot column
+    int issued;                 // producer: the last row issued
+    bool producer;
+    bool ok;
+
+    static constexpr int SLOT_D = tma::SLOT_BYTES / 8;
+    __device__ __forceinline__ int slot(int r) const { return (r - first) & (tma::RING - 1); }
+    __device__ __forceinline__ uint32_t parity(int r) const { return (uint32_t)((r - first) / tma::RING) & 1u; }
+    __device__ __forceinline__ const double* row(int r) const { return ring + slot(r) * SLOT_D; }
+    __device__ __forceinline__ void issue(int r) {
+        const int s = slot(r);
+        double* base = ring + s * SLOT_D;
+        const bool with_u0 = map_u0 != nullptr && r >= u0_lo && r < u0_hi;
+        tma::arrive_expect(&full[s], tma::IN_BYTES + (with_u0 ? tma::U0_BYTES : 0));
+        tma::load_3d(base, map_in, x_in, r + YO, 0, &full[s]);
+        if (with_u0) tma::load_3d(base + tma::IN_BYTES / 8, map_u0, x_u0, r + YO, 0, &full[s]);
+        issued = r;
+    }
+    __device__ __forceinline__ void fail() {
+        ok = false;
+        atomicOr(&st->nonphysical, tma::TIMEOUT_BIT);
+    }
+    __device__ __forceinline__ void bind(const Geometry&, int i, int /*ic*/) { scol = i - col0; }
+    __device__ __forceinline__ U4 col(int jj) const {
+        const double* p = row(jj) + scol;
+        return U4{p[0], p[tma::IN_COLS], p[2 * tma::IN_COLS], p[3 * tma::IN_COLS]};
+    }
+    __device__ __forceinline__ U4 at(const Geometry&, int ii, int jj) const {
+        const double* p = row(jj) + (ii - col0);
+        return U4{p[0], p[tma::IN_COLS], p[2 * tma::IN_COLS], p[3 * tma::IN_COLS]};
+    }
+    __device__ __forceinline__ double u0v(int v, long long, int i, int j) const {
+        return row(j)[tma::IN_BYTES / 8 + v * tma::U0_COLS + (i - col0 - 2)];
+    }
+    // Every lane waits; the warp goes on only if all of them saw the row land.
+    __device__ __forceinline__ bool wait_row(int r) {
+        const bool got = ok && tma::wait(&full[slot(r)], parity(r));
+        if (__all_sync(0xffffffffu, got)) return true;
+        if (ok) fail();
+        return false;
+    }
+    __device__ __forceinline__ void refill(int j) {
+        if (!producer || !ok) return;
+        const int r = j + 3;
+        if (r > last) return;
+        if (j - 1 >= first && !tma::wait(&empty[slot(j - 1)], parity(j - 1))) {
+            fail();
+            return;
+        }
+        issue(r);
+    }
+    __device__ __forceinline__ void release(int r) {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) tma::arrive(&empty[slot(r)]);
+    }
+    // Thread 0 before the block exits after a wait ran out: wait (bounded) for
+    // every copy it issued, so that none lands after the block is gone.
+    __device__ __forceinline__ void drain() {
+        for (int r = max(first, issued - (tma::RING - 1)); r <= issued; ++r)
+            if (!tma::wait(&full[slot(r)], parity(r))) return;
+    }
+};
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -316,8 +425,8 @@ constexpr int WPB = 4;     // warps per block
 // on a step's last stage, the sponge, refills the boundary ghosts of the output
 // and takes the wave-speed max for the next step's CFL dt.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true, bool CG = false>
-__device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
+template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR, bool XFIRST, bool CG, class SRC>
+__device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip, int by, SRC& src) {
     if (!(CG ? *(volatile const int*)&a.st->active : a.st->active)) return;
     const Geometry& g = a.g;
     const Physics& ph = a.ph;
@@ -356,10 +465,10 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
         const bool true_seam = ph.periodic_seam == EFVM_SEAM_TRUE_PERIODIC;
         const double gm1 = ph.gamma - 1.0;
         const R rg = R(ph.gamma), rgm1 = R(gm1);
-        const double* __restrict__ uin = a.uin;
-        auto ld = [&](int ii, int jj) { return load4g<CG>(uin, P, cidx(g, ii, jj)); };
-        const double* __restrict__ colp = uin + cidx(g, ic, 0);  // this lane's column at row 0
-        auto ldrow = [&](int jj) { return toR<R>(load4g<CG>(colp, P, (long long)jj * g.pitch)); };
+        const double* __restrict__ uin = a.uin;  // the viscous neighbours
+        src.bind(g, i, ic);
+        auto ld = [&](int ii, int jj) { return src.at(g, ii, jj); };
+        auto ldrow = [&](int jj) { return toR<R>(src.col(jj)); };
 
         // Reconstruction flags of the faces on the domain edge; every interior
         // face reconstructs both sides under MUSCL.  x: this lane's face, between
@@ -382,14 +491,18 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
         // row early, where it only forms the face below the first row, so that
         // every y-face flux comes from the same code: a face on the edge of two
         // warps' row ranges is computed by both and must agree bit for bit.
+        const bool rows_ok = src.wait_row(jb - 2) && src.wait_row(jb - 1) && src.wait_row(jb);
         V4<R> uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
         if (MUSCL) {
             V4<R> unused;
             slope_faces(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
         }
+        src.release(jb - 2);
         const double dt = gld<CG>(&a.st->dt);  // set by the step's set-up, constant during the stage
         Q4<R> gb{R(0), R(0), R(0), R(0)};
-        for (int j = jb - 1; j < je; ++j) {
+        for (int j = jb - 1; rows_ok && j < je; ++j) {
+            src.refill(j);
+            if (!src.wait_row(j + 2)) break;
             const V4<R> un2 = ldrow(j + 2);
             const bool row = j >= jb;  // warp-uniform: the first pass only forms the face below row jb
 
@@ -563,7 +676,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
                     const double w0 = a.stage == 1 ? 0.75 : (1.0 / 3.0);
                     const double w1 = a.stage == 1 ? 0.25 : (2.0 / 3.0);
 #pragma unroll
-                    for (int v = 0; v < 4; ++v) un_[v] = fma(w1, fma(rhs[v], dt, ucv[v]), w0 * gld<CG>(a.u0 + v * P + o));
+                    for (int v = 0; v < 4; ++v) un_[v] = fma(w1, fma(rhs[v], dt, ucv[v]), w0 * src.u0v(v, o, i, j));
                 } else {
 #pragma unroll
                     for (int v = 0; v < 4; ++v) un_[v] = fma(rhs[v], dt, ucv[v]);
@@ -607,6 +720,7 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
 
                 if (a.completes_step && a.want_cfl) lam = fmax(lam, wave_speed(g, ph, nw));
             }
+            src.release(j);
             gb = gt;
             uc = un;
             un = un2;
@@ -621,11 +735,74 @@ __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int
     }
 }
 
+// The strip code reading its rows from global memory.
+template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true, bool CG = false>
+__device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
+    GlobalSrc<CG> src{a.uin, a.u0};
+    stage_strip_src<SCHEME, RECON, R, VISC, A, CORR, XFIRST, CG>(a, rows, strip, by, src);
+}
+
 template <int SCHEME, int RECON, class R, int MINB, bool VISC, bool CORR = false, bool XFIRST = true>
 __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
     pdl_wait_then_release();
     stage_strip<SCHEME, RECON, R, VISC, StageArgs, CORR, XFIRST>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5),
                                                                    blockIdx.y);
+}
+
+// The same stage with its rows fed by TMA (2-D meshes without viscous terms,
+// immersed bodies or the learned correction).  A block's four warps march the
+// same rows of four adjacent strips (124 columns); each row of the stage input
+// with two halo columns on each side, and the block's row of U^n, reach the
+// shared-memory ring (efvm_tma.cuh) one iteration before they are read, so the
+// strip code's halo cells and U^n no longer wait on L2 and its rows come from
+// shared memory.  The arithmetic is the strip code's.
+template <int SCHEME, int RECON, class R, int MINB, bool XFIRST>
+__global__ void __launch_bounds__(32 * WPB, MINB)
+    stage_tma_kernel(StageArgs a, int rows, const __grid_constant__ CUtensorMap map_in,
+                     const __grid_constant__ CUtensorMap map_u0) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    pdl_wait_then_release();
+    if (!a.st->active) return;  // the whole grid, before any barrier
+    const int strips = (a.g.nx + STRIP - 1) / STRIP;
+    const int n_active = min(WPB, strips - (int)blockIdx.x * WPB);  // warps with columns
+    const int jb = blockIdx.y * rows, je = min(jb + rows, a.g.ny);
+    const bool with_u0 = a.stage == 1 || a.stage == 2;
+    const int i0b = blockIdx.x * WPB * STRIP;
+    TmaSrc src;
+    src.ring = reinterpret_cast<double*>(smem);
+    src.full = reinterpret_cast<uint64_t*>(smem + tma::RING * tma::SLOT_BYTES);
+    src.empty = src.full + tma::RING;
+    src.map_in = &map_in;
+    src.map_u0 = with_u0 ? &map_u0 : nullptr;
+    src.st = a.st;
+    src.first = jb - 2;
+    src.last = je + 1;
+    src.u0_lo = jb;
+    src.u0_hi = je;
+    src.x_in = XO + i0b - 2;  // even: a 16-byte boundary
+    src.x_u0 = XO + i0b;
+    src.col0 = i0b - 2;
+    src.scol = 0;
+    src.issued = src.first - 1;
+    src.producer = threadIdx.x == 0;
+    src.ok = true;
+    if (threadIdx.x == 0) {
+        tma::prefetch_map(&map_in);
+        if (with_u0) tma::prefetch_map(&map_u0);
+        for (int s = 0; s < tma::RING; ++s) {
+            tma::bar_init(&src.full[s], 1);
+            tma::bar_init(&src.empty[s], (uint32_t)n_active);
+        }
+        tma::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int r = src.first; r < src.first + tma::RING && r <= src.last; ++r) src.issue(r);
+    const int warp = threadIdx.x >> 5;
+    if (warp < n_active)
+        stage_strip_src<SCHEME, RECON, R, false, StageArgs, false, XFIRST, false>(a, rows, blockIdx.x * WPB + warp,
+                                                                                  blockIdx.y, src);
+    if (threadIdx.x == 0 && !src.ok) src.drain();
 }
 
 // The stage arguments of one batch case, with its geometry and physics in the
@@ -1237,11 +1414,12 @@ __global__ void total_mass_kernel(Geometry g, const double* __restrict__ q, doub
 // Launch with programmatic stream serialization when `pdl` is set (the kernel
 // must begin with pdl_wait_then_release).
 template <typename... KArgs, typename... Args>
-static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, bool pdl, Args... args) {
+static void launch_ks(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl,
+                      Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1249,6 +1427,10 @@ static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream
     cfg.attrs = attr;
     cfg.numAttrs = pdl ? 1 : 0;
     cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, bool pdl, Args... args) {
+    launch_ks(kernel, grid, block, 0, s, pdl, args...);
 }
 
 static int grid_for(long long n, int block) {
@@ -1297,7 +1479,7 @@ static int rows_per_warp(int nx, int ny, int blocks_per_sm) {
 template <int SCHEME, int RECON, class R, bool VISC>
 static void launch_stage_t(const StageArgs& a, bool pdl, cudaStream_t s) {
     using F = StageForm<R, VISC>;
-    const int rows = rows_per_warp(a.g.nx, a.g.ny, F::MINB);
+    const int rows = a.rows > 0 ? a.rows : rows_per_warp(a.g.nx, a.g.ny, F::MINB);
     const int strips = (a.g.nx + STRIP - 1) / STRIP;
     dim3 block(32 * WPB);
     dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
@@ -1330,11 +1512,90 @@ static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
     else launch_stage_v<R, false>(a, pdl, s);
 }
 
+// ---- the TMA-fed stage kernel ----------------------------------------------
+// Resident blocks per SM: the shared-memory ring (32.3 KB per block) fits six
+// blocks in the SM's 228 KB, for both precisions.
+constexpr int TMA_MINB = 6;
+
+bool stage_tma_eligible(const Geometry& g, const Physics& ph, bool ibm, bool corr) {
+    return g.nz <= 1 && !ph.viscous && !ibm && !corr;
+}
+
+template <int SCHEME, int RECON, class R>
+static void launch_stage_tma_t(const StageArgs& a, bool pdl, cudaStream_t s) {
+    constexpr bool XFIRST = StageForm<R, false>::XFIRST;
+    auto kernel = stage_tma_kernel<SCHEME, RECON, R, TMA_MINB, XFIRST>;
+    // the largest shared-memory carve-out, once per device
+    static unsigned long long carveout_set = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !(carveout_set & (1ull << dev))) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        carveout_set |= 1ull << dev;
+    }
+    const int rows = a.rows > 0 ? a.rows : rows_per_warp(a.g.nx, a.g.ny, TMA_MINB);
+    const int strips = (a.g.nx + STRIP - 1) / STRIP;
+    const dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
+    const CUtensorMap* m_in = static_cast<const CUtensorMap*>(a.tmap_in);
+    const CUtensorMap* m_u0 = static_cast<const CUtensorMap*>(a.tmap_u0 ? a.tmap_u0 : a.tmap_in);
+    launch_ks(kernel, grid, dim3(32 * WPB), (size_t)tma::SMEM_BYTES, s, pdl, a, rows, *m_in, *m_u0);
+}
+
+template <class R>
+static void launch_stage_tma_r(const StageArgs& a, bool pdl, cudaStream_t s) {
+    const bool muscl = a.ph.reconstruction == EFVM_RECON_MUSCL;
+    switch (a.ph.flux_scheme) {
+        case EFVM_FLUX_RUSANOV:
+            muscl ? launch_stage_tma_t<EFVM_FLUX_RUSANOV, EFVM_RECON_MUSCL, R>(a, pdl, s)
+                  : launch_stage_tma_t<EFVM_FLUX_RUSANOV, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
+            break;
+        case EFVM_FLUX_HLLC_TEXTBOOK:
+            muscl ? launch_stage_tma_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_MUSCL, R>(a, pdl, s)
+                  : launch_stage_tma_t<EFVM_FLUX_HLLC_TEXTBOOK, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
+            break;
+        default:
+            muscl ? launch_stage_tma_t<EFVM_FLUX_HLLC, EFVM_RECON_MUSCL, R>(a, pdl, s)
+                  : launch_stage_tma_t<EFVM_FLUX_HLLC, EFVM_RECON_FIRST_ORDER, R>(a, pdl, s);
+    }
+}
+
+// A state buffer (4 planes of ny + 4 rows x pitch doubles) as a 3-D tensor
+// (columns, rows, planes); the box is one row of the 4 planes, 128 columns for
+// the stage input and 124 for U^n.  cuTensorMapEncodeTiled comes from the
+// driver through the runtime's entry-point query, so the library links no
+// driver library.
+int encode_state_map(const Geometry& g, const double* buf, bool u0, void* map_out) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return 1;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)(g.ny + 2 * YO), 4};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * sizeof(double), (cuuint64_t)g.plane * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)(u0 ? tma::U0_COLS : tma::IN_COLS), 1, 4};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    const CUresult r = encode(static_cast<CUtensorMap*>(map_out), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                              const_cast<double*>(buf), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : 2;
+}
+
 #include "efvm_kernels3d.cuh"
 
 int launch_stage(const StageArgs& a, bool pdl, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if (a.g.nz > 1) return launch_stage3(a, pdl, s);
+    if (a.tmap_in && stage_tma_eligible(a.g, a.ph, a.mask != nullptr, a.corr != nullptr)) {
+        if (a.ph.precision == EFVM_PREC_FP32_FLUX) launch_stage_tma_r<float>(a, pdl, s);
+        else launch_stage_tma_r<double>(a, pdl, s);
+        return 1;
+    }
     if (a.corr) {  // the learned correction runs with MUSCL + HLLC (checked when it is attached)
         using F32 = StageForm<float, false>;
         using F64 = StageForm<double, false>;
@@ -1356,7 +1617,10 @@ int launch_stage(const StageArgs& a, bool pdl, void* stream) {
 
 int stage_strips(int nx) { return (nx + STRIP - 1) / STRIP; }
 
-int stage_rows(int nx, int ny, bool fp32, bool viscous) { return rows_per_warp(nx, ny, form_minb(fp32, viscous)); }
+int stage_rows(int nx, int ny, bool fp32, bool viscous, bool tma) {
+    return rows_per_warp(nx, ny, tma ? TMA_MINB : form_minb(fp32, viscous));
+}
+int stage_blocks_per_sm(bool fp32, bool viscous, bool tma) { return tma ? TMA_MINB : form_minb(fp32, viscous); }
 
 template <int SCHEME, int RECON, class R, bool VISC>
 static void launch_batch_f(const BatchStageArgs& b, int n_tiles, bool pdl, cudaStream_t s) {

@@ -23,7 +23,7 @@ EXPORTS = (
     "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_set_spheres", "efvm_set_discs", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
-    "efvm_profile_steps", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
+    "efvm_profile_steps", "efvm_set_stage_tiling", "efvm_get_stage_tiling", "efvm_autotune_stage", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
     "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
     "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
@@ -77,6 +77,9 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_profile_steps.argtypes = [vp, i64, dp]
+    L.efvm_set_stage_tiling.argtypes = [vp, i32, i32]
+    L.efvm_get_stage_tiling.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.efvm_autotune_stage.argtypes = [vp, i32, dp]
     L.efvm_create_slab.argtypes = [C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), i32, i32, C.POINTER(vp)]
     L.efvm_prepare.argtypes = [vp]
     L.efvm_halo_pack.argtypes = [vp, i32, vp]
@@ -238,6 +241,22 @@ class Context:
         out = np.zeros(4)
         self._check(self.L.efvm_profile_steps(self.h, int(n_steps), _dp(out)))
         return out
+
+    def set_stage_tiling(self, form: int = abi.STAGE_AUTO, rows_per_warp: int = 0) -> None:
+        """Stage-kernel form (abi.STAGE_*) and rows per warp (0: built-in)."""
+        self._check(self.L.efvm_set_stage_tiling(self.h, int(form), int(rows_per_warp)))
+
+    def stage_tiling(self) -> tuple[int, int]:
+        """(form the next stage runs, its rows per warp)."""
+        f, r = C.c_int32(), C.c_int32()
+        self._check(self.L.efvm_get_stage_tiling(self.h, C.byref(f), C.byref(r)))
+        return f.value, r.value
+
+    def autotune_stage(self, n_steps: int = 3) -> float:
+        """Keep the fastest stage tiling (state restored); device ms per step."""
+        ms = C.c_double()
+        self._check(self.L.efvm_autotune_stage(self.h, int(n_steps), C.byref(ms)))
+        return ms.value
 
     def step(self, n_steps: int, t_stop: float | None = None, history: bool = False):
         info = abi.EfvmStepInfo()

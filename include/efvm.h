@@ -342,6 +342,35 @@ int efvm_launch_count(efvm_ctx* ctx, uint64_t* out);
  * (the reference has no timers). */
 int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
 
+/* ---- stage-kernel form and tiling ------------------------------------------ */
+
+/* The stage kernel of a 2-D context comes in two forms with the same
+ * arithmetic.  EFVM_STAGE_STRIP: each warp marches a strip of 31 columns and
+ * reads its rows, halo cells and U^n through L1/L2.  EFVM_STAGE_TMA: a block's
+ * four warps march the same rows of four adjacent strips, fed by TMA
+ * (cp.async.bulk.tensor) into a shared-memory ring of rows one iteration ahead
+ * of their use; it runs for cases without viscous terms, immersed bodies or a
+ * flux correction, and the other cases run the strip form whatever is set.
+ * EFVM_STAGE_AUTO is the built-in choice.  Both give the reference's results
+ * (the forms differ from each other by a few ulps at most; a form gives the
+ * same bits for any rows per warp). */
+typedef enum { EFVM_STAGE_AUTO = 0, EFVM_STAGE_STRIP = 1, EFVM_STAGE_TMA = 2 } efvm_stage_form;
+/* Select the form and the rows each warp marches (0 = built-in choice).  The
+ * reference runs its systems on the CPU and has no counterpart; this replaces
+ * no call.  EFVM_ERR_UNSUPPORTED for EFVM_STAGE_TMA on a 3-D context. */
+int efvm_set_stage_tiling(efvm_ctx* ctx, int32_t form, int32_t rows_per_warp);
+/* The form the context's next stage runs and its rows per warp. */
+int efvm_get_stage_tiling(efvm_ctx* ctx, int32_t* form, int32_t* rows_per_warp);
+/* Time n_steps whole steps (default 3) of every candidate tiling on the live
+ * state -- each form the case allows, with 4, 8, 16 and 32 rows per warp and
+ * with the rows that put the whole grid in one wave of resident blocks -- and
+ * keep the fastest.  The state, the clock and the force outputs are restored
+ * after every candidate, so tuning changes no result.  2-D RK3 contexts at a
+ * step boundary without slabs or a flux correction; *best_ms_per_step (may be
+ * NULL) receives the winner's device time per step.  No counterpart in the
+ * reference. */
+int efvm_autotune_stage(efvm_ctx* ctx, int32_t n_steps, double* best_ms_per_step);
+
 /* ---- slabs of one grid on several GPUs ------------------------------------ */
 
 /* A grid split into row slabs runs one context per slab (one process per GPU).
