@@ -1464,15 +1464,15 @@ static int form_minb(bool fp32, bool viscous) {
 
 // Rows each warp marches.  Small grids take the fewest rows that still fill the
 // resident slots in one wave (the warp's first row also pays for the face below
-// it); large grids take 8, measured fastest at 4096^2: with longer runs the rows
-// that the resident blocks span at once no longer fit in L2 and the halo rows
-// each block re-reads come from HBM.
+// it); large grids take 16, measured fastest at 4096^2 (ms per step, FP64 strip
+// / FP32-flux TMA form: 8 rows 2.589 / 1.737, 16 rows 2.575 / 1.671, 32 rows
+// 2.599 / 1.689, 64 rows 2.874 / 1.779, one wave of 158 rows 2.681 / 1.813).
 static int rows_per_warp(int nx, int ny, int blocks_per_sm) {
     const long long strips = (nx + STRIP - 1) / STRIP;
     const long long slots = 148LL * blocks_per_sm * WPB;
     long long rows = (strips * ny + slots - 1) / slots;
     if (rows < 2) rows = 2;
-    if (rows > 8) rows = 8;
+    if (rows > 16) rows = 16;
     return (int)rows;
 }
 

@@ -351,7 +351,8 @@ int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
  * (cp.async.bulk.tensor) into a shared-memory ring of rows one iteration ahead
  * of their use; it runs for cases without viscous terms, immersed bodies or a
  * flux correction, and the other cases run the strip form whatever is set.
- * EFVM_STAGE_AUTO is the built-in choice.  Both give the reference's results
+ * EFVM_STAGE_AUTO is the built-in choice (the TMA-fed form for FP32 fluxes,
+ * the strip form for FP64: the faster of the two at 4096^2).  Both give the reference's results
  * (the forms differ from each other by a few ulps at most; a form gives the
  * same bits for any rows per warp). */
 typedef enum { EFVM_STAGE_AUTO = 0, EFVM_STAGE_STRIP = 1, EFVM_STAGE_TMA = 2 } efvm_stage_form;
