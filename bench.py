@@ -382,6 +382,18 @@ def with_params(params, **changes):
     return p
 
 
+def tune(ctx, d3):
+    """The library's stage autotuner on the live state (restored afterwards),
+    outside every timed region: the tiling it keeps and its device ms/step."""
+    from dev_field_efvm_b200 import abi
+    if d3:
+        return None
+    ms = ctx.autotune_stage(5)
+    form, rows = ctx.stage_tiling()
+    return {"form": "tma" if form == abi.STAGE_TMA else "strip", "rows_per_warp": rows,
+            "tuner_ms_per_step": ms}
+
+
 def fp32_leg(args, grid, params, u, ex, flush, world, cells):
     """The chosen form on the same case: FP32 reconstruction and fluxes, FP64
     accumulation, device-timed as the FP64 leg."""
@@ -393,6 +405,7 @@ def fp32_leg(args, grid, params, u, ex, flush, world, cells):
         ctx32.set_cylinders(ex["cylinders"], ex["freestream"])
     ctx32.upload(u)
     ctx32.step(args.warmup)
+    tiling32 = tune(ctx32, False)
     s32 = torch.cuda.ExternalStream(ctx32.stream())
     ev32 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
@@ -408,7 +421,7 @@ def fp32_leg(args, grid, params, u, ex, flush, world, cells):
     prof32 = ctx32.profile_steps(max(10, min(args.steps, 50)))
     stage32 = prof32[0] / (3 * max(10, min(args.steps, 50)))
     ctx32.close()
-    return value32, ms32, stage32
+    return value32, ms32, stage32, tiling32
 
 
 def accuracy_leg(grid, params, u, ex, t_end):
@@ -560,6 +573,7 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     ctx.step(args.warmup)
+    tiling = tune(ctx, d3)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -628,10 +642,10 @@ def main():
     # ---- chosen form: FP32 reconstruction/fluxes, FP64 accumulation -------
     chosen = None
     if not d3:  # 3-D meshes run in FP64 only
-        value32, ms32, stage32 = fp32_leg(args, grid, params, u, ex, flush, world, cells)
+        value32, ms32, stage32, tiling32 = fp32_leg(args, grid, params, u, ex, flush, world, cells)
         a32 = bytes_per_launch / (stage32 * 1e-3) / 1e9
         chosen = {"precision": "fp32 reconstruction+flux, fp64 accumulation", "value": value32, "unit": UNIT,
-                  "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
+                  "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value, "stage_tiling": tiling32,
                   "roofline": {"achieved": a32, "peak": peak, "unit": "GB/s", "frac": a32 / peak,
                                "stage_ms_per_launch": stage32}}
         if "vortex" in ex and not args.no_accuracy:
@@ -677,6 +691,7 @@ def main():
                               "flushed between timed steps (256 MB write)",
                            time=st.time, final_step=int(st.step)),
             "roofline": roofline,
+            "stage_tiling": tiling,
             "fp64": fp64,
             "chosen_form": chosen,
             "cpu_baseline": cpu,
