@@ -94,6 +94,11 @@ struct efvm_ctx {
     bool tmaps = false;
     int stage_form = EFVM_STAGE_AUTO;
     int stage_rows = 0;
+    // halo peers of a slab (efvm_set_halo_peer): per y side the neighbour's
+    // three state buffers, their plane and the neighbour's rows
+    double* peer_bufs[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    long long peer_plane[2] = {0, 0};
+    int peer_rows[2] = {0, 0};
     std::string err;
 };
 
@@ -535,6 +540,13 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
         a.tmap_u0 = &c->tmap_u0;
     }
     a.rows = c->stage_rows;
+    for (int side = 0; side < 2; ++side) {
+        if (!c->peer_bufs[side][0]) continue;
+        for (int k = 0; k < 3; ++k)
+            if (uout == c->U[k]) a.peer_out[side] = c->peer_bufs[side][k];
+        a.peer_plane[side] = c->peer_plane[side];
+        a.peer_ny[side] = c->peer_rows[side];
+    }
     c->launches += launch_stage(a, pdl, S(c));
 }
 
@@ -1238,6 +1250,42 @@ int efvm_halo_pack(efvm_ctx* c, int32_t side, double* dev_buf) { return halo_row
 
 int efvm_halo_unpack(efvm_ctx* c, int32_t side, const double* dev_buf) {
     return halo_rows(c, side, const_cast<double*>(dev_buf), 1);
+}
+
+int efvm_get_state_buffers(efvm_ctx* c, double* bufs[3], int64_t* plane, int32_t* rows) {
+    if (!c || !bufs || !plane || !rows) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (is_3d(c)) return refuse_3d(c, "efvm_get_state_buffers");
+    for (int k = 0; k < 3; ++k) bufs[k] = c->U[k];
+    *plane = c->g.plane;
+    *rows = c->g.ny;
+    return EFVM_OK;
+}
+
+int efvm_set_halo_peer(efvm_ctx* c, int32_t side, double* const peer_bufs[3], int64_t peer_plane,
+                       int32_t peer_rows) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (is_3d(c)) return refuse_3d(c, "efvm_set_halo_peer");
+    if (side != EFVM_YLO && side != EFVM_YHI) return fail(c, EFVM_ERR_INVALID_ARG, "side must be EFVM_YLO or EFVM_YHI");
+    if (!(side == EFVM_YLO ? c->ph.halo_ylo : c->ph.halo_yhi))
+        return fail(c, EFVM_ERR_INVALID_ARG, "efvm_set_halo_peer: that side does not face another slab");
+    const int s = side == EFVM_YLO ? 0 : 1;
+    if (!peer_bufs) {  // back to the pack / unpack exchange
+        for (int k = 0; k < 3; ++k) c->peer_bufs[s][k] = nullptr;
+        c->peer_plane[s] = 0;
+        c->peer_rows[s] = 0;
+        c->graph_valid = false;
+        return EFVM_OK;
+    }
+    for (int k = 0; k < 3; ++k)
+        if (!peer_bufs[k]) return fail(c, EFVM_ERR_INVALID_ARG, "efvm_set_halo_peer: null peer buffer");
+    if (peer_rows < 2 || peer_plane < (int64_t)(peer_rows + 2 * YO) * c->g.pitch)
+        return fail(c, EFVM_ERR_INVALID_ARG, "efvm_set_halo_peer: the peer needs >= 2 rows and a plane of "
+                                             "(rows + 4) x pitch doubles");
+    for (int k = 0; k < 3; ++k) c->peer_bufs[s][k] = peer_bufs[k];
+    c->peer_plane[s] = peer_plane;
+    c->peer_rows[s] = peer_rows;
+    c->graph_valid = false;
+    return EFVM_OK;
 }
 
 int efvm_wave_speed_slot(efvm_ctx* c, uint64_t** dev_slot) {

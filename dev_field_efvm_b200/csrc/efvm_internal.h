@@ -207,6 +207,13 @@ struct StageArgs {
     const void* tmap_in;
     const void* tmap_u0;
     int rows;                         // rows per warp; 0 = the built-in choice
+    // Slabs with halo peers (efvm_set_halo_peer): the output buffer of this
+    // stage of the neighbouring slab below (0) and above (1), its plane and
+    // rows; the stage stores its two edge rows straight into that slab's
+    // ghost rows.  Null: the side is filled by efvm_halo_unpack instead.
+    double* peer_out[2];
+    long long peer_plane[2];
+    int peer_ny[2];
 };
 
 // ---- batches of independent cases (efvm_batch.cu) --------------------------

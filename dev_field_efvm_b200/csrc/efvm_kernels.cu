@@ -181,6 +181,22 @@ __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& p
     }
 }
 
+// A slab's two rows next to a side with a halo peer go straight into the
+// peer's ghost rows of the same stage's output: rows 0, 1 become the lower
+// slab's rows ny_lo, ny_lo + 1, and rows ny - 2, ny - 1 the upper slab's rows
+// -2, -1 (the peers share this slab's nx, hence its pitch).  The exchange that
+// halo_exchange_forward_all does between stages then happens as the stage
+// writes, on this GPU's peer memory path (another slab's buffer on the same
+// GPU, or a peer GPU's buffer over NVLink).  Batch cases have no peers.
+__device__ __forceinline__ void peer_rows(const StageArgs& a, const Geometry& g, int i, int j, const U4& u) {
+    if (a.peer_out[0] && j < NG)
+        store4(a.peer_out[0], a.peer_plane[0], (long long)(YO + a.peer_ny[0] + j) * g.pitch + (XO + i), u);
+    if (a.peer_out[1] && j >= g.ny - NG)
+        store4(a.peer_out[1], a.peer_plane[1], (long long)(YO + j - g.ny) * g.pitch + (XO + i), u);
+}
+template <class A>
+__device__ __forceinline__ void peer_rows(const A&, const Geometry&, int, int, const U4&) {}
+
 // The wave-speed accumulator of the current step: the context's own double
 // buffer, or the external slot that slabs max-reduce across GPUs.
 __device__ __forceinline__ unsigned long long* lam_slot(DevState* st) {
@@ -705,6 +721,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
 
                 store4(a.uout, P, o, nw);
                 write_ghosts(g, ph, a.uout, i, j, nw);
+                peer_rows(a, g, i, j, nw);
 
                 // non-physical state flag (rho<=0, p<=0, NaN)
                 // p > 0 with rho > 0 is 2 E rho > m^2 (no division)

@@ -24,7 +24,7 @@ EXPORTS = (
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
     "efvm_profile_steps", "efvm_set_stage_tiling", "efvm_get_stage_tiling", "efvm_autotune_stage", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
-    "efvm_wave_speed_slot", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
+    "efvm_wave_speed_slot", "efvm_get_state_buffers", "efvm_set_halo_peer", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
     "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
     "efvm_batch_set_persistent", "efvm_batch_set_wait_limit", "efvm_batch_inject_stall", "efvm_batch_get_blocks_per_sm",
@@ -85,6 +85,8 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_halo_pack.argtypes = [vp, i32, vp]
     L.efvm_halo_unpack.argtypes = [vp, i32, vp]
     L.efvm_wave_speed_slot.argtypes = [vp, C.POINTER(vp)]
+    L.efvm_get_state_buffers.argtypes = [vp, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]
+    L.efvm_set_halo_peer.argtypes = [vp, i32, C.POINTER(vp), i64, i32]
     L.efvm_batch_create.argtypes = [C.POINTER(abi.EfvmGrid), i32, C.POINTER(abi.EfvmParams), C.POINTER(vp)]
     L.efvm_batch_destroy.argtypes = [vp]
     L.efvm_batch_last_error.restype = C.c_char_p
@@ -225,6 +227,18 @@ class Context:
 
     def halo_unpack(self, side: int, dev_ptr: int) -> None:
         self._check(self.L.efvm_halo_unpack(self.h, side, C.c_void_p(dev_ptr)))
+
+    def state_buffers(self) -> tuple[list[int], int, int]:
+        """Device addresses of the three state buffers, their plane (doubles) and the rows."""
+        bufs = (C.c_void_p * 3)()
+        plane, rows = C.c_int64(), C.c_int32()
+        self._check(self.L.efvm_get_state_buffers(self.h, bufs, C.byref(plane), C.byref(rows)))
+        return [int(b) for b in bufs], plane.value, rows.value
+
+    def set_halo_peer(self, side: int, bufs: list[int] | None, plane: int = 0, rows: int = 0) -> None:
+        """Store this slab's edge rows of `side` into the neighbour's buffers (None: pack / unpack)."""
+        arr = None if bufs is None else (C.c_void_p * 3)(*bufs)
+        self._check(self.L.efvm_set_halo_peer(self.h, int(side), arr, int(plane), int(rows)))
 
     def wave_speed_slot(self) -> int:
         """Device address of the external wave-speed slot (a uint64)."""

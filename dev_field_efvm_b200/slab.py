@@ -250,3 +250,49 @@ class LocalTransport:
                 for e in self.engines:
                     e.substep()
         self._sync()
+
+
+class PeerLocalSlabs:
+    """Every slab on this GPU, with the halo exchange fused into the stage
+    kernels (efvm_set_halo_peer): each stage stores its edge rows straight into
+    the neighbouring slabs' ghost rows of the same stage's output, so no pack,
+    copy or unpack runs between stages.  Stage t of a slab waits (a stream
+    event, no host round trip) for stage t - 1 of both neighbours: their rows
+    in its input have been written, and its own stores cannot overtake their
+    reads of the buffer it writes.  One pack / unpack exchange fills the ghost
+    rows of the uploaded state before the first step; the wave-speed slot is
+    max-reduced once per step as in LocalTransport."""
+
+    def __init__(self, engines, periodic_y: bool):
+        self.engines = engines
+        self.local = LocalTransport(engines, periodic_y)
+        self.nbs = self.local.nbs
+        for k, e in enumerate(engines):
+            for side, other in ((YLO, self.nbs[k].lower), (YHI, self.nbs[k].upper)):
+                if other is not None:
+                    bufs, plane, rows = engines[other].ctx.state_buffers()
+                    e.ctx.set_halo_peer(side, bufs, plane, rows)
+        self.events = [[torch.cuda.Event() for _ in engines] for _ in range(2)]
+        self.stage = 0
+        self.primed = False
+
+    def step(self, n_steps: int) -> None:
+        if not self.primed:  # the ghost rows of the uploaded state
+            for e in self.engines:
+                e.prepare()
+            self.local.exchange()
+            self.primed = True
+        for _ in range(n_steps):
+            for e in self.engines:
+                e.prepare()
+            self.local.reduce()
+            for _s in range(3):
+                prev, cur = self.events[(self.stage + 1) % 2], self.events[self.stage % 2]
+                for k, e in enumerate(self.engines):
+                    if self.stage > 0:
+                        for o in {self.nbs[k].lower, self.nbs[k].upper} - {None, k}:
+                            e.stream.wait_event(prev[o])
+                    e.substep()
+                    cur[k].record(e.stream)
+                self.stage += 1
+        self.local._sync()

@@ -420,6 +420,28 @@ int efvm_halo_unpack(efvm_ctx* ctx, int32_t side, const double* dev_buf);
  * the two the caller max-reduces the word across slabs (an integer max). */
 int efvm_wave_speed_slot(efvm_ctx* ctx, uint64_t** dev_slot);
 
+/* Halo peers: the exchange fused into the stage kernel.  Instead of
+ * efvm_halo_pack -> transport -> efvm_halo_unpack between stages (the
+ * reference's halo_exchange_forward_all, crates/cfd_solver/src/lib.rs:79-81),
+ * a slab's stage kernel can store its two rows next to a y side straight into
+ * the ghost rows of the neighbouring slab's output buffer of the same stage:
+ * another slab's buffer on the same GPU, or a peer GPU's buffer mapped into
+ * this process (peer access or CUDA IPC).  All slabs must share nx and run the
+ * same integrator in lockstep; the caller orders stage t of a slab after stage
+ * t - 1 of both neighbours (stream events on one GPU) and still max-reduces the
+ * wave-speed slot once per step.  Ghost rows of a freshly uploaded state come
+ * from one pack / unpack exchange before the first substep.
+ *
+ * efvm_get_state_buffers: the context's three state buffers (U^n and the two
+ * stage buffers, each 4 planes of `plane` doubles) and its rows. */
+int efvm_get_state_buffers(efvm_ctx* ctx, double* bufs[3], int64_t* plane, int32_t* rows);
+/* Write side `side`'s edge rows into the neighbour's buffers peer_bufs[0..2]
+ * (as that neighbour's efvm_get_state_buffers returns them, in its order) of
+ * peer_plane doubles per plane and peer_rows rows; NULL peer_bufs returns the
+ * side to the pack / unpack exchange.  The side must face another slab. */
+int efvm_set_halo_peer(efvm_ctx* ctx, int32_t side, double* const peer_bufs[3], int64_t peer_plane,
+                       int32_t peer_rows);
+
 /* ---- batches of independent cases ---------------------------------------- */
 
 /* A batch advances many independent cases (an ensemble or a parameter sweep;

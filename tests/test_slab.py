@@ -184,7 +184,7 @@ def test_gloo_ranks_match_one_slab(world, periodic):
 # ---------------------------------------------------------------------------
 # device slabs on one GPU
 # ---------------------------------------------------------------------------
-def _device_run(builder, n_slabs, steps):
+def _device_run(builder, n_slabs, steps, peers=False):
     from dev_field_efvm_b200.device import Context
 
     grid, params, u, ex = builder()
@@ -199,7 +199,12 @@ def _device_run(builder, n_slabs, steps):
         e = slab.DeviceSlab(grid, params, r0, n)
         e.ctx.upload(u[r0:r0 + n])
         engines.append(e)
-    slab.LocalTransport(engines, per_y).step(steps)
+    if peers:  # the exchange fused into the stage kernels, in two calls to check the stage chain
+        drv = slab.PeerLocalSlabs(engines, per_y)
+        drv.step(steps // 2)
+        drv.step(steps - steps // 2)
+    else:
+        slab.LocalTransport(engines, per_y).step(steps)
     return np.concatenate([e.ctx.download() for e in engines]), engines[0].ctx.solver_state(), ex, grid
 
 
@@ -231,6 +236,44 @@ def test_device_slabs_match_unsplit_context(name, builder, steps):
         vol = (grid.hi[0] - grid.lo[0]) / grid.nx * (grid.hi[1] - grid.lo[1]) / grid.ny * (grid.hi[2] - grid.lo[2])
         m = cases.moments(ref, ex["x"], vol)
         assert np.all(np.isfinite(m)) and m[0] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,builder,steps", [
+    ("mpi_pulse", cases.mpi_pulse_case, 10),
+    ("vortex_muscl_reference_seam", _vortex(abi.SEAM_REFERENCE), 8),
+    ("vortex_muscl_true_periodic", _vortex(abi.SEAM_TRUE_PERIODIC), 8),
+    ("channel_walls_viscous_muscl", _channel, 8),
+])
+def test_halo_peer_slabs_match_unsplit_context(name, builder, steps):
+    """The exchange fused into the stage kernels (efvm_set_halo_peer): each
+    stage stores its edge rows into the neighbours' ghost rows; 1-4 slabs equal
+    the unsplit context bit for bit."""
+    ref, s_ref, _, _ = _device_run(builder, 0, steps)
+    for n in (1, 2, 3, 4):
+        got, s, _, _ = _device_run(builder, n, steps, peers=True)
+        assert s.step == s_ref.step == steps
+        assert s.time == s_ref.time, (n, s.time, s_ref.time)
+        assert np.array_equal(got, ref), f"{name}: {n} peer slabs differ from the unsplit context"
+
+
+@pytest.mark.gpu
+def test_halo_peer_argument_checks():
+    from dev_field_efvm_b200.device import Context, EfvmError
+
+    grid, params, u, ex = _channel()  # walls in y: the outer sides face no slab
+    lo = Context(grid, params, rows=(0, 16))
+    hi = Context(grid, params, rows=(16, 16))
+    bufs, plane, rows = hi.state_buffers()
+    assert rows == 16 and plane >= (rows + 4) * 8
+    with pytest.raises(EfvmError):
+        lo.set_halo_peer(abi.YLO, bufs, plane, rows)  # a wall side
+    with pytest.raises(EfvmError):
+        lo.set_halo_peer(abi.YHI, bufs, plane, 1)  # too few rows
+    with pytest.raises(EfvmError):
+        lo.set_halo_peer(abi.YHI, bufs, 8, rows)  # plane too small
+    lo.set_halo_peer(abi.YHI, bufs, plane, rows)
+    lo.set_halo_peer(abi.YHI, None)
 
 
 @pytest.mark.gpu
