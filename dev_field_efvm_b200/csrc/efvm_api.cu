@@ -99,6 +99,7 @@ struct efvm_ctx {
     double* peer_bufs[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     long long peer_plane[2] = {0, 0};
     int peer_rows[2] = {0, 0};
+    void* peer_ipc[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};  // mapped by this context
     std::string err;
 };
 
@@ -917,6 +918,9 @@ int efvm_destroy(efvm_ctx* c) {
     if (!c) return EFVM_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    for (auto& side : c->peer_ipc)
+        for (void* p : side)
+            if (p) cudaIpcCloseMemHandle(p);
     for (int k = 0; k < 3; ++k) cudaFree(c->U[k]);
     cudaFree(c->mask);
     cudaFree(c->yw);
@@ -1269,8 +1273,12 @@ int efvm_set_halo_peer(efvm_ctx* c, int32_t side, double* const peer_bufs[3], in
     if (!(side == EFVM_YLO ? c->ph.halo_ylo : c->ph.halo_yhi))
         return fail(c, EFVM_ERR_INVALID_ARG, "efvm_set_halo_peer: that side does not face another slab");
     const int s = side == EFVM_YLO ? 0 : 1;
-    if (!peer_bufs) {  // back to the pack / unpack exchange
-        for (int k = 0; k < 3; ++k) c->peer_bufs[s][k] = nullptr;
+    if (!peer_bufs) {  // back to the pack / unpack exchange (and unmap a neighbour's IPC buffers)
+        for (int k = 0; k < 3; ++k) {
+            if (c->peer_ipc[s][k]) cudaIpcCloseMemHandle(c->peer_ipc[s][k]);
+            c->peer_ipc[s][k] = nullptr;
+            c->peer_bufs[s][k] = nullptr;
+        }
         c->peer_plane[s] = 0;
         c->peer_rows[s] = 0;
         c->graph_valid = false;
@@ -1285,6 +1293,47 @@ int efvm_set_halo_peer(efvm_ctx* c, int32_t side, double* const peer_bufs[3], in
     c->peer_plane[s] = peer_plane;
     c->peer_rows[s] = peer_rows;
     c->graph_valid = false;
+    return EFVM_OK;
+}
+
+int efvm_get_state_ipc(efvm_ctx* c, void* handles) {
+    if (!c || !handles) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (is_3d(c)) return refuse_3d(c, "efvm_get_state_ipc");
+    auto* h = static_cast<cudaIpcMemHandle_t*>(handles);
+    for (int k = 0; k < 3; ++k) CUDA_TRY(c, cudaIpcGetMemHandle(&h[k], c->U[k]));
+    return EFVM_OK;
+}
+
+static void close_peer_ipc(efvm_ctx* c, int s) {
+    for (int k = 0; k < 3; ++k) {
+        if (c->peer_ipc[s][k]) cudaIpcCloseMemHandle(c->peer_ipc[s][k]);
+        c->peer_ipc[s][k] = nullptr;
+    }
+}
+
+int efvm_set_halo_peer_ipc(efvm_ctx* c, int32_t side, const void* handles, int64_t peer_plane, int32_t peer_rows) {
+    if (!c || !handles) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (side != EFVM_YLO && side != EFVM_YHI) return fail(c, EFVM_ERR_INVALID_ARG, "side must be EFVM_YLO or EFVM_YHI");
+    const int s = side == EFVM_YLO ? 0 : 1;
+    const auto* h = static_cast<const cudaIpcMemHandle_t*>(handles);
+    void* opened[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; ++k) {
+        const cudaError_t e = cudaIpcOpenMemHandle(&opened[k], h[k], cudaIpcMemLazyEnablePeerAccess);
+        if (e != cudaSuccess) {
+            for (int q = 0; q < k; ++q) cudaIpcCloseMemHandle(opened[q]);
+            return fail(c, EFVM_ERR_CUDA, std::string("efvm_set_halo_peer_ipc: cudaIpcOpenMemHandle: ") +
+                                              cudaGetErrorString(e));
+        }
+    }
+    double* bufs[3] = {static_cast<double*>(opened[0]), static_cast<double*>(opened[1]),
+                       static_cast<double*>(opened[2])};
+    const int rc = efvm_set_halo_peer(c, side, bufs, peer_plane, peer_rows);
+    if (rc) {
+        for (auto* p : opened) cudaIpcCloseMemHandle(p);
+        return rc;
+    }
+    close_peer_ipc(c, s);  // a mapping this one replaces
+    for (int k = 0; k < 3; ++k) c->peer_ipc[s][k] = opened[k];
     return EFVM_OK;
 }
 

@@ -193,6 +193,8 @@ __device__ __forceinline__ void peer_rows(const StageArgs& a, const Geometry& g,
         store4(a.peer_out[0], a.peer_plane[0], (long long)(YO + a.peer_ny[0] + j) * g.pitch + (XO + i), u);
     if (a.peer_out[1] && j >= g.ny - NG)
         store4(a.peer_out[1], a.peer_plane[1], (long long)(YO + j - g.ny) * g.pitch + (XO + i), u);
+    // a peer on another GPU reads these rows after the stage: make them visible system-wide
+    if ((a.peer_out[0] && j < NG) || (a.peer_out[1] && j >= g.ny - NG)) __threadfence_system();
 }
 template <class A>
 __device__ __forceinline__ void peer_rows(const A&, const Geometry&, int, int, const U4&) {}

@@ -24,7 +24,7 @@ EXPORTS = (
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
     "efvm_profile_steps", "efvm_set_stage_tiling", "efvm_get_stage_tiling", "efvm_autotune_stage", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
-    "efvm_wave_speed_slot", "efvm_get_state_buffers", "efvm_set_halo_peer", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
+    "efvm_wave_speed_slot", "efvm_get_state_buffers", "efvm_set_halo_peer", "efvm_get_state_ipc", "efvm_set_halo_peer_ipc", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
     "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
     "efvm_batch_set_persistent", "efvm_batch_set_wait_limit", "efvm_batch_inject_stall", "efvm_batch_get_blocks_per_sm",
@@ -87,6 +87,8 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_wave_speed_slot.argtypes = [vp, C.POINTER(vp)]
     L.efvm_get_state_buffers.argtypes = [vp, C.POINTER(vp), C.POINTER(i64), C.POINTER(i32)]
     L.efvm_set_halo_peer.argtypes = [vp, i32, C.POINTER(vp), i64, i32]
+    L.efvm_get_state_ipc.argtypes = [vp, C.c_char_p]
+    L.efvm_set_halo_peer_ipc.argtypes = [vp, i32, C.c_char_p, i64, i32]
     L.efvm_batch_create.argtypes = [C.POINTER(abi.EfvmGrid), i32, C.POINTER(abi.EfvmParams), C.POINTER(vp)]
     L.efvm_batch_destroy.argtypes = [vp]
     L.efvm_batch_last_error.restype = C.c_char_p
@@ -239,6 +241,16 @@ class Context:
         """Store this slab's edge rows of `side` into the neighbour's buffers (None: pack / unpack)."""
         arr = None if bufs is None else (C.c_void_p * 3)(*bufs)
         self._check(self.L.efvm_set_halo_peer(self.h, int(side), arr, int(plane), int(rows)))
+
+    def state_ipc(self) -> bytes:
+        """CUDA IPC handles of the three state buffers (3 x 64 bytes)."""
+        buf = C.create_string_buffer(3 * 64)
+        self._check(self.L.efvm_get_state_ipc(self.h, buf))
+        return buf.raw
+
+    def set_halo_peer_ipc(self, side: int, handles: bytes, plane: int, rows: int) -> None:
+        """Map another process's state buffers (efvm_get_state_ipc) as the side's halo peer."""
+        self._check(self.L.efvm_set_halo_peer_ipc(self.h, int(side), bytes(handles), int(plane), int(rows)))
 
     def wave_speed_slot(self) -> int:
         """Device address of the external wave-speed slot (a uint64)."""

@@ -96,6 +96,23 @@ class DeviceSlab:
     def synchronize(self) -> None:
         self.stream.synchronize()
 
+    # halo peers across processes (DistPeerSlabs)
+    def export_peer(self) -> tuple[bytes, int, int]:
+        """CUDA IPC handles of this slab's state buffers, their plane and rows."""
+        _, plane, rows = self.ctx.state_buffers()
+        return self.ctx.state_ipc(), plane, rows
+
+    def map_peer(self, side: int, handles: bytes, plane: int, rows: int) -> None:
+        self.ctx.set_halo_peer_ipc(side, handles, plane, rows)
+
+    def map_self(self, side: int) -> None:
+        """One slab on a periodic axis: its own buffers are the peer across the wrap."""
+        bufs, plane, rows = self.ctx.state_buffers()
+        self.ctx.set_halo_peer(side, bufs, plane, rows)
+
+    def token(self) -> torch.Tensor:
+        return torch.zeros(1, dtype=torch.int64, device=self.device)
+
 
 class _CudaWord:
     """__cuda_array_interface__ of one int64 at a device address."""
@@ -296,3 +313,55 @@ class PeerLocalSlabs:
                     cur[k].record(e.stream)
                 self.stage += 1
         self.local._sync()
+
+
+class DistPeerSlabs:
+    """This process's slab, one process per GPU, with the halo exchange fused
+    into its stage kernels over peer memory: every rank exports its three state
+    buffers as CUDA IPC handles, all ranks gather them, and each slab maps its
+    neighbours' buffers (peer access over NVLink) and stores its edge rows into
+    their ghost rows as it writes them.  What remains of the collective is
+    ordering: after stages 1 and 2 every rank all-reduces an 8-byte token on the
+    context's stream, so no rank starts a stage before every rank has finished
+    the one before (its rows have landed, and the buffer it writes is no longer
+    read); before stage 1 the per-step max-reduce of the wave-speed slot does the
+    same.  One pack / exchange / unpack through DistTransport fills the ghost
+    rows of the uploaded state first.  Every rank takes the same collective
+    steps in the same order."""
+
+    def __init__(self, engine, nb: Neighbours, group=None):
+        import torch.distributed as dist
+
+        self.e, self.nb, self.dist, self.group = engine, nb, dist, group
+        rank = dist.get_rank(group)
+        exports = [None] * dist.get_world_size(group)
+        dist.all_gather_object(exports, engine.export_peer(), group=group)
+        self.mapped = {}
+        for side, other in ((YLO, nb.lower), (YHI, nb.upper)):
+            if other is None:
+                continue
+            if other == rank:
+                engine.map_self(side)
+            else:
+                engine.map_peer(side, *exports[other])
+            self.mapped[side] = other
+        self.token = engine.token()
+        self.rank = SlabRank(engine, nb, DistTransport(group))
+        self.primed = False
+
+    def _all_reduce(self, t) -> None:
+        with self.rank._ctx():
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX, group=self.group)
+
+    def step(self, n_steps: int) -> None:
+        if not self.primed:
+            self.e.prepare()
+            self.rank.exchange()
+            self.primed = True
+        for _ in range(n_steps):
+            self.e.prepare()
+            self._all_reduce(self.e.slot())
+            for s in range(3):
+                self.e.substep()
+                if s < 2:
+                    self._all_reduce(self.token)

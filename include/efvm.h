@@ -441,6 +441,17 @@ int efvm_get_state_buffers(efvm_ctx* ctx, double* bufs[3], int64_t* plane, int32
  * side to the pack / unpack exchange.  The side must face another slab. */
 int efvm_set_halo_peer(efvm_ctx* ctx, int32_t side, double* const peer_bufs[3], int64_t peer_plane,
                        int32_t peer_rows);
+/* The same across processes (one process per GPU): efvm_get_state_ipc writes
+ * the CUDA IPC handles of the three state buffers (3 x 64 bytes) for the
+ * neighbours to map; efvm_set_halo_peer_ipc maps a neighbour's handles into
+ * this process (with peer access) and sets them as the side's peer.  The
+ * mapping is released when the side is reset or the context is destroyed.
+ * A process cannot map its own handles: slabs in one process use
+ * efvm_get_state_buffers. */
+#define EFVM_IPC_HANDLE_BYTES 64
+int efvm_get_state_ipc(efvm_ctx* ctx, void* handles);
+int efvm_set_halo_peer_ipc(efvm_ctx* ctx, int32_t side, const void* handles, int64_t peer_plane,
+                           int32_t peer_rows);
 
 /* ---- batches of independent cases ---------------------------------------- */
 

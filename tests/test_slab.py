@@ -114,6 +114,54 @@ class FakeSlab:
         return self.U[0][2:-2].copy()
 
 
+class FakePeerSlab(FakeSlab):
+    """FakeSlab whose three buffers live in shared memory-mapped files, so that
+    gloo ranks can act as halo peers of one another (the host-side stand-in for
+    CUDA IPC mappings): export_peer names the files, map_peer opens a
+    neighbour's, and each stage stores its two edge rows straight into the
+    neighbour's ghost rows of the same stage's output, as the device stage
+    kernel does with efvm_set_halo_peer."""
+
+    def __init__(self, u_global, row0, rows, lo_wall, hi_wall, folder, rank):
+        super().__init__(u_global, row0, rows, lo_wall, hi_wall)
+        self.paths = [os.path.join(folder, f"slab{rank}_U{k}.bin") for k in range(3)]
+        mm = []
+        for k, path in enumerate(self.paths):
+            m = np.memmap(path, dtype=np.float64, mode="w+", shape=self.U[k].shape)
+            m[:] = self.U[k]
+            m.flush()
+            mm.append(m)
+        self.U = mm
+        self.peer = {}
+
+    def export_peer(self):
+        return "\n".join(self.paths).encode(), 0, self.ny
+
+    def map_peer(self, side, handles, plane, rows):
+        self.peer[side] = [np.memmap(p, dtype=np.float64, mode="r+", shape=(rows + 4, self.nx))
+                           for p in handles.decode().split("\n")]
+
+    def map_self(self, side):
+        self.peer[side] = self.U
+
+    def token(self):
+        return torch.zeros(1, dtype=torch.int64)
+
+    def substep(self):
+        out = (self.stage + 1) % 3
+        super().substep()
+        q = self.U[out]
+        if abi.YLO in self.peer:  # rows 0, 1 -> the lower slab's top ghost rows
+            lo = self.peer[abi.YLO][out]
+            lo[-2:] = q[2:4]
+            lo.flush()
+        if abi.YHI in self.peer:  # rows ny-2, ny-1 -> the upper slab's bottom ghost rows
+            hi = self.peer[abi.YHI][out]
+            hi[0:2] = q[-4:-2]
+            hi.flush()
+        q.flush()
+
+
 def initial(ny=24, nx=20, seed=3):
     rng = np.random.default_rng(seed)
     y, x = np.meshgrid(np.arange(ny) / ny, np.arange(nx) / nx, indexing="ij")
@@ -176,6 +224,40 @@ def test_gloo_ranks_match_one_slab(world, periodic):
     with tempfile.TemporaryDirectory() as d:
         port = 29500 + (os.getpid() % 1000) + 7 * world + (1 if periodic else 0)
         mp.start_processes(_gloo_worker, args=(world, periodic, port, d), nprocs=world, join=True,
+                           start_method="spawn")
+        got = np.concatenate([np.load(os.path.join(d, f"r{k}.npy")) for k in range(world)])
+    assert np.array_equal(got, ref)
+
+
+def _gloo_peer_worker(rank, world, periodic, port, out_dir):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        u = initial()
+        r0, n = slab.split_rows(u.shape[0], world)[rank]
+        nb = slab.neighbours(rank, world, periodic)
+        eng = FakePeerSlab(u, r0, n, nb.lower is None, nb.upper is None, out_dir, rank)
+        drv = slab.DistPeerSlabs(eng, nb)
+        assert set(drv.mapped) == {s for s, o in ((abi.YLO, nb.lower), (abi.YHI, nb.upper)) if o is not None}
+        drv.step(2)
+        drv.step(4)
+        np.save(os.path.join(out_dir, f"r{rank}.npy"), eng.interior())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [1, 2, 4])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_gloo_peer_ranks_match_one_slab(world, periodic):
+    """DistPeerSlabs over gloo ranks on CPU: each rank maps its neighbours'
+    buffers (shared files standing in for CUDA IPC), stores its edge rows into
+    their ghost rows during the stage, and orders the stages with token
+    all-reduces; the gathered slabs equal the one-slab run bit for bit."""
+    ref, _ = run_local(initial(), 1, periodic)
+    with tempfile.TemporaryDirectory() as d:
+        port = 29900 + (os.getpid() % 500) + 5 * world + (1 if periodic else 0)
+        mp.start_processes(_gloo_peer_worker, args=(world, periodic, port, d), nprocs=world, join=True,
                            start_method="spawn")
         got = np.concatenate([np.load(os.path.join(d, f"r{k}.npy")) for k in range(world)])
     assert np.array_equal(got, ref)
