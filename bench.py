@@ -28,9 +28,12 @@ GEMM.  `cpu_baseline` times the CPU oracle (the reference's algorithm
 restated in C++, OpenMP over the host cores) on a bounded sample of the same
 workload, and the serial oracle on one core.
 
-Under torchrun (N > 1) every rank advances its own replica of the case (weak
-scaling, no data-path collective), timing is the max over ranks, and `value`
-counts the cells of all ranks.
+Under torchrun (N > 1) the 4096^2 grid is split into N row slabs, one per
+GPU (strong scaling): each stage stores its edge rows straight into the
+neighbouring GPUs' ghost rows over CUDA IPC peer mappings, an 8-byte NCCL
+all-reduce orders the stages, timing is the max over ranks, and `value`
+counts the grid's cells.  `--replicas` restores one replica per GPU (weak
+scaling); `--slabs K` runs K slabs on one GPU.
 """
 from __future__ import annotations
 
@@ -374,6 +377,108 @@ def run_batch(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_slabs(args, rank, world, local):
+    """One grid split into row slabs (strong scaling): one slab per GPU under
+    torchrun (DistPeerSlabs: CUDA IPC peers, token all-reduces ordering the
+    stages), or `--slabs K` slabs on one GPU (PeerLocalSlabs: stream events).
+    Each stage stores its edge rows straight into the neighbours' ghost rows
+    (efvm_set_halo_peer), so no pack / send / receive / unpack runs between
+    stages.  `value` counts the grid's cells over the max over ranks of the
+    device time; e2e uploads every slab from pinned memory, steps, downloads."""
+    import datetime
+    import torch
+    from dev_field_efvm_b200 import abi, slab
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    grid, params, u, ex, desc = workload(args.workload, args.size)
+    cells = grid.nx * grid.ny
+    n_slabs = world if world > 1 else args.slabs
+    parts = slab.split_rows(grid.ny, n_slabs)
+    per_y = grid.bc[abi.YLO].kind == abi.BC_PERIODIC
+    mine = [parts[rank]] if world > 1 else parts
+
+    def build():
+        engines = []
+        for r0, rows in mine:
+            e = slab.DeviceSlab(grid, params, r0, rows)
+            e.ctx.upload(u[r0:r0 + rows])
+            engines.append(e)
+        if world > 1:
+            return engines, slab.DistPeerSlabs(engines[0], slab.neighbours(rank, world, per_y))
+        return engines, slab.PeerLocalSlabs(engines, per_y)
+
+    engines, drv = build()
+    drv.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    n0 = sum(e.ctx.launch_count() for e in engines)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in engines]
+    with ClockSampler(local) as clocks:
+        for (a, _), e in zip(ev, engines):
+            a.record(e.stream)
+        drv.step(args.steps)
+        for (_, b), e in zip(ev, engines):
+            b.record(e.stream)
+        torch.cuda.synchronize()
+    ms = max(a.elapsed_time(b) for a, b in ev)
+    launches = sum(e.ctx.launch_count() for e in engines) - n0
+    st = engines[0].ctx.solver_state()
+    # end to end: every slab's rows up from pinned memory, one step, down again
+    host = [torch.from_numpy(np.ascontiguousarray(u[r0:r0 + rows])).pin_memory() for r0, rows in mine]
+    n_e2e = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        for e, h, (r0, rows) in zip(engines, host, mine):
+            e.ctx.upload_ptr(h.data_ptr(), 5, 5 * grid.nx, 1)
+        drv.primed = False  # the uploaded rows' ghosts come from one exchange
+        drv.step(1)
+        for e, h in zip(engines, host):
+            e.ctx.download_ptr(h.data_ptr(), 5, 5 * grid.nx, 1)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(t[0].item()), float(t[1].item())
+        lt = torch.tensor([launches], dtype=torch.int64, device="cuda")
+        dist.all_reduce(lt)
+        launches = int(lt.item())
+        dist.barrier()
+        del drv
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    value = cells * args.steps / (ms * 1e-3)
+    peak, peak_kind = measured_peaks()
+    achieved = cells * 256.0 / (ms / args.steps * 1e-3) / 1e9 / max(world, 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(desc, parallelism=f"slabs{n_slabs}" + ("" if world > 1 else " on one GPU"),
+                       halo="fused into the stage kernels (peer stores into the neighbours' ghost rows)",
+                       l2="inputs larger than L2 (537 MB per state buffer)", time=st.time,
+                       final_step=int(st.step)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind,
+                     "kernel": "whole steps per GPU (256 algorithmic B per cell-update over the step time)"},
+        "cpu_baseline": None,
+        "e2e": {"value": cells * n_e2e / e2e_s, "unit": UNIT, "h2d_bytes_per_step": cells * 5 * 8,
+                "d2h_bytes_per_step": cells * 5 * 8, "steps": n_e2e,
+                "note": "every slab uploaded from pinned memory, one step, downloaded"},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def with_params(params, **changes):
     from dev_field_efvm_b200 import abi
     p = abi.make_params(**{f: getattr(params, f) for f, _ in abi.EfvmParams._fields_})
@@ -530,6 +635,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the density-error leg (profiler captures)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 512-case batch leg of the default line")
+    ap.add_argument("--slabs", type=int, default=1,
+                    help="vortex workloads on one GPU: split the grid into this many row slabs with the halo "
+                         "exchange fused into the stage kernels")
+    ap.add_argument("--replicas", action="store_true",
+                    help="under torchrun: one replica of the case per GPU (weak scaling) instead of row slabs")
     ap.add_argument("--size", type=int, default=None,
                     help="vortex workloads only: a smaller n x n (x n) grid of the same case "
                          "(for profiler captures)")
@@ -549,6 +659,9 @@ def main():
         return
     if args.workload == "batch512":
         run_batch(args, rank, world, local)
+        return
+    if args.workload == "vortex4096" and ((world > 1 and not args.replicas) or (world == 1 and args.slabs > 1)):
+        run_slabs(args, rank, world, local)
         return
 
     import torch
