@@ -350,9 +350,9 @@ struct GlobalSrc {
 };
 
 // TmaSrc reads them from the block's shared-memory row ring (efvm_tma.cuh),
-// which TMA fills one iteration ahead: before the first read of row r the warp
+// which TMA fills ahead of use: before the first read of row r the warp
 // waits for its slot (wait_row), at the start of iteration j thread 0 loads row
-// j + 3 into the slot that row j - 1 held (refill), and at the end of iteration
+// j - 1 + RING into the slot that row j - 1 held (refill), and at the end of iteration
 // j every warp releases row j (release).
 struct TmaSrc {
     double* ring;
@@ -377,7 +377,7 @@ struct TmaSrc {
     __device__ __forceinline__ void issue(int r) {
         const int s = slot(r);
         double* base = ring + s * SLOT_D;
-        const bool with_u0 = map_u0 != nullptr && r >= u0_lo && r < u0_hi;
+        const bool with_u0 = tma::U0_IN_RING && map_u0 != nullptr && r >= u0_lo && r < u0_hi;
         tma::arrive_expect(&full[s], tma::IN_BYTES + (with_u0 ? tma::U0_BYTES : 0));
         tma::load_3d(base, map_in, x_in, r + YO, 0, &full[s]);
         if (with_u0) tma::load_3d(base + tma::IN_BYTES / 8, map_u0, x_u0, r + YO, 0, &full[s]);
@@ -396,8 +396,11 @@ struct TmaSrc {
         const double* p = row(jj) + (ii - col0);
         return U4{p[0], p[tma::IN_COLS], p[2 * tma::IN_COLS], p[3 * tma::IN_COLS]};
     }
-    __device__ __forceinline__ double u0v(int v, long long, int i, int j) const {
-        return row(j)[tma::IN_BYTES / 8 + v * tma::U0_COLS + (i - col0 - 2)];
+    const double* u0;           // U^n in global memory (when the ring holds no U^n rows)
+    long long plane;
+    __device__ __forceinline__ double u0v(int v, long long o, int i, int j) const {
+        if constexpr (tma::U0_IN_RING) return row(j)[tma::IN_BYTES / 8 + v * tma::U0_COLS + (i - col0 - 2)];
+        else return u0[v * plane + o];
     }
     // Every lane waits; the warp goes on only if all of them saw the row land.
     __device__ __forceinline__ bool wait_row(int r) {
@@ -408,7 +411,7 @@ struct TmaSrc {
     }
     __device__ __forceinline__ void refill(int j) {
         if (!producer || !ok) return;
-        const int r = j + 3;
+        const int r = j - 1 + tma::RING;  // into the slot that row j - 1 held
         if (r > last) return;
         if (j - 1 >= first && !tma::wait(&empty[slot(j - 1)], parity(j - 1))) {
             fail();
@@ -793,6 +796,8 @@ __global__ void __launch_bounds__(32 * WPB, MINB)
     src.empty = src.full + tma::RING;
     src.map_in = &map_in;
     src.map_u0 = with_u0 ? &map_u0 : nullptr;
+    src.u0 = a.u0;
+    src.plane = a.g.plane;
     src.st = a.st;
     src.first = jb - 2;
     src.last = je + 1;

@@ -11,8 +11,8 @@
 //
 // Row r of the block's row stream lives in slot (r - first) % RING.  The loop
 // of iteration j reads rows j, j+1 and j+2; at its start thread 0 waits until
-// every warp has released row j-1 and loads row j+3 into that slot, one
-// iteration ahead of its first use.
+// every warp has released row j-1 and loads row j-1+RING into that slot, ahead
+// of its first use.
 //
 // Every wait is bounded: one that runs out sets bit 3 of the context's
 // nonphysical word (reported as EFVM_ERR_TIMEOUT), and the block stops
@@ -26,12 +26,15 @@
 namespace efvm {
 namespace tma {
 
-constexpr int RING = 4;                          // row slots
+constexpr int RING = 4;                          // row slots (a power of two)
 constexpr int IN_COLS = 128;                     // stage-input columns per slot (124 + 2 x 2 halo)
 constexpr int U0_COLS = 124;                     // U^n columns per slot (the block's own cells)
 constexpr int IN_BYTES = 4 * IN_COLS * 8;        // 4096
 constexpr int U0_BYTES = 4 * U0_COLS * 8;        // 3968
-constexpr int SLOT_BYTES = IN_BYTES + U0_BYTES;  // 8064 = 63 x 128
+// U^n rows in the ring (true), or read from global memory in the epilogue
+// (false: 4 KB slots, so more slots or blocks fit the SM's shared memory)
+constexpr bool U0_IN_RING = true;
+constexpr int SLOT_BYTES = IN_BYTES + (U0_IN_RING ? U0_BYTES : 0);  // 8064 = 63 x 128
 constexpr int SMEM_BYTES = RING * SLOT_BYTES + 2 * RING * 8;
 constexpr uint32_t WAIT_LIMIT = 1u << 22;        // polls of a wait before it gives up (seconds)
 constexpr int TIMEOUT_BIT = 8;                   // DevState::nonphysical bit of a wait that ran out
