@@ -494,9 +494,9 @@ def tune(ctx, d3):
     if d3:
         return None
     ms = ctx.autotune_stage(5)
-    form, rows = ctx.stage_tiling()
+    form, rows, blocks = ctx.stage_tiling()
     return {"form": "tma" if form == abi.STAGE_TMA else "strip", "rows_per_warp": rows,
-            "tuner_ms_per_step": ms}
+            "blocks_per_sm": blocks, "tuner_ms_per_step": ms}
 
 
 def fp32_leg(args, grid, params, u, ex, flush, world, cells):

@@ -94,6 +94,7 @@ struct efvm_ctx {
     bool tmaps = false;
     int stage_form = EFVM_STAGE_AUTO;
     int stage_rows = 0;
+    int stage_blocks = 0;
     // halo peers of a slab (efvm_set_halo_peer): per y side the neighbour's
     // three state buffers, their plane and the neighbour's rows
     double* peer_bufs[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -541,6 +542,7 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
         a.tmap_u0 = &c->tmap_u0;
     }
     a.rows = c->stage_rows;
+    a.blocks = c->stage_blocks;
     for (int side = 0; side < 2; ++side) {
         if (!c->peer_bufs[side][0]) continue;
         for (int k = 0; k < 3; ++k)
@@ -1727,8 +1729,12 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
     return EFVM_OK;
 }
 
-int efvm_set_stage_tiling(efvm_ctx* c, int32_t form, int32_t rows_per_warp) {
+int efvm_set_stage_tiling(efvm_ctx* c, int32_t form, int32_t rows_per_warp, int32_t blocks_per_sm) {
     if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    const bool fp32 = c->ph.precision == EFVM_PREC_FP32_FLUX, visc = c->ph.viscous != 0;
+    if (blocks_per_sm != 0 && blocks_per_sm != stage_blocks_per_sm(fp32, visc, false) &&
+        blocks_per_sm != stage_alt_blocks(fp32, visc) && blocks_per_sm != stage_blocks_per_sm(fp32, visc, true))
+        return fail(c, EFVM_ERR_INVALID_ARG, "blocks_per_sm must be 0 or a count the case's stage forms are built for");
     if (form < EFVM_STAGE_AUTO || form > EFVM_STAGE_TMA)
         return fail(c, EFVM_ERR_INVALID_ARG, "form must be EFVM_STAGE_AUTO, EFVM_STAGE_STRIP or EFVM_STAGE_TMA");
     if (rows_per_warp < 0 || rows_per_warp > 65536)
@@ -1737,23 +1743,41 @@ int efvm_set_stage_tiling(efvm_ctx* c, int32_t form, int32_t rows_per_warp) {
         return fail(c, EFVM_ERR_UNSUPPORTED, "the TMA-fed stage kernel needs a 2-D context with tensor maps");
     c->stage_form = form;
     c->stage_rows = rows_per_warp;
+    c->stage_blocks = blocks_per_sm;
     c->graph_valid = false;
     return EFVM_OK;
 }
 
-int efvm_get_stage_tiling(efvm_ctx* c, int32_t* form, int32_t* rows_per_warp) {
-    if (!c || !form || !rows_per_warp) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+// The blocks per SM a stage of this context runs with: the strip form's
+// alternate count when it was selected, else the form's built-in count.
+static int resolved_blocks(const efvm_ctx* c, int form) {
+    const bool fp32 = c->ph.precision == EFVM_PREC_FP32_FLUX, visc = c->ph.viscous != 0;
+    const int alt = stage_alt_blocks(fp32, visc);
+    if (form == EFVM_STAGE_STRIP && alt > 0 && c->stage_blocks == alt) return alt;
+    return stage_blocks_per_sm(fp32, visc, form == EFVM_STAGE_TMA);
+}
+
+int efvm_get_stage_tiling(efvm_ctx* c, int32_t* form, int32_t* rows_per_warp, int32_t* blocks_per_sm) {
+    if (!c || !form || !rows_per_warp || !blocks_per_sm) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     *form = resolved_form(c);
+    *blocks_per_sm = resolved_blocks(c, *form);
     *rows_per_warp = c->stage_rows > 0 ? c->stage_rows
                                        : stage_rows(c->g.nx, c->g.ny, c->ph.precision == EFVM_PREC_FP32_FLUX,
                                                     c->ph.viscous != 0, *form == EFVM_STAGE_TMA);
+    if (c->stage_rows <= 0 && *blocks_per_sm != stage_blocks_per_sm(c->ph.precision == EFVM_PREC_FP32_FLUX,
+                                                                     c->ph.viscous != 0, *form == EFVM_STAGE_TMA)) {
+        // the built-in rows follow the resident slots of the count in use
+        const long long strips = stage_strips(c->g.nx), slots = 148LL * *blocks_per_sm * 4;
+        *rows_per_warp = (int)std::min<long long>(16, std::max<long long>(2, (strips * c->g.ny + slots - 1) / slots));
+    }
     return EFVM_OK;
 }
 
 // Times whole steps of every candidate tiling on the live state and keeps the
-// fastest: the strip kernel and (where the case allows it) the TMA-fed kernel,
-// each with 4, 8, 16 and 32 rows per warp and with the rows that fit the whole
-// grid into one wave of resident blocks.  The state, the clock and the force
+// fastest: the strip kernel at its built-in and its alternate resident-block
+// count and (where the case allows it) the TMA-fed kernel, each with 4, 8, 16
+// and 32 rows per warp and with the rows that fit the whole grid into one wave
+// of resident blocks.  The state, the clock and the force
 // outputs are saved first and restored after every candidate, so tuning
 // changes no result.
 int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) {
@@ -1791,12 +1815,20 @@ int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) 
     cudaEvent_t e0, e1;
     CUDA_TRY(c, cudaEventCreate(&e0));
     CUDA_TRY(c, cudaEventCreate(&e1));
-    const int saved_form = c->stage_form, saved_rows = c->stage_rows;
+    const int saved_form = c->stage_form, saved_rows = c->stage_rows, saved_blocks = c->stage_blocks;
     float best = 1e30f;
-    int best_form = saved_form, best_rows = saved_rows;
-    for (int form : forms) {
+    int best_form = saved_form, best_rows = saved_rows, best_blocks = saved_blocks;
+    // (form, resident blocks per SM) pairs: the strip form at its built-in count
+    // and at its alternate one, the TMA form at its own
+    std::vector<std::pair<int, int>> shapes{{EFVM_STAGE_STRIP, 0}};
+    const int alt = stage_alt_blocks(fp32, c->ph.viscous != 0);
+    if (alt > 0) shapes.push_back({EFVM_STAGE_STRIP, alt});
+    for (int form : forms)
+        if (form == EFVM_STAGE_TMA) shapes.push_back({EFVM_STAGE_TMA, 0});
+    for (const auto& shape : shapes) {
+        const int form = shape.first, blocks = shape.second;
         // one wave: the rows that spread the grid's strips over every resident block once
-        const int minb = stage_blocks_per_sm(fp32, c->ph.viscous != 0, form == EFVM_STAGE_TMA);
+        const int minb = blocks > 0 ? blocks : stage_blocks_per_sm(fp32, c->ph.viscous != 0, form == EFVM_STAGE_TMA);
         const int bx = (stage_strips(c->g.nx) + 3) / 4;
         const int by = std::max(1, sms * minb / std::max(bx, 1));
         std::vector<int> rows{4, 8, 16, 32, (c->g.ny + by - 1) / by};
@@ -1806,6 +1838,7 @@ int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) 
             if (r > c->g.ny && r != rows.front()) continue;
             c->stage_form = form;
             c->stage_rows = r;
+            c->stage_blocks = blocks;
             rc = capture_step_graph(c);
             if (rc) break;
             CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, S(c)));  // warm-up
@@ -1826,6 +1859,7 @@ int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) 
                 best = ms;
                 best_form = form;
                 best_rows = r;
+                best_blocks = blocks;
             }
         }
         if (rc) break;
@@ -1836,6 +1870,7 @@ int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) 
     cudaFree(backup);
     c->stage_form = rc ? saved_form : best_form;
     c->stage_rows = rc ? saved_rows : best_rows;
+    c->stage_blocks = rc ? saved_blocks : best_blocks;
     c->graph_valid = false;
     if (rc) return rc;
     if (rc2) return rc2;

@@ -207,6 +207,7 @@ struct StageArgs {
     const void* tmap_in;
     const void* tmap_u0;
     int rows;                         // rows per warp; 0 = the built-in choice
+    int blocks;                       // resident blocks per SM of the strip form; 0 = the built-in choice
     // Slabs with halo peers (efvm_set_halo_peer): the output buffer of this
     // stage of the neighbouring slab below (0) and above (1), its plane and
     // rows; the stage stores its two edge rows straight into that slab's
@@ -268,8 +269,10 @@ int batch_form_blocks(bool fp32, bool viscous);
 // case that runs alone (fp32: the FP32-flux form; viscous: with viscous terms).
 int stage_strips(int nx);
 int stage_rows(int nx, int ny, bool fp32, bool viscous, bool tma = false);
-// Resident blocks per SM of the stage-kernel form (tma: the TMA-fed kernel).
+// Resident blocks per SM of the stage-kernel form (tma: the TMA-fed kernel), and
+// the strip form's second choice for the autotuner (0: none).
 int stage_blocks_per_sm(bool fp32, bool viscous, bool tma);
+int stage_alt_blocks(bool fp32, bool viscous);
 // Whether a stage of this case can run the TMA-fed kernel (2-D, inviscid, no
 // immersed bodies, no learned correction), and the tensor map of a state
 // buffer of the case's layout as a 3-D tensor (columns, rows, planes) with the

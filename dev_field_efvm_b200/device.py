@@ -77,8 +77,8 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.efvm_launch_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.efvm_profile_steps.argtypes = [vp, i64, dp]
-    L.efvm_set_stage_tiling.argtypes = [vp, i32, i32]
-    L.efvm_get_stage_tiling.argtypes = [vp, C.POINTER(i32), C.POINTER(i32)]
+    L.efvm_set_stage_tiling.argtypes = [vp, i32, i32, i32]
+    L.efvm_get_stage_tiling.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.efvm_autotune_stage.argtypes = [vp, i32, dp]
     L.efvm_create_slab.argtypes = [C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), i32, i32, C.POINTER(vp)]
     L.efvm_prepare.argtypes = [vp]
@@ -268,15 +268,15 @@ class Context:
         self._check(self.L.efvm_profile_steps(self.h, int(n_steps), _dp(out)))
         return out
 
-    def set_stage_tiling(self, form: int = abi.STAGE_AUTO, rows_per_warp: int = 0) -> None:
-        """Stage-kernel form (abi.STAGE_*) and rows per warp (0: built-in)."""
-        self._check(self.L.efvm_set_stage_tiling(self.h, int(form), int(rows_per_warp)))
+    def set_stage_tiling(self, form: int = abi.STAGE_AUTO, rows_per_warp: int = 0, blocks_per_sm: int = 0) -> None:
+        """Stage-kernel form (abi.STAGE_*), rows per warp and blocks per SM (0: built-in)."""
+        self._check(self.L.efvm_set_stage_tiling(self.h, int(form), int(rows_per_warp), int(blocks_per_sm)))
 
-    def stage_tiling(self) -> tuple[int, int]:
-        """(form the next stage runs, its rows per warp)."""
-        f, r = C.c_int32(), C.c_int32()
-        self._check(self.L.efvm_get_stage_tiling(self.h, C.byref(f), C.byref(r)))
-        return f.value, r.value
+    def stage_tiling(self) -> tuple[int, int, int]:
+        """(form the next stage runs, its rows per warp, its blocks per SM)."""
+        f, r, b = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.L.efvm_get_stage_tiling(self.h, C.byref(f), C.byref(r), C.byref(b)))
+        return f.value, r.value, b.value
 
     def autotune_stage(self, n_steps: int = 3) -> float:
         """Keep the fastest stage tiling (state restored); device ms per step."""

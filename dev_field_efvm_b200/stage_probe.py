@@ -33,7 +33,7 @@ def main() -> None:
         c.set_stage_tiling(FORMS[args.form], args.rows)
         c.upload(u)
         c.step(args.steps)
-        form, rows = c.stage_tiling()
+        form, rows, _ = c.stage_tiling()
         print(f"{args.steps} steps of the {args.n}^2 vortex, {args.precision}, "
               f"form {'tma' if form == abi.STAGE_TMA else 'strip'}, {rows} rows per warp: "
               f"step {c.solver_state().step}")

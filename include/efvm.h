@@ -356,15 +356,18 @@ int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
  * (the forms differ from each other by a few ulps at most; a form gives the
  * same bits for any rows per warp). */
 typedef enum { EFVM_STAGE_AUTO = 0, EFVM_STAGE_STRIP = 1, EFVM_STAGE_TMA = 2 } efvm_stage_form;
-/* Select the form and the rows each warp marches (0 = built-in choice).  The
- * reference runs its systems on the CPU and has no counterpart; this replaces
- * no call.  EFVM_ERR_UNSUPPORTED for EFVM_STAGE_TMA on a 3-D context. */
-int efvm_set_stage_tiling(efvm_ctx* ctx, int32_t form, int32_t rows_per_warp);
-/* The form the context's next stage runs and its rows per warp. */
-int efvm_get_stage_tiling(efvm_ctx* ctx, int32_t* form, int32_t* rows_per_warp);
+/* Select the form, the rows each warp marches and the strip form's resident
+ * blocks per SM (0 = built-in choice for each; the FP64 inviscid strip form is
+ * built for 6 and 7 blocks, every other form for one count).  The reference
+ * runs its systems on the CPU and has no counterpart; this replaces no call.
+ * EFVM_ERR_UNSUPPORTED for EFVM_STAGE_TMA on a 3-D context. */
+int efvm_set_stage_tiling(efvm_ctx* ctx, int32_t form, int32_t rows_per_warp, int32_t blocks_per_sm);
+/* The form the context's next stage runs, its rows per warp and blocks per SM. */
+int efvm_get_stage_tiling(efvm_ctx* ctx, int32_t* form, int32_t* rows_per_warp, int32_t* blocks_per_sm);
 /* Time n_steps whole steps (default 3) of every candidate tiling on the live
- * state -- each form the case allows, with 4, 8, 16 and 32 rows per warp and
- * with the rows that put the whole grid in one wave of resident blocks -- and
+ * state -- each form the case allows (the strip form at each block count it is
+ * built for), with 4, 8, 16 and 32 rows per warp and with the rows that put the
+ * whole grid in one wave of resident blocks -- and
  * keep the fastest.  The state, the clock and the force outputs are restored
  * after every candidate, so tuning changes no result.  2-D RK3 contexts at a
  * step boundary without slabs or a flux correction; *best_ms_per_step (may be

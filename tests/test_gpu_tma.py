@@ -158,8 +158,8 @@ def test_autotune_restores_state_and_clock():
     before, s_before = d.download(), d.solver_state()
     ms = d.autotune_stage(2)
     assert ms > 0.0
-    form, rows = d.stage_tiling()
-    assert form in (abi.STAGE_STRIP, abi.STAGE_TMA) and rows >= 1
+    form, rows, blocks = d.stage_tiling()
+    assert form in (abi.STAGE_STRIP, abi.STAGE_TMA) and rows >= 1 and blocks in (6, 7)
     assert np.array_equal(d.download(), before)
     s_after = d.solver_state()
     assert (s_after.step, s_after.time, s_after.dt) == (s_before.step, s_before.time, s_before.dt)
@@ -168,3 +168,23 @@ def test_autotune_restores_state_and_clock():
     ref.upload(u)
     ref.step(5)
     assert rel_err(d.download(), ref.download()) < 1e-13
+
+
+def test_strip_form_at_its_alternate_block_count_matches_oracle():
+    """The FP64 inviscid strip form is also built for 7 resident blocks per SM
+    (the autotuner's second count); it holds the same 1e-12 bar, and a count no
+    form is built for is refused."""
+    from dev_field_efvm_b200.device import EfvmError
+
+    grid, params, u, ex = cases.vortex_case(200, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4, ny=77)
+    o = po.OracleCase(grid, params)
+    o.upload(u)
+    d = Context(grid, params)
+    d.set_stage_tiling(abi.STAGE_STRIP, 0, 7)
+    assert d.stage_tiling()[0] == abi.STAGE_STRIP and d.stage_tiling()[2] == 7
+    d.upload(u)
+    o.step(1)
+    d.step(1)
+    assert rel_err(d.download(), o.download()) < TOL_ONE_STEP
+    with pytest.raises(EfvmError):
+        d.set_stage_tiling(abi.STAGE_STRIP, 0, 5)
