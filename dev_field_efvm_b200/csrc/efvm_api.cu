@@ -95,6 +95,8 @@ struct efvm_ctx {
     int stage_form = EFVM_STAGE_AUTO;
     int stage_rows = 0;
     int stage_blocks = 0;
+    unsigned long long stage_wait_ns = 4000000000ull;  // one TMA ring wait (efvm_set_stage_wait_limit)
+    int stage_stall = 0;                               // efvm_inject_stage_stall
     // halo peers of a slab (efvm_set_halo_peer): per y side the neighbour's
     // three state buffers, their plane and the neighbour's rows
     double* peer_bufs[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -543,6 +545,8 @@ void enqueue_stage_kernel(efvm_ctx* c, int stage, double* uin, double* uout, boo
     }
     a.rows = c->stage_rows;
     a.blocks = c->stage_blocks;
+    a.wait_ns = c->stage_wait_ns;
+    a.stall = c->stage_stall;
     for (int side = 0; side < 2; ++side) {
         if (!c->peer_bufs[side][0]) continue;
         for (int k = 0; k < 3; ++k)
@@ -1875,6 +1879,21 @@ int efvm_autotune_stage(efvm_ctx* c, int32_t n_steps, double* best_ms_per_step) 
     if (rc) return rc;
     if (rc2) return rc2;
     if (best_ms_per_step) *best_ms_per_step = best / n_steps;
+    return EFVM_OK;
+}
+
+int efvm_set_stage_wait_limit(efvm_ctx* c, double seconds) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    if (!(seconds > 0.0) || seconds > 600.0) return fail(c, EFVM_ERR_INVALID_ARG, "the limit must be in (0, 600] s");
+    c->stage_wait_ns = (unsigned long long)(seconds * 1e9);
+    c->graph_valid = false;
+    return EFVM_OK;
+}
+
+int efvm_inject_stage_stall(efvm_ctx* c, int32_t enable) {
+    if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
+    c->stage_stall = enable != 0;
+    c->graph_valid = false;
     return EFVM_OK;
 }
 

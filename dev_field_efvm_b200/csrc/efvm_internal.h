@@ -208,6 +208,8 @@ struct StageArgs {
     const void* tmap_u0;
     int rows;                         // rows per warp; 0 = the built-in choice
     int blocks;                       // resident blocks per SM of the strip form; 0 = the built-in choice
+    unsigned long long wait_ns;       // limit of one wait of the TMA-fed kernel for a row (ns)
+    int stall;                        // failure injection: the first block's ring stops being refilled
     // Slabs with halo peers (efvm_set_halo_peer): the output buffer of this
     // stage of the neighbouring slab below (0) and above (1), its plane and
     // rows; the stage stores its two edge rows straight into that slab's

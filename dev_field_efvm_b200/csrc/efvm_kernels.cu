@@ -367,7 +367,9 @@ struct TmaSrc {
     int col0;                   // interior column of input slot column 0
     int scol;                   // this lane's input slot column
     int issued;                 // producer: the last row issued
+    unsigned long long wait_ns; // limit of one wait
     bool producer;
+    bool stall;                 // failure injection: the producer issues no row after the first RING
     bool ok;
 
     static constexpr int SLOT_D = tma::SLOT_BYTES / 8;
@@ -404,16 +406,16 @@ struct TmaSrc {
     }
     // Every lane waits; the warp goes on only if all of them saw the row land.
     __device__ __forceinline__ bool wait_row(int r) {
-        const bool got = ok && tma::wait(&full[slot(r)], parity(r));
+        const bool got = ok && tma::wait(&full[slot(r)], parity(r), wait_ns);
         if (__all_sync(0xffffffffu, got)) return true;
         if (ok) fail();
         return false;
     }
     __device__ __forceinline__ void refill(int j) {
-        if (!producer || !ok) return;
+        if (!producer || !ok || stall) return;
         const int r = j - 1 + tma::RING;  // into the slot that row j - 1 held
         if (r > last) return;
-        if (j - 1 >= first && !tma::wait(&empty[slot(j - 1)], parity(j - 1))) {
+        if (j - 1 >= first && !tma::wait(&empty[slot(j - 1)], parity(j - 1), wait_ns)) {
             fail();
             return;
         }
@@ -427,7 +429,7 @@ struct TmaSrc {
     // every copy it issued, so that none lands after the block is gone.
     __device__ __forceinline__ void drain() {
         for (int r = max(first, issued - (tma::RING - 1)); r <= issued; ++r)
-            if (!tma::wait(&full[slot(r)], parity(r))) return;
+            if (!tma::wait(&full[slot(r)], parity(r), wait_ns)) return;
     }
 };
 
@@ -809,6 +811,8 @@ __global__ void __launch_bounds__(32 * WPB, MINB)
     src.scol = 0;
     src.issued = src.first - 1;
     src.producer = threadIdx.x == 0;
+    src.wait_ns = a.wait_ns;
+    src.stall = a.stall && blockIdx.x == 0 && blockIdx.y == 0;
     src.ok = true;
     if (threadIdx.x == 0) {
         tma::prefetch_map(&map_in);

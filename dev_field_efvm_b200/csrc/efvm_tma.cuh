@@ -36,7 +36,7 @@ constexpr int U0_BYTES = 4 * U0_COLS * 8;        // 3968
 constexpr bool U0_IN_RING = true;
 constexpr int SLOT_BYTES = IN_BYTES + (U0_IN_RING ? U0_BYTES : 0);  // 8064 = 63 x 128
 constexpr int SMEM_BYTES = RING * SLOT_BYTES + 2 * RING * 8;
-constexpr uint32_t WAIT_LIMIT = 1u << 22;        // polls of a wait before it gives up (seconds)
+constexpr uint32_t WAIT_LIMIT = 1u << 26;        // polls of a wait before it gives up, whatever the time
 constexpr int TIMEOUT_BIT = 8;                   // DevState::nonphysical bit of a wait that ran out
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -66,10 +66,20 @@ __device__ __forceinline__ bool try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return done != 0;
 }
-// Bounded wait for phase `parity` of *bar; false if it ran out.
-__device__ __forceinline__ bool wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for phase `parity` of *bar: false once limit_ns have passed
+// (or WAIT_LIMIT polls, whichever comes first).
+__device__ __forceinline__ bool wait(uint64_t* bar, uint32_t parity, unsigned long long limit_ns) {
+    if (try_wait(bar, parity)) return true;
+    const unsigned long long t0 = now_ns();
+    for (uint32_t it = 1; it < WAIT_LIMIT; ++it) {
         if (try_wait(bar, parity)) return true;
+        if ((it & 31u) == 0u && now_ns() - t0 > limit_ns) return false;
+    }
     return false;
 }
 // One 3-D tile (x, y, plane) of a tensor map into shared memory, completing on *bar.

@@ -23,7 +23,7 @@ EXPORTS = (
     "efvm_download_state", "efvm_upload_state_3d", "efvm_download_state_3d", "efvm_set_spheres", "efvm_set_discs", "efvm_get_solver_state", "efvm_set_solver_state", "efvm_substep", "efvm_step",
     "efvm_cfl", "efvm_set_cylinders", "efvm_marker_force", "efvm_wall_force", "efvm_ibm_counts", "efvm_get_solid_mask",
     "efvm_density_error", "efvm_init_vortex", "efvm_total_mass", "efvm_get_stream", "efvm_launch_count",
-    "efvm_profile_steps", "efvm_set_stage_tiling", "efvm_get_stage_tiling", "efvm_autotune_stage", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
+    "efvm_profile_steps", "efvm_set_stage_tiling", "efvm_get_stage_tiling", "efvm_autotune_stage", "efvm_set_stage_wait_limit", "efvm_inject_stage_stall", "efvm_create_slab", "efvm_prepare", "efvm_halo_pack", "efvm_halo_unpack",
     "efvm_wave_speed_slot", "efvm_get_state_buffers", "efvm_set_halo_peer", "efvm_get_state_ipc", "efvm_set_halo_peer_ipc", "efvm_batch_create", "efvm_batch_destroy", "efvm_batch_last_error",
     "efvm_batch_upload_state", "efvm_batch_download_state", "efvm_batch_get_solver_state", "efvm_batch_run",
     "efvm_batch_launch_count", "efvm_batch_get_stream", "efvm_batch_set_autotune", "efvm_batch_get_rows",
@@ -80,6 +80,8 @@ def load(path: str | None = None) -> C.CDLL:
     L.efvm_set_stage_tiling.argtypes = [vp, i32, i32, i32]
     L.efvm_get_stage_tiling.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.efvm_autotune_stage.argtypes = [vp, i32, dp]
+    L.efvm_set_stage_wait_limit.argtypes = [vp, C.c_double]
+    L.efvm_inject_stage_stall.argtypes = [vp, i32]
     L.efvm_create_slab.argtypes = [C.POINTER(abi.EfvmGrid), C.POINTER(abi.EfvmParams), i32, i32, C.POINTER(vp)]
     L.efvm_prepare.argtypes = [vp]
     L.efvm_halo_pack.argtypes = [vp, i32, vp]
@@ -277,6 +279,13 @@ class Context:
         f, r, b = C.c_int32(), C.c_int32(), C.c_int32()
         self._check(self.L.efvm_get_stage_tiling(self.h, C.byref(f), C.byref(r), C.byref(b)))
         return f.value, r.value, b.value
+
+    def set_stage_wait_limit(self, seconds: float) -> None:
+        self._check(self.L.efvm_set_stage_wait_limit(self.h, float(seconds)))
+
+    def inject_stage_stall(self, enable: bool) -> None:
+        """Test hook: the TMA-fed stage's first block stops refilling its ring."""
+        self._check(self.L.efvm_inject_stage_stall(self.h, 1 if enable else 0))
 
     def autotune_stage(self, n_steps: int = 3) -> float:
         """Keep the fastest stage tiling (state restored); device ms per step."""

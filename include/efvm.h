@@ -374,6 +374,16 @@ int efvm_get_stage_tiling(efvm_ctx* ctx, int32_t* form, int32_t* rows_per_warp, 
  * NULL) receives the winner's device time per step.  No counterpart in the
  * reference. */
 int efvm_autotune_stage(efvm_ctx* ctx, int32_t n_steps, double* best_ms_per_step);
+/* Limit of one wait of the TMA-fed stage kernel for a row of its ring (default
+ * 4 s, far above any real wait).  A wait that runs out ends the stage's march
+ * in that block and the next status read returns EFVM_ERR_TIMEOUT; the GPU and
+ * other contexts stay usable.  No counterpart in the reference. */
+int efvm_set_stage_wait_limit(efvm_ctx* ctx, double seconds);
+/* Failure injection for tests: enable != 0 makes the first block of the
+ * TMA-fed stage stop refilling its ring after the first rows, so its waits run
+ * out (EFVM_ERR_TIMEOUT).  The state is then meaningless.  No counterpart in
+ * the reference. */
+int efvm_inject_stage_stall(efvm_ctx* ctx, int32_t enable);
 
 /* ---- slabs of one grid on several GPUs ------------------------------------ */
 

@@ -188,3 +188,30 @@ def test_strip_form_at_its_alternate_block_count_matches_oracle():
     assert rel_err(d.download(), o.download()) < TOL_ONE_STEP
     with pytest.raises(EfvmError):
         d.set_stage_tiling(abi.STAGE_STRIP, 0, 5)
+
+
+def test_ring_wait_that_runs_out_reports_a_timeout():
+    """The ring's waits are bounded in time (efvm_set_stage_wait_limit).  With
+    the first block's refills withheld (efvm_inject_stage_stall) its warps wait
+    for a row that never comes; each wait ends after the limit, the step
+    reports EFVM_ERR_TIMEOUT within a few limits, and the GPU stays usable: a
+    fresh context on it matches the oracle."""
+    import time
+    from dev_field_efvm_b200.device import EfvmError
+
+    grid, params, u, ex = cases.vortex_case(256, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4)
+    d = tma_context(grid, params, u)
+    d.set_stage_wait_limit(0.05)
+    d.inject_stage_stall(True)
+    t0 = time.perf_counter()
+    with pytest.raises(EfvmError) as e:
+        d.step(1)
+    assert e.value.code == abi.ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 10.0
+    d.close()
+    o = po.OracleCase(grid, params)
+    o.upload(u)
+    f = tma_context(grid, params, u)
+    o.step(1)
+    f.step(1)
+    assert rel_err(f.download(), o.download()) < TOL_ONE_STEP
