@@ -294,6 +294,12 @@ def _vortex(seam, muscl=True):
     return lambda: cases.vortex_case(64, periodic=True, muscl=muscl, mean=(1.0, 1.0), cfl=0.4, seam=seam)
 
 
+def _vortex_fp32():
+    """FP32 fluxes: the built-in stage form is the TMA-fed kernel, with the peer stores in its epilogue."""
+    return cases.vortex_case(256, periodic=True, muscl=True, mean=(1.0, 1.0), cfl=0.4, precision=abi.PREC_FP32_FLUX,
+                             ny=96)
+
+
 def _channel():
     grid, params, u, ex = cases.poiseuille_case(ny=32, nx=8)
     params.reconstruction = abi.RECON_MUSCL
@@ -326,6 +332,7 @@ def test_device_slabs_match_unsplit_context(name, builder, steps):
     ("vortex_muscl_reference_seam", _vortex(abi.SEAM_REFERENCE), 8),
     ("vortex_muscl_true_periodic", _vortex(abi.SEAM_TRUE_PERIODIC), 8),
     ("channel_walls_viscous_muscl", _channel, 8),
+    ("vortex_fp32_flux_tma_form", _vortex_fp32, 6),
 ])
 def test_halo_peer_slabs_match_unsplit_context(name, builder, steps):
     """The exchange fused into the stage kernels (efvm_set_halo_peer): each
