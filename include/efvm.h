@@ -369,7 +369,8 @@ int efvm_get_stage_tiling(efvm_ctx* ctx, int32_t* form, int32_t* rows_per_warp, 
  * built for), with 4, 8, 16 and 32 rows per warp and with the rows that put the
  * whole grid in one wave of resident blocks -- and
  * keep the fastest.  The state, the clock and the force outputs are restored
- * after every candidate, so tuning changes no result.  2-D RK3 contexts at a
+ * after every candidate, so tuning changes no result; the call holds a
+ * temporary device copy of the state (4 planes) while it runs.  2-D RK3 contexts at a
  * step boundary without slabs or a flux correction; *best_ms_per_step (may be
  * NULL) receives the winner's device time per step.  No counterpart in the
  * reference. */
