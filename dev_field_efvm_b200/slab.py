@@ -278,7 +278,8 @@ class PeerLocalSlabs:
     in its input have been written, and its own stores cannot overtake their
     reads of the buffer it writes.  One pack / unpack exchange fills the ghost
     rows of the uploaded state before the first step; the wave-speed slot is
-    max-reduced once per step as in LocalTransport."""
+    max-reduced once per step on the device, ordered by events, so a run of
+    steps makes no host round trip."""
 
     def __init__(self, engines, periodic_y: bool):
         self.engines = engines
@@ -290,8 +291,28 @@ class PeerLocalSlabs:
                     bufs, plane, rows = engines[other].ctx.state_buffers()
                     e.ctx.set_halo_peer(side, bufs, plane, rows)
         self.events = [[torch.cuda.Event() for _ in engines] for _ in range(2)]
+        self.rstream = torch.cuda.Stream()
+        self.prepared = [torch.cuda.Event() for _ in engines]
+        self.reduced = torch.cuda.Event()
         self.stage = 0
         self.primed = False
+
+    def _reduce(self) -> None:
+        """Max of the slabs' wave-speed words on the device: after every slab's
+        set-up work (and so after its last stage), before any slab's next stage,
+        with no host round trip (the words are the bits of non-negative doubles,
+        so their integer max is the max wave speed)."""
+        for ev, e in zip(self.prepared, self.engines):
+            ev.record(e.stream)
+            self.rstream.wait_event(ev)
+        with torch.cuda.stream(self.rstream):
+            words = [e.slot() for e in self.engines]
+            m = torch.stack(words).max(dim=0).values
+            for w in words:
+                w.copy_(m)
+        self.reduced.record(self.rstream)
+        for e in self.engines:
+            e.stream.wait_event(self.reduced)
 
     def step(self, n_steps: int) -> None:
         if not self.primed:  # the ghost rows of the uploaded state
@@ -302,7 +323,7 @@ class PeerLocalSlabs:
         for _ in range(n_steps):
             for e in self.engines:
                 e.prepare()
-            self.local.reduce()
+            self._reduce()
             for _s in range(3):
                 prev, cur = self.events[(self.stage + 1) % 2], self.events[self.stage % 2]
                 for k, e in enumerate(self.engines):
