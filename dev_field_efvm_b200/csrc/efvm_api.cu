@@ -509,12 +509,11 @@ int prologue(efvm_ctx* c) {
 
 // The stage-kernel form a context runs.  The TMA-fed kernel runs where it is
 // selected and the case allows it (2-D, inviscid, no bodies, no learned
-// correction); EFVM_STAGE_AUTO selects it for the FP32-flux form, where it
-// measured 4 % faster than the strip kernel at 4096^2, and keeps the strip
-// kernel for FP64, where the ring's extra registers made it 4 % slower.
+// correction); EFVM_STAGE_AUTO selects it in both precisions: at 4096^2 it
+// measured 1.70 against 1.85 ms per step (FP32 fluxes) and 2.26 against 2.47
+// (FP64) for the strip kernel.
 int resolved_form(const efvm_ctx* c) {
-    const bool want = c->stage_form == EFVM_STAGE_TMA ||
-                      (c->stage_form == EFVM_STAGE_AUTO && c->ph.precision == EFVM_PREC_FP32_FLUX);
+    const bool want = c->stage_form == EFVM_STAGE_TMA || c->stage_form == EFVM_STAGE_AUTO;
     if (want && c->tmaps && stage_tma_eligible(c->g, c->ph, c->ibm, c->nn != nullptr)) return EFVM_STAGE_TMA;
     return EFVM_STAGE_STRIP;
 }
@@ -1736,9 +1735,16 @@ int efvm_profile_steps(efvm_ctx* c, int64_t n_steps, double out_ms[4]) {
 int efvm_set_stage_tiling(efvm_ctx* c, int32_t form, int32_t rows_per_warp, int32_t blocks_per_sm) {
     if (!c) return fail(c, EFVM_ERR_INVALID_ARG, "null argument");
     const bool fp32 = c->ph.precision == EFVM_PREC_FP32_FLUX, visc = c->ph.viscous != 0;
-    if (blocks_per_sm != 0 && blocks_per_sm != stage_blocks_per_sm(fp32, visc, false) &&
-        blocks_per_sm != stage_alt_blocks(fp32, visc) && blocks_per_sm != stage_blocks_per_sm(fp32, visc, true))
-        return fail(c, EFVM_ERR_INVALID_ARG, "blocks_per_sm must be 0 or a count the case's stage forms are built for");
+    // a count the selected form is built for (the strip form: its built-in and
+    // alternate counts; the TMA-fed form: its own; AUTO: any of them)
+    const bool strip_count = blocks_per_sm == stage_blocks_per_sm(fp32, visc, false) ||
+                             blocks_per_sm == stage_alt_blocks(fp32, visc);
+    const bool tma_count = blocks_per_sm == stage_blocks_per_sm(fp32, visc, true);
+    const bool count_ok = blocks_per_sm == 0 || (form == EFVM_STAGE_STRIP && strip_count) ||
+                          (form == EFVM_STAGE_TMA && tma_count) ||
+                          (form == EFVM_STAGE_AUTO && (strip_count || tma_count));
+    if (!count_ok)
+        return fail(c, EFVM_ERR_INVALID_ARG, "blocks_per_sm must be 0 or a count the selected stage form is built for");
     if (form < EFVM_STAGE_AUTO || form > EFVM_STAGE_TMA)
         return fail(c, EFVM_ERR_INVALID_ARG, "form must be EFVM_STAGE_AUTO, EFVM_STAGE_STRIP or EFVM_STAGE_TMA");
     if (rows_per_warp < 0 || rows_per_warp > 65536)

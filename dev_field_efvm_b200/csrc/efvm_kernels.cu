@@ -24,6 +24,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 
@@ -274,17 +275,31 @@ __device__ __forceinline__ Q4<R> yq(const V4<R>& u) {
 // (limited_slope_cons and reconstruct_to_face, crates/cfd_solver/src/lib.rs:199-211,273-286);
 // m/c/p are the previous/own/next cells along the face normal.  The FP32 path
 // takes the differences in FP32.
+//
+// fp and fm scale the slope of the two states: 0.5 where the face on that side
+// reconstructs this cell, 0 where it takes the cell value itself (a first-order
+// side on the domain edge), so the edge faces need no select of whole states.
+// c + s fp and c - s fm are each one multiply-add; with fp = fm = 0.5 the
+// product is exact, so they are the bits of c + (s/2) and c - (s/2), and with 0
+// they are c.
 template <class R>
 __device__ __forceinline__ R half_slope(int limiter, R m, R c, R p) {
     return limit<R>(limiter, p - c, c - m) * R(0.5);
 }
+__device__ __forceinline__ double fma_(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fma_(float a, float b, float c) { return fmaf(a, b, c); }
 template <class R>
-__device__ __forceinline__ void slope_faces(int limiter, const V4<R>& m, const V4<R>& c, const V4<R>& p, V4<R>& plus,
-                                            V4<R>& minus) {
-    const R hr = half_slope(limiter, m.r, c.r, p.r), hx = half_slope(limiter, m.mx, c.mx, p.mx);
-    const R hy = half_slope(limiter, m.my, c.my, p.my), he = half_slope(limiter, m.E, c.E, p.E);
-    plus = V4<R>{c.r + hr, c.mx + hx, c.my + hy, c.E + he};
-    minus = V4<R>{c.r - hr, c.mx - hx, c.my - hy, c.E - he};
+__device__ __forceinline__ void slope_faces(int limiter, const V4<R>& m, const V4<R>& c, const V4<R>& p, R fp, R fm,
+                                            V4<R>& plus, V4<R>& minus) {
+    const R sr = limit<R>(limiter, p.r - c.r, c.r - m.r), sx = limit<R>(limiter, p.mx - c.mx, c.mx - m.mx);
+    const R sy = limit<R>(limiter, p.my - c.my, c.my - m.my), se = limit<R>(limiter, p.E - c.E, c.E - m.E);
+    plus = V4<R>{fma_(sr, fp, c.r), fma_(sx, fp, c.mx), fma_(sy, fp, c.my), fma_(se, fp, c.E)};
+    minus = V4<R>{fma_(-sr, fm, c.r), fma_(-sx, fm, c.mx), fma_(-sy, fm, c.my), fma_(-se, fm, c.E)};
+}
+// The slope factor of a side that a face does (0.5) or does not (0) reconstruct.
+template <class R>
+__device__ __forceinline__ R rec_factor(bool rec) {
+    return rec ? R(0.5) : R(0);
 }
 
 template <class R>
@@ -493,20 +508,47 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         auto ld = [&](int ii, int jj) { return src.at(g, ii, jj); };
         auto ldrow = [&](int jj) { return toR<R>(src.col(jj)); };
 
-        // Reconstruction flags of the faces on the domain edge; every interior
-        // face reconstructs both sides under MUSCL.  x: this lane's face, between
-        // columns i-1 and i.  y: the faces below row 0 and above row ny-1.
-        bool rec_l = MUSCL, rec_r = MUSCL;
+        // What a lane carries from one row to the next (the flux of the y face
+        // below the row, in the face frame, and the row's +y face state) and,
+        // within a row, the x part of the flux divergence while the y face is
+        // formed.  The FP32-flux forms keep them in registers.  The FP64 forms
+        // keep them in shared memory, one slot per thread (12 doubles, 12 KB per
+        // block): that frees 24 registers through both flux evaluations, halves
+        // the FP64 inviscid form's spills, and took the 4096^2 vortex from 2.64
+        // to 2.52 ms per step (FP32 fluxes: 1.73 -> 1.90 ms, so not there).
+        constexpr bool CARRY_SMEM = FP64;
+        __shared__ double carry_s[CARRY_SMEM ? 12 : 1][32 * WPB];
+        const int tq = threadIdx.x;
+
+        // Which sides of the faces on the domain edge are reconstructed; every
+        // interior face reconstructs both sides under MUSCL.  x: this lane's face,
+        // between columns i-1 and i, takes column i-1's +x state (rec_l) and
+        // column i's -x state (rec_r), or the cell values where they are false.
+        // y: the faces below row 0 and above row ny-1, whose flags become the
+        // slope factors of the row states (fy_below, fy_above).
+        bool rec_l = true, rec_r = true;  // face i: column i-1's +x state, column i's -x state
         if (i == 0) {
-            rec_l = MUSCL && ph.periodic_x && true_seam;
-            rec_r = MUSCL && ph.periodic_x;
+            rec_l = ph.periodic_x && true_seam;
+            rec_r = ph.periodic_x;
         } else if (i == g.nx) {
-            rec_l = MUSCL && ph.periodic_x;
-            rec_r = MUSCL && ph.periodic_x && true_seam;
+            rec_l = ph.periodic_x;
+            rec_r = ph.periodic_x && true_seam;
         }
         const bool y_periodic = ph.periodic_y || ph.seam_ylo || ph.seam_yhi;
-        const bool seam_rec = MUSCL && y_periodic && true_seam;  // the side across the periodic seam
-        const bool edge_rec = MUSCL && y_periodic;               // the side inside the domain
+        const bool seam_rec = y_periodic && true_seam;  // the side across the periodic seam
+        const bool edge_rec = y_periodic;               // the side inside the domain
+        // y face above row jj: the slope factors of its lower side (row jj's +y
+        // state) and of its upper side (row jj+1's -y state); an edge between
+        // slabs is an interior face.  Warp-uniform.
+        const bool lo_edge_rows = !ph.halo_ylo || ph.seam_ylo, hi_edge_rows = !ph.halo_yhi || ph.seam_yhi;
+        auto fy_below = [&](int jj) {
+            const bool lo = jj == -1 && lo_edge_rows, hi = jj + 1 == g.ny && hi_edge_rows;
+            return rec_factor<R>(lo ? seam_rec : (hi ? edge_rec : true));
+        };
+        auto fy_above = [&](int jj) {
+            const bool lo = jj == -1 && lo_edge_rows, hi = jj + 1 == g.ny && hi_edge_rows;
+            return rec_factor<R>(lo ? edge_rec : (hi ? seam_rec : true));
+        };
 
         // Row window of this lane's column: uc = U(j), un = U(j+1); pc = +y face
         // state of row j; gb = flux of the y-face below row j (face frame).  Each
@@ -518,15 +560,49 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         V4<R> uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
         if (MUSCL) {
             V4<R> unused;
-            slope_faces(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
+            slope_faces(ph.limiter, ldrow(jb - 2), uc, un, fy_below(jb - 1), R(0), pc, unused);
         }
         src.release(jb - 2);
         const double dt = gld<CG>(&a.st->dt);  // set by the step's set-up, constant during the stage
         Q4<R> gb{R(0), R(0), R(0), R(0)};
+        // carry slots: 0-3 gb (r, mn, mt, E), 4-7 pc (r, mx, my, E), 8-11 the x part
+        auto put_gb = [&](const Q4<R>& q) {
+            if constexpr (CARRY_SMEM) {
+                carry_s[0][tq] = q.r; carry_s[1][tq] = q.mn; carry_s[2][tq] = q.mt; carry_s[3][tq] = q.E;
+            } else {
+                gb = q;
+            }
+        };
+        auto get_gb = [&]() {
+            if constexpr (CARRY_SMEM) return Q4<R>{carry_s[0][tq], carry_s[1][tq], carry_s[2][tq], carry_s[3][tq]};
+            else return gb;
+        };
+        auto put_pc = [&](const V4<R>& u) {
+            if constexpr (CARRY_SMEM) {
+                carry_s[4][tq] = u.r; carry_s[5][tq] = u.mx; carry_s[6][tq] = u.my; carry_s[7][tq] = u.E;
+            } else {
+                pc = u;
+            }
+        };
+        auto get_pc = [&]() {
+            if constexpr (CARRY_SMEM) return V4<R>{carry_s[4][tq], carry_s[5][tq], carry_s[6][tq], carry_s[7][tq]};
+            else return pc;
+        };
+        put_gb(gb);
+        if (MUSCL) put_pc(pc);
         for (int j = jb - 1; rows_ok && j < je; ++j) {
             src.refill(j);
             if (!src.wait_row(j + 2)) break;
-            const V4<R> un2 = ldrow(j + 2);
+            // Rows j, j+1 and j+2 of the window.  The FP64 TMA-fed form reads
+            // them from the ring at each use instead of holding them through the
+            // row: with the carry in shared memory that left it no spills at 80
+            // registers, and took the 4096^2 vortex from 2.64 (strip form) to
+            // 2.26 ms per step.  The other forms hold them in registers.
+            constexpr bool REREAD = FP64 && std::is_same<SRC, TmaSrc>::value;
+            const V4<R> un2 = REREAD ? V4<R>{} : ldrow(j + 2);
+            auto row_c = [&]() { if constexpr (REREAD) return ldrow(j); else return uc; };
+            auto row_n = [&]() { if constexpr (REREAD) return ldrow(j + 1); else return un; };
+            auto row_n2 = [&]() { if constexpr (REREAD) return ldrow(j + 2); else return un2; };
             const bool row = j >= jb;  // warp-uniform: the first pass only forms the face below row jb
 
             // ---- x-face on the left of column i, row j, and the divergence of
@@ -538,9 +614,17 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
             // fluxes of neighbouring faces) and one multiply-add, a few ulps from
             // the reference's sequential sum.  Only the x part stays live through
             // the y-face flux below.
-            double part[4];
+            double part_r[4];
+            auto put_part = [&](int v, double x) {
+                if constexpr (CARRY_SMEM) carry_s[8 + v][tq] = x;
+                else part_r[v] = x;
+            };
+            auto get_part = [&](int v) {
+                if constexpr (CARRY_SMEM) return carry_s[8 + v][tq];
+                else return part_r[v];
+            };
             auto x_face = [&]() {
-                V4<R> ul = shfl_up_v(uc, 1), ur = shfl_down_v(uc, 1);
+                V4<R> ul = shfl_up_v(row_c(), 1), ur = shfl_down_v(row_c(), 1);
                 V4<R> ull = ul;  // column i-2 (lane 0 only)
                 if (lane == 0) {
                     ul = toR<R>(ld(i0 - 1, j));
@@ -550,53 +634,47 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                 Q4<R> fx;
                 if (MUSCL) {
                     V4<R> pp, mm;  // this column's +x and -x face states
-                    slope_faces(ph.limiter, ul, uc, ur, pp, mm);
+                    slope_faces(ph.limiter, ul, row_c(), ur, R(0.5), R(0.5), pp, mm);
                     V4<R> lp = shfl_up_v(pp, 1);  // +x state of column i-1
                     if (lane == 0) {
                         V4<R> unused;
-                        slope_faces(ph.limiter, ull, ul, uc, lp, unused);
+                        slope_faces(ph.limiter, ull, ul, row_c(), R(0.5), R(0), lp, unused);
                     }
-                    fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : uc), rg, rgm1);
+                    fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : row_c()), rg, rgm1);
                 } else {
-                    fx = face_flux<SCHEME, R>(xq(ul), xq(uc), rg, rgm1);
+                    fx = face_flux<SCHEME, R>(xq(ul), xq(row_c()), rg, rgm1);
                 }
                 const Q4<R> fxr = shfl_down_q(fx, 1);  // face on the right of column i
                 const double fl[4] = {(double)fx.r, (double)fx.mn, (double)fx.mt, (double)fx.E};
                 const double fr[4] = {(double)fxr.r, (double)fxr.mn, (double)fxr.mt, (double)fxr.E};
 #pragma unroll
-                for (int v = 0; v < 4; ++v) part[v] = (fl[v] - fr[v]) * g.inv_x;
+                for (int v = 0; v < 4; ++v) put_part(v, (fl[v] - fr[v]) * g.inv_x);
             };
             Q4<R> gt;
-            V4<R> pn = un;  // +y face state of row j+1
-            // faces on the domain's y edges; an edge between slabs is an interior face
-            auto y_edge_rec = [&](bool& rb, bool& rt) {
-                const bool lo_edge = j == -1 && (!ph.halo_ylo || ph.seam_ylo);
-                const bool hi_edge = j + 1 == g.ny && (!ph.halo_yhi || ph.seam_yhi);
-                rb = lo_edge ? seam_rec : (hi_edge ? edge_rec : true);
-                rt = lo_edge ? edge_rec : (hi_edge ? seam_rec : true);
-            };
+            V4<R> pn = row_n();  // +y face state of row j+1
             if (XFIRST && row) x_face();
             // ---- y-face above row j ----
             if (MUSCL) {
                 V4<R> mn;
-                slope_faces(ph.limiter, uc, un, un2, pn, mn);
-                bool rb, rt;
-                y_edge_rec(rb, rt);
-                gt = face_flux<SCHEME, R>(yq(rb ? pc : uc), yq(rt ? mn : un), rg, rgm1);
+                const V4<R> pcr = get_pc();
+                slope_faces(ph.limiter, row_c(), row_n(), row_n2(), fy_below(j + 1), fy_above(j), pn, mn);
+                put_pc(pn);
+                gt = face_flux<SCHEME, R>(yq(pcr), yq(mn), rg, rgm1);
             } else {
-                gt = face_flux<SCHEME, R>(yq(uc), yq(un), rg, rgm1);
+                gt = face_flux<SCHEME, R>(yq(row_c()), yq(row_n()), rg, rgm1);
             }
             if (!XFIRST && row) x_face();
 
             if (row && owner) {
                 const long long o = cidx(g, i, j);
                 // the cell's state in FP64 (the FP32 path reads it again)
-                const U4 ucd = FP64 ? toU4(uc) : ld(i, j);
+                const U4 ucd = FP64 ? toU4(row_c()) : ld(i, j);
                 const double gtv[4] = {(double)gt.r, (double)gt.mt, (double)gt.mn, (double)gt.E};
-                const double gbd[4] = {(double)gb.r, (double)gb.mt, (double)gb.mn, (double)gb.E};
+                const Q4<R> gbq = get_gb();
+                const double gbd[4] = {(double)gbq.r, (double)gbq.mt, (double)gbq.mn, (double)gbq.E};
                 double rhs[4];
 #pragma unroll
-                for (int v = 0; v < 4; ++v) rhs[v] = fma(gbd[v] - gtv[v], g.inv_y, part[v]);
+                for (int v = 0; v < 4; ++v) rhs[v] = fma(gbd[v] - gtv[v], g.inv_y, get_part(v));
                 if constexpr (CORR) {
                     // learned corrections of the four faces (periodic grid): the
                     // x face on the left of a cell, the y face below it
@@ -625,7 +703,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                     for (int k = 0; k < 4; ++k) sn[k] = ibm && a.mask[no[k]];
                     const double r0 = ucd.r, r1 = sn[0] ? 1.0 : gld<CG>(uin + no[0]),
                                  r2 = sn[1] ? 1.0 : gld<CG>(uin + no[1]);
-                    const double r3 = sn[2] ? 1.0 : (FP64 ? (double)un.r : gld<CG>(uin + no[2]));
+                    const double r3 = sn[2] ? 1.0 : (FP64 ? (double)row_n().r : gld<CG>(uin + no[2]));
                     const double r4 = sn[3] ? 1.0 : gld<CG>(uin + no[3]);
                     const double p1 = r0 * r1, p2 = p1 * r2, p3 = p2 * r3;
                     double w = rcp_(p3 * r4);
@@ -647,7 +725,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                         }
                         U4 q;
                         if (FP64 && k == 2) {
-                            q = toU4(un);
+                            q = toU4(row_n());
                         } else {
                             q.r = rn[k];
                             q.mx = gld<CG>(uin + P + no[k]);
@@ -745,10 +823,9 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                 if (a.completes_step && a.want_cfl) lam = fmax(lam, wave_speed(g, ph, nw));
             }
             src.release(j);
-            gb = gt;
+            put_gb(gt);
             uc = un;
             un = un2;
-            pc = pn;
         }
     }
     // wave-speed max for the next step's CFL dt: one atomic per warp
@@ -1552,9 +1629,11 @@ static void launch_stage_r(const StageArgs& a, bool pdl, cudaStream_t s) {
 }
 
 // ---- the TMA-fed stage kernel ----------------------------------------------
-// Resident blocks per SM: the shared-memory ring (32.3 KB per block) fits six
-// blocks in the SM's 228 KB, for both precisions.
+// Resident blocks per SM.  The kernels are built for six (80 registers).  The
+// FP32-flux form's shared memory is the ring (32.3 KB per block), so six fit in
+// the SM's 228 KB; the FP64 form adds its 12 KB row carry, and five fit.
 constexpr int TMA_MINB = 6;
+constexpr int tma_resident(bool fp32) { return fp32 ? TMA_MINB : 5; }
 
 bool stage_tma_eligible(const Geometry& g, const Physics& ph, bool ibm, bool corr) {
     return g.nz <= 1 && !ph.viscous && !ibm && !corr;
@@ -1573,7 +1652,7 @@ static void launch_stage_tma_t(const StageArgs& a, bool pdl, cudaStream_t s) {
                              (int)cudaSharedmemCarveoutMaxShared);
         carveout_set |= 1ull << dev;
     }
-    const int rows = a.rows > 0 ? a.rows : rows_per_warp(a.g.nx, a.g.ny, TMA_MINB);
+    const int rows = a.rows > 0 ? a.rows : rows_per_warp(a.g.nx, a.g.ny, tma_resident(sizeof(R) == sizeof(float)));
     const int strips = (a.g.nx + STRIP - 1) / STRIP;
     const dim3 grid((strips + WPB - 1) / WPB, (a.g.ny + rows - 1) / rows);
     const CUtensorMap* m_in = static_cast<const CUtensorMap*>(a.tmap_in);
@@ -1657,9 +1736,9 @@ int launch_stage(const StageArgs& a, bool pdl, void* stream) {
 int stage_strips(int nx) { return (nx + STRIP - 1) / STRIP; }
 
 int stage_rows(int nx, int ny, bool fp32, bool viscous, bool tma) {
-    return rows_per_warp(nx, ny, tma ? TMA_MINB : form_minb(fp32, viscous));
+    return rows_per_warp(nx, ny, tma ? tma_resident(fp32) : form_minb(fp32, viscous));
 }
-int stage_blocks_per_sm(bool fp32, bool viscous, bool tma) { return tma ? TMA_MINB : form_minb(fp32, viscous); }
+int stage_blocks_per_sm(bool fp32, bool viscous, bool tma) { return tma ? tma_resident(fp32) : form_minb(fp32, viscous); }
 
 int stage_alt_blocks(bool fp32, bool viscous) {
     return fp32 ? (viscous ? StageForm<float, true>::ALT : StageForm<float, false>::ALT)

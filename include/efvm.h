@@ -351,14 +351,16 @@ int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
  * (cp.async.bulk.tensor) into a shared-memory ring of rows one iteration ahead
  * of their use; it runs for cases without viscous terms, immersed bodies or a
  * flux correction, and the other cases run the strip form whatever is set.
- * EFVM_STAGE_AUTO is the built-in choice (the TMA-fed form for FP32 fluxes,
- * the strip form for FP64: the faster of the two at 4096^2).  Both give the reference's results
+ * EFVM_STAGE_AUTO is the built-in choice: the TMA-fed form wherever the case
+ * allows it (the faster of the two at 4096^2 in both precisions), else the
+ * strip form.  Both give the reference's results
  * (the forms differ from each other by a few ulps at most; a form gives the
  * same bits for any rows per warp). */
 typedef enum { EFVM_STAGE_AUTO = 0, EFVM_STAGE_STRIP = 1, EFVM_STAGE_TMA = 2 } efvm_stage_form;
 /* Select the form, the rows each warp marches and the strip form's resident
  * blocks per SM (0 = built-in choice for each; the FP64 inviscid strip form is
- * built for 6 and 7 blocks, every other form for one count).  The reference
+ * built for 6 and 7 blocks, every other form for one count; a count the
+ * selected form is not built for returns EFVM_ERR_INVALID_ARG).  The reference
  * runs its systems on the CPU and has no counterpart; this replaces no call.
  * EFVM_ERR_UNSUPPORTED for EFVM_STAGE_TMA on a 3-D context. */
 int efvm_set_stage_tiling(efvm_ctx* ctx, int32_t form, int32_t rows_per_warp, int32_t blocks_per_sm);

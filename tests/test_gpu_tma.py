@@ -159,7 +159,7 @@ def test_autotune_restores_state_and_clock():
     ms = d.autotune_stage(2)
     assert ms > 0.0
     form, rows, blocks = d.stage_tiling()
-    assert form in (abi.STAGE_STRIP, abi.STAGE_TMA) and rows >= 1 and blocks in (6, 7)
+    assert form in (abi.STAGE_STRIP, abi.STAGE_TMA) and rows >= 1 and blocks in (5, 6, 7)
     assert np.array_equal(d.download(), before)
     s_after = d.solver_state()
     assert (s_after.step, s_after.time, s_after.dt) == (s_before.step, s_before.time, s_before.dt)
