@@ -732,6 +732,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": peak_kind,
                 "kernel": ("stage3_kernel (fused 3-D MUSCL/HLLC/RK3 substage, x/y/z faces)" if d3
+                           else "stage_tma_kernel (fused MUSCL/HLLC/RK3 substage, rows fed by TMA into a "
+                                "shared-memory ring)" if tiling and tiling.get("form") == "tma"
                            else "stage_kernel (fused MUSCL/HLLC/RK3 substage)"),
                 "bytes_per_cell_update": bytes_per_cell_update, "cells_per_launch": cells,
                 "stage_ms_per_launch": stage_ms_per_launch,
