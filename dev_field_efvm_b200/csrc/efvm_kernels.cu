@@ -296,6 +296,17 @@ __device__ __forceinline__ void slope_faces(int limiter, const V4<R>& m, const V
     plus = V4<R>{fma_(sr, fp, c.r), fma_(sx, fp, c.mx), fma_(sy, fp, c.my), fma_(se, fp, c.E)};
     minus = V4<R>{fma_(-sr, fm, c.r), fma_(-sx, fm, c.mx), fma_(-sy, fm, c.my), fma_(-se, fm, c.E)};
 }
+// The same two states with both factors 0.5, as c + h and c - h of one half
+// slope h = s/2: the same bits as the factor form.  The FP32-flux forms and
+// the batch kernels use this one (the factor form raised their spills).
+template <class R>
+__device__ __forceinline__ void slope_faces_half(int limiter, const V4<R>& m, const V4<R>& c, const V4<R>& p,
+                                                 V4<R>& plus, V4<R>& minus) {
+    const R hr = half_slope(limiter, m.r, c.r, p.r), hx = half_slope(limiter, m.mx, c.mx, p.mx);
+    const R hy = half_slope(limiter, m.my, c.my, p.my), he = half_slope(limiter, m.E, c.E, p.E);
+    plus = V4<R>{c.r + hr, c.mx + hx, c.my + hy, c.E + he};
+    minus = V4<R>{c.r - hr, c.mx - hx, c.my - hy, c.E - he};
+}
 // The slope factor of a side that a face does (0.5) or does not (0) reconstruct.
 template <class R>
 __device__ __forceinline__ R rec_factor(bool rec) {
@@ -541,14 +552,21 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         // state) and of its upper side (row jj+1's -y state); an edge between
         // slabs is an interior face.  Warp-uniform.
         const bool lo_edge_rows = !ph.halo_ylo || ph.seam_ylo, hi_edge_rows = !ph.halo_yhi || ph.seam_yhi;
-        auto fy_below = [&](int jj) {
+        auto rec_below = [&](int jj) {
             const bool lo = jj == -1 && lo_edge_rows, hi = jj + 1 == g.ny && hi_edge_rows;
-            return rec_factor<R>(lo ? seam_rec : (hi ? edge_rec : true));
+            return lo ? seam_rec : (hi ? edge_rec : true);
         };
-        auto fy_above = [&](int jj) {
+        auto rec_above = [&](int jj) {
             const bool lo = jj == -1 && lo_edge_rows, hi = jj + 1 == g.ny && hi_edge_rows;
-            return rec_factor<R>(lo ? edge_rec : (hi ? seam_rec : true));
+            return lo ? edge_rec : (hi ? seam_rec : true);
         };
+        // The FP64 single-case forms take the y-edge flags as slope factors; the
+        // FP32-flux forms and the persistent batch kernel (CG) keep the select
+        // of whole states, which measured faster for them (FP32 strip form
+        // 37.5 against 36.6 ms per 20 steps at 4096^2).
+        constexpr bool Y_FACTORS = FP64 && !CG;
+        auto fy_below = [&](int jj) { return rec_factor<R>(rec_below(jj)); };
+        auto fy_above = [&](int jj) { return rec_factor<R>(rec_above(jj)); };
 
         // Row window of this lane's column: uc = U(j), un = U(j+1); pc = +y face
         // state of row j; gb = flux of the y-face below row j (face frame).  Each
@@ -560,7 +578,8 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         V4<R> uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
         if (MUSCL) {
             V4<R> unused;
-            slope_faces(ph.limiter, ldrow(jb - 2), uc, un, fy_below(jb - 1), R(0), pc, unused);
+            if constexpr (Y_FACTORS) slope_faces(ph.limiter, ldrow(jb - 2), uc, un, fy_below(jb - 1), R(0), pc, unused);
+            else slope_faces_half(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
         }
         src.release(jb - 2);
         const double dt = gld<CG>(&a.st->dt);  // set by the step's set-up, constant during the stage
@@ -634,11 +653,13 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                 Q4<R> fx;
                 if (MUSCL) {
                     V4<R> pp, mm;  // this column's +x and -x face states
-                    slope_faces(ph.limiter, ul, row_c(), ur, R(0.5), R(0.5), pp, mm);
+                    if constexpr (FP64) slope_faces(ph.limiter, ul, row_c(), ur, R(0.5), R(0.5), pp, mm);
+                    else slope_faces_half(ph.limiter, ul, row_c(), ur, pp, mm);
                     V4<R> lp = shfl_up_v(pp, 1);  // +x state of column i-1
                     if (lane == 0) {
                         V4<R> unused;
-                        slope_faces(ph.limiter, ull, ul, row_c(), R(0.5), R(0), lp, unused);
+                        if constexpr (FP64) slope_faces(ph.limiter, ull, ul, row_c(), R(0.5), R(0), lp, unused);
+                        else slope_faces_half(ph.limiter, ull, ul, row_c(), lp, unused);
                     }
                     fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : row_c()), rg, rgm1);
                 } else {
@@ -657,9 +678,15 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
             if (MUSCL) {
                 V4<R> mn;
                 const V4<R> pcr = get_pc();
-                slope_faces(ph.limiter, row_c(), row_n(), row_n2(), fy_below(j + 1), fy_above(j), pn, mn);
+                if constexpr (Y_FACTORS) slope_faces(ph.limiter, row_c(), row_n(), row_n2(), fy_below(j + 1), fy_above(j), pn, mn);
+                else slope_faces_half(ph.limiter, row_c(), row_n(), row_n2(), pn, mn);
                 put_pc(pn);
-                gt = face_flux<SCHEME, R>(yq(pcr), yq(mn), rg, rgm1);
+                if constexpr (Y_FACTORS) {
+                    gt = face_flux<SCHEME, R>(yq(pcr), yq(mn), rg, rgm1);
+                } else {
+                    const bool rb = rec_below(j), rt = rec_above(j);
+                    gt = face_flux<SCHEME, R>(yq(rb ? pcr : row_c()), yq(rt ? mn : row_n()), rg, rgm1);
+                }
             } else {
                 gt = face_flux<SCHEME, R>(yq(row_c()), yq(row_n()), rg, rgm1);
             }
