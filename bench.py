@@ -499,6 +499,15 @@ def tune(ctx, d3):
             "blocks_per_sm": blocks, "tuner_ms_per_step": ms}
 
 
+def hold_stream(n_steps):
+    """A sleep kernel on the current stream, long enough for the host to
+    enqueue the timed steps behind it: a short step (the cylinder's is ~90 us)
+    then never waits on the host between its events, so the events time the
+    device.  Outside every timed pair of events."""
+    import torch
+    torch.cuda._sleep(int(2.0e6 * max(5.0, 0.2 * n_steps)))  # ~2e6 cycles per ms
+
+
 def fp32_leg(args, grid, params, u, ex, flush, world, cells):
     """The chosen form on the same case: FP32 reconstruction and fluxes, FP64
     accumulation, device-timed as the FP64 leg."""
@@ -515,6 +524,7 @@ def fp32_leg(args, grid, params, u, ex, flush, world, cells):
     ev32 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
     with torch.cuda.stream(s32):
+        hold_stream(args.steps)
         for a, b in ev32:
             flush.zero_()
             a.record(s32)
@@ -697,6 +707,7 @@ def main():
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
         with torch.cuda.stream(stream):
+            hold_stream(args.steps)
             for a, b in evs:
                 flush.zero_()
                 a.record(stream)
@@ -804,6 +815,8 @@ def main():
                            l2=("inputs larger than L2 (537 MB per state buffer); L2 also flushed between timed steps "
                                "(256 MB write)") if cells * 32 > 126e6 else
                               "flushed between timed steps (256 MB write)",
+                           timing="CUDA events around each step on the context stream; the timed steps are "
+                                  "enqueued behind a sleep kernel so no host launch gap falls between events",
                            time=st.time, final_step=int(st.step)),
             "roofline": roofline,
             "stage_tiling": tiling,

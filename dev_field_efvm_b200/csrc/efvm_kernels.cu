@@ -527,8 +527,10 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         // block): that frees 24 registers through both flux evaluations, halves
         // the FP64 inviscid form's spills, and took the 4096^2 vortex from 2.64
         // to 2.52 ms per step (FP32 fluxes: 1.73 -> 1.90 ms, so not there).
-        constexpr bool CARRY_SMEM = FP64;
-        __shared__ double carry_s[CARRY_SMEM ? 12 : 1][32 * WPB];
+        constexpr bool CARRY_GB = FP64, CARRY_PC = FP64, CARRY_PART = FP64;
+        constexpr int SLOT_GB = 0, SLOT_PC = SLOT_GB + (CARRY_GB ? 4 : 0), SLOT_PART = SLOT_PC + (CARRY_PC ? 4 : 0);
+        constexpr int CARRY_SLOTS = SLOT_PART + (CARRY_PART ? 4 : 0);
+        __shared__ double carry_s[CARRY_SLOTS > 0 ? CARRY_SLOTS : 1][32 * WPB];
         const int tq = threadIdx.x;
 
         // Which sides of the faces on the domain edge are reconstructed; every
@@ -548,15 +550,18 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         const bool y_periodic = ph.periodic_y || ph.seam_ylo || ph.seam_yhi;
         const bool seam_rec = y_periodic && true_seam;  // the side across the periodic seam
         const bool edge_rec = y_periodic;               // the side inside the domain
-        // y face above row jj: the slope factors of its lower side (row jj's +y
-        // state) and of its upper side (row jj+1's -y state); an edge between
-        // slabs is an interior face.  Warp-uniform.
-        const bool lo_edge_rows = !ph.halo_ylo || ph.seam_ylo, hi_edge_rows = !ph.halo_yhi || ph.seam_yhi;
+        // y face above row jj: whether its lower side (row jj's +y state) and
+        // its upper side (row jj+1's -y state) are reconstructed; an edge between
+        // slabs is an interior face.  Warp-uniform.  (The edge conditions are
+        // read where they are used: hoisted out of the loop they made the batch
+        // kernels, whose physics is read from the case table, 6 % slower.)
         auto rec_below = [&](int jj) {
+            const bool lo_edge_rows = !ph.halo_ylo || ph.seam_ylo, hi_edge_rows = !ph.halo_yhi || ph.seam_yhi;
             const bool lo = jj == -1 && lo_edge_rows, hi = jj + 1 == g.ny && hi_edge_rows;
             return lo ? seam_rec : (hi ? edge_rec : true);
         };
         auto rec_above = [&](int jj) {
+            const bool lo_edge_rows = !ph.halo_ylo || ph.seam_ylo, hi_edge_rows = !ph.halo_yhi || ph.seam_yhi;
             const bool lo = jj == -1 && lo_edge_rows, hi = jj + 1 == g.ny && hi_edge_rows;
             return lo ? edge_rec : (hi ? seam_rec : true);
         };
@@ -586,25 +591,31 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         Q4<R> gb{R(0), R(0), R(0), R(0)};
         // carry slots: 0-3 gb (r, mn, mt, E), 4-7 pc (r, mx, my, E), 8-11 the x part
         auto put_gb = [&](const Q4<R>& q) {
-            if constexpr (CARRY_SMEM) {
-                carry_s[0][tq] = q.r; carry_s[1][tq] = q.mn; carry_s[2][tq] = q.mt; carry_s[3][tq] = q.E;
+            if constexpr (CARRY_GB) {
+                carry_s[SLOT_GB][tq] = q.r; carry_s[SLOT_GB + 1][tq] = q.mn;
+                carry_s[SLOT_GB + 2][tq] = q.mt; carry_s[SLOT_GB + 3][tq] = q.E;
             } else {
                 gb = q;
             }
         };
         auto get_gb = [&]() {
-            if constexpr (CARRY_SMEM) return Q4<R>{carry_s[0][tq], carry_s[1][tq], carry_s[2][tq], carry_s[3][tq]};
+            if constexpr (CARRY_GB)
+                return Q4<R>{carry_s[SLOT_GB][tq], carry_s[SLOT_GB + 1][tq], carry_s[SLOT_GB + 2][tq],
+                             carry_s[SLOT_GB + 3][tq]};
             else return gb;
         };
         auto put_pc = [&](const V4<R>& u) {
-            if constexpr (CARRY_SMEM) {
-                carry_s[4][tq] = u.r; carry_s[5][tq] = u.mx; carry_s[6][tq] = u.my; carry_s[7][tq] = u.E;
+            if constexpr (CARRY_PC) {
+                carry_s[SLOT_PC][tq] = u.r; carry_s[SLOT_PC + 1][tq] = u.mx;
+                carry_s[SLOT_PC + 2][tq] = u.my; carry_s[SLOT_PC + 3][tq] = u.E;
             } else {
                 pc = u;
             }
         };
         auto get_pc = [&]() {
-            if constexpr (CARRY_SMEM) return V4<R>{carry_s[4][tq], carry_s[5][tq], carry_s[6][tq], carry_s[7][tq]};
+            if constexpr (CARRY_PC)
+                return V4<R>{carry_s[SLOT_PC][tq], carry_s[SLOT_PC + 1][tq], carry_s[SLOT_PC + 2][tq],
+                             carry_s[SLOT_PC + 3][tq]};
             else return pc;
         };
         put_gb(gb);
@@ -635,11 +646,11 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
             // the y-face flux below.
             double part_r[4];
             auto put_part = [&](int v, double x) {
-                if constexpr (CARRY_SMEM) carry_s[8 + v][tq] = x;
+                if constexpr (CARRY_PART) carry_s[SLOT_PART + v][tq] = x;
                 else part_r[v] = x;
             };
             auto get_part = [&](int v) {
-                if constexpr (CARRY_SMEM) return carry_s[8 + v][tq];
+                if constexpr (CARRY_PART) return carry_s[SLOT_PART + v][tq];
                 else return part_r[v];
             };
             auto x_face = [&]() {
@@ -715,7 +726,10 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                         rhs[v] += ((double)cx[c] - (double)cx[cr]) * g.inv_x + ((double)cy[c] - (double)cy[ct]) * g.inv_y;
                     }
                 }
-                const bool ibm = a.mask != nullptr;
+                // the TMA-fed form runs only cases without bodies, a body force or
+                // a sponge: those paths are not compiled into it
+                constexpr bool LEAN = std::is_same<SRC, TmaSrc>::value;
+                const bool ibm = !LEAN && a.mask != nullptr;
                 const bool solid = ibm && a.mask[o];
                 if (VISC && !solid) {
                     // viscous_system, crates/cfd_solver/src/lib.rs:514-557 (z terms vanish in 2-D).
@@ -791,7 +805,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                     rhs[3] += us * fxv + vs * fyv + kappa * lt;
                 }
                 if (solid) rhs[0] = rhs[1] = rhs[2] = rhs[3] = 0.0;  // zero_solid_rhs, crates/cfd_ibm/src/lib.rs:293-301
-                if (ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
+                if (!LEAN && ph.body_force_x != 0.0) {  // crates/cfd_solver/tests/poiseuille_channel_validation.rs:100-118
                     rhs[1] += ucd.r * ph.body_force_x;
                     rhs[3] += ph.body_force_x * ucd.mx;
                 }
@@ -811,7 +825,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                 }
                 U4 nw{un_[0], un_[1], un_[2], un_[3]};
 
-                if (a.completes_step && ph.sponge) {
+                if (!LEAN && a.completes_step && ph.sponge) {
                     // outlet_sponge_system, examples/cylinder_drag_validation/main.rs:186-229
                     const double cx = centre(g.lo[0], g.h[0], i);
                     if (cx >= ph.sponge_x_start) {
@@ -1663,7 +1677,7 @@ constexpr int TMA_MINB = 6;
 constexpr int tma_resident(bool fp32) { return fp32 ? TMA_MINB : 5; }
 
 bool stage_tma_eligible(const Geometry& g, const Physics& ph, bool ibm, bool corr) {
-    return g.nz <= 1 && !ph.viscous && !ibm && !corr;
+    return g.nz <= 1 && !ph.viscous && !ibm && !corr && !ph.sponge && ph.body_force_x == 0.0;
 }
 
 template <int SCHEME, int RECON, class R>

@@ -349,8 +349,9 @@ int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
  * reads its rows, halo cells and U^n through L1/L2.  EFVM_STAGE_TMA: a block's
  * four warps march the same rows of four adjacent strips, fed by TMA
  * (cp.async.bulk.tensor) into a shared-memory ring of rows one iteration ahead
- * of their use; it runs for cases without viscous terms, immersed bodies or a
- * flux correction, and the other cases run the strip form whatever is set.
+ * of their use; it runs for cases without viscous terms, immersed bodies, a
+ * body force, an outlet sponge or a flux correction, and the other cases run
+ * the strip form whatever is set.
  * EFVM_STAGE_AUTO is the built-in choice: the TMA-fed form wherever the case
  * allows it (the faster of the two at 4096^2 in both precisions), else the
  * strip form.  Both give the reference's results
