@@ -149,11 +149,14 @@ __device__ __forceinline__ U4 bc_ghost(const DevBC& bc, int side, const U4& in, 
 // Boundary-ghost refill for the cell (i, j) whose new value is `u`: the Halo
 // (periodic wrap) and Boundary phases of the next substage, done by the thread
 // that owns the interior source cell (each ghost has exactly one writer).
+// PXY: both axes are known to be periodic at compile time (the TMA-fed form
+// of fully periodic cases), so the boundary-condition paths are not compiled.
+template <bool PXY = false>
 __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& ph, double* q, int i, int j,
                                              const U4& u) {
     const long long P = g.plane;
     const double gm1 = ph.gamma - 1.0;
-    if (ph.periodic_x) {
+    if (PXY || ph.periodic_x) {
         if (i >= g.nx - NG) store4(q, P, cidx(g, i - g.nx, j), u);
         if (i < NG) store4(q, P, cidx(g, i + g.nx, j), u);
     } else {
@@ -172,7 +175,7 @@ __device__ __forceinline__ void write_ghosts(const Geometry& g, const Physics& p
         }
         if (i == g.nx - 1) store4(q, P, cidx(g, g.nx, j), bc_ghost(ph.bc[1], 1, u, gm1));
     }
-    if (ph.periodic_y) {
+    if (PXY || ph.periodic_y) {
         if (j >= g.ny - NG) store4(q, P, cidx(g, i, j - g.ny), u);
         if (j < NG) store4(q, P, cidx(g, i, j + g.ny), u);
     } else {
@@ -474,7 +477,11 @@ struct TmaSrc {
 // on a step's last stage, the sponge, refills the boundary ghosts of the output
 // and takes the wave-speed max for the next step's CFL dt.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR, bool XFIRST, bool CG, class SRC>
+// LIM >= 0 fixes the limiter at compile time and PXY a fully periodic grid
+// (the TMA-fed form is built per limiter and for that case); -1 and false read
+// them from the physics at run time.
+template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR, bool XFIRST, bool CG, class SRC,
+          int LIM = -1, bool PXY = false>
 __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip, int by, SRC& src) {
     if (!(CG ? *(volatile const int*)&a.st->active : a.st->active)) return;
     const Geometry& g = a.g;
@@ -514,6 +521,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         const bool true_seam = ph.periodic_seam == EFVM_SEAM_TRUE_PERIODIC;
         const double gm1 = ph.gamma - 1.0;
         const R rg = R(ph.gamma), rgm1 = R(gm1);
+        const int limiter = LIM >= 0 ? LIM : ph.limiter;
         const double* __restrict__ uin = a.uin;  // the viscous neighbours
         src.bind(g, i, ic);
         auto ld = [&](int ii, int jj) { return src.at(g, ii, jj); };
@@ -583,8 +591,8 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         V4<R> uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
         if (MUSCL) {
             V4<R> unused;
-            if constexpr (Y_FACTORS) slope_faces(ph.limiter, ldrow(jb - 2), uc, un, fy_below(jb - 1), R(0), pc, unused);
-            else slope_faces_half(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
+            if constexpr (Y_FACTORS) slope_faces(limiter, ldrow(jb - 2), uc, un, fy_below(jb - 1), R(0), pc, unused);
+            else slope_faces_half(limiter, ldrow(jb - 2), uc, un, pc, unused);
         }
         src.release(jb - 2);
         const double dt = gld<CG>(&a.st->dt);  // set by the step's set-up, constant during the stage
@@ -664,13 +672,13 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                 Q4<R> fx;
                 if (MUSCL) {
                     V4<R> pp, mm;  // this column's +x and -x face states
-                    if constexpr (FP64) slope_faces(ph.limiter, ul, row_c(), ur, R(0.5), R(0.5), pp, mm);
-                    else slope_faces_half(ph.limiter, ul, row_c(), ur, pp, mm);
+                    if constexpr (FP64) slope_faces(limiter, ul, row_c(), ur, R(0.5), R(0.5), pp, mm);
+                    else slope_faces_half(limiter, ul, row_c(), ur, pp, mm);
                     V4<R> lp = shfl_up_v(pp, 1);  // +x state of column i-1
                     if (lane == 0) {
                         V4<R> unused;
-                        if constexpr (FP64) slope_faces(ph.limiter, ull, ul, row_c(), R(0.5), R(0), lp, unused);
-                        else slope_faces_half(ph.limiter, ull, ul, row_c(), lp, unused);
+                        if constexpr (FP64) slope_faces(limiter, ull, ul, row_c(), R(0.5), R(0), lp, unused);
+                        else slope_faces_half(limiter, ull, ul, row_c(), lp, unused);
                     }
                     fx = face_flux<SCHEME, R>(xq(rec_l ? lp : ul), xq(rec_r ? mm : row_c()), rg, rgm1);
                 } else {
@@ -689,8 +697,8 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
             if (MUSCL) {
                 V4<R> mn;
                 const V4<R> pcr = get_pc();
-                if constexpr (Y_FACTORS) slope_faces(ph.limiter, row_c(), row_n(), row_n2(), fy_below(j + 1), fy_above(j), pn, mn);
-                else slope_faces_half(ph.limiter, row_c(), row_n(), row_n2(), pn, mn);
+                if constexpr (Y_FACTORS) slope_faces(limiter, row_c(), row_n(), row_n2(), fy_below(j + 1), fy_above(j), pn, mn);
+                else slope_faces_half(limiter, row_c(), row_n(), row_n2(), pn, mn);
                 put_pc(pn);
                 if constexpr (Y_FACTORS) {
                     gt = face_flux<SCHEME, R>(yq(pcr), yq(mn), rg, rgm1);
@@ -846,7 +854,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
                 }
 
                 store4(a.uout, P, o, nw);
-                write_ghosts(g, ph, a.uout, i, j, nw);
+                write_ghosts<PXY>(g, ph, a.uout, i, j, nw);
                 peer_rows(a, g, i, j, nw);
 
                 // non-physical state flag (rho<=0, p<=0, NaN)
@@ -898,7 +906,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int 
 // shared-memory ring (efvm_tma.cuh) one iteration before they are read, so the
 // strip code's halo cells and U^n no longer wait on L2 and its rows come from
 // shared memory.  The arithmetic is the strip code's.
-template <int SCHEME, int RECON, class R, int MINB, bool XFIRST>
+template <int SCHEME, int RECON, class R, int MINB, bool XFIRST, int LIM, bool PXY>
 __global__ void __launch_bounds__(32 * WPB, MINB)
     stage_tma_kernel(StageArgs a, int rows, const __grid_constant__ CUtensorMap map_in,
                      const __grid_constant__ CUtensorMap map_u0) {
@@ -946,7 +954,7 @@ __global__ void __launch_bounds__(32 * WPB, MINB)
         for (int r = src.first; r < src.first + tma::RING && r <= src.last; ++r) src.issue(r);
     const int warp = threadIdx.x >> 5;
     if (warp < n_active)
-        stage_strip_src<SCHEME, RECON, R, false, StageArgs, false, XFIRST, false>(a, rows, blockIdx.x * WPB + warp,
+        stage_strip_src<SCHEME, RECON, R, false, StageArgs, false, XFIRST, false, TmaSrc, LIM, PXY>(a, rows, blockIdx.x * WPB + warp,
                                                                                   blockIdx.y, src);
     if (threadIdx.x == 0 && !src.ok) src.drain();
 }
@@ -1680,10 +1688,10 @@ bool stage_tma_eligible(const Geometry& g, const Physics& ph, bool ibm, bool cor
     return g.nz <= 1 && !ph.viscous && !ibm && !corr && !ph.sponge && ph.body_force_x == 0.0;
 }
 
-template <int SCHEME, int RECON, class R>
-static void launch_stage_tma_t(const StageArgs& a, bool pdl, cudaStream_t s) {
+template <int SCHEME, int RECON, class R, int LIM, bool PXY>
+static void launch_stage_tma_k(const StageArgs& a, bool pdl, cudaStream_t s) {
     constexpr bool XFIRST = StageForm<R, false>::XFIRST;
-    auto kernel = stage_tma_kernel<SCHEME, RECON, R, TMA_MINB, XFIRST>;
+    auto kernel = stage_tma_kernel<SCHEME, RECON, R, TMA_MINB, XFIRST, LIM, PXY>;
     // the largest shared-memory carve-out, once per device
     static unsigned long long carveout_set = 0;
     int dev = 0;
@@ -1699,6 +1707,26 @@ static void launch_stage_tma_t(const StageArgs& a, bool pdl, cudaStream_t s) {
     const CUtensorMap* m_in = static_cast<const CUtensorMap*>(a.tmap_in);
     const CUtensorMap* m_u0 = static_cast<const CUtensorMap*>(a.tmap_u0 ? a.tmap_u0 : a.tmap_in);
     launch_ks(kernel, grid, dim3(32 * WPB), (size_t)tma::SMEM_BYTES, s, pdl, a, rows, *m_in, *m_u0);
+}
+
+// The TMA-fed form is built per limiter (MUSCL) and for fully periodic grids,
+// so that those branches are decided at compile time: with the sponge, body
+// force and solid mask compiled out as well, the FP64 form's no_instruction and
+// branch_resolving stalls were the largest after the FP64 dependency chains.
+template <int SCHEME, int RECON, class R>
+static void launch_stage_tma_t(const StageArgs& a, bool pdl, cudaStream_t s) {
+    const bool pxy = a.ph.periodic_x && a.ph.periodic_y;
+    if constexpr (RECON == EFVM_RECON_MUSCL) {
+        if (a.ph.limiter == EFVM_LIMITER_MC)
+            pxy ? launch_stage_tma_k<SCHEME, RECON, R, EFVM_LIMITER_MC, true>(a, pdl, s)
+                : launch_stage_tma_k<SCHEME, RECON, R, EFVM_LIMITER_MC, false>(a, pdl, s);
+        else
+            pxy ? launch_stage_tma_k<SCHEME, RECON, R, EFVM_LIMITER_MINMOD, true>(a, pdl, s)
+                : launch_stage_tma_k<SCHEME, RECON, R, EFVM_LIMITER_MINMOD, false>(a, pdl, s);
+    } else {
+        pxy ? launch_stage_tma_k<SCHEME, RECON, R, -1, true>(a, pdl, s)
+            : launch_stage_tma_k<SCHEME, RECON, R, -1, false>(a, pdl, s);
+    }
 }
 
 template <class R>
