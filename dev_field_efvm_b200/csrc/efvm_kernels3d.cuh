@@ -83,26 +83,29 @@ __device__ __forceinline__ U5 bc_ghost5(const DevBC& bc, int side, const U5& in,
 
 // The Halo (periodic wrap of both ghost layers) and Boundary (first ghost
 // layer) phases for the ghosts whose source is interior cell (i, j, k) with
-// value u, written by the thread that owns that cell.
+// value u, written by the thread that owns that cell.  PXYZ: all three axes
+// are known to be periodic at compile time (the boundary-condition paths are
+// not compiled).
+template <bool PXYZ = false>
 __device__ __forceinline__ void write_ghosts3(const Geometry& g, const Physics& ph, double* q, int i, int j, int k,
                                               const U5& u) {
     const long long P = g.plane;
     const double gm1 = ph.gamma - 1.0;
-    if (ph.periodic_x) {
+    if (PXYZ || ph.periodic_x) {
         if (i >= g.nx - NG) store5(q, P, cidx3(g, i - g.nx, j, k), u);
         if (i < NG) store5(q, P, cidx3(g, i + g.nx, j, k), u);
     } else {
         if (i == 0) store5(q, P, cidx3(g, -1, j, k), bc_ghost5(ph.bc[0], 0, u, gm1));
         if (i == g.nx - 1) store5(q, P, cidx3(g, g.nx, j, k), bc_ghost5(ph.bc[1], 1, u, gm1));
     }
-    if (ph.periodic_y) {
+    if (PXYZ || ph.periodic_y) {
         if (j >= g.ny - NG) store5(q, P, cidx3(g, i, j - g.ny, k), u);
         if (j < NG) store5(q, P, cidx3(g, i, j + g.ny, k), u);
     } else {
         if (j == 0) store5(q, P, cidx3(g, i, -1, k), bc_ghost5(ph.bc[2], 2, u, gm1));
         if (j == g.ny - 1) store5(q, P, cidx3(g, i, g.ny, k), bc_ghost5(ph.bc[3], 3, u, gm1));
     }
-    if (ph.periodic_z) {
+    if (PXYZ || ph.periodic_z) {
         if (k >= g.nz - NG) store5(q, P, cidx3(g, i, j, k - g.nz), u);
         if (k < NG) store5(q, P, cidx3(g, i, j, k + g.nz), u);
     } else {
@@ -199,12 +202,15 @@ constexpr int MINB3 = 4;  // resident blocks per SM of the 3-D stage kernel (128
 // (its loads stay in bounds) and stores nothing; it only keeps the block's
 // barriers.
 // ---------------------------------------------------------------------------
-template <int SCHEME, int RECON, bool VISC>
+// LIM >= 0 fixes the limiter and PXYZ a fully periodic mesh at compile time
+// (the inviscid forms are built so); -1 and false read them at run time.
+template <int SCHEME, int RECON, bool VISC, int LIM, bool PXYZ>
 __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, int rows) {
     pdl_wait_then_release();
     if (!a.st->active) return;
     const Geometry& g = a.g;
     const Physics& ph = a.ph;
+    const int limiter = LIM >= 0 ? LIM : ph.limiter;
     const long long P = g.plane;
     const int lane = threadIdx.x & 31;
     const int strips = (g.nx + STRIP - 1) / STRIP;
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
         V5 uc = ldrow(jb - 1), un = ldrow(jb), pc = uc;
         if (MUSCL) {
             V5 unused;
-            slope_faces5(ph.limiter, ldrow(jb - 2), uc, un, pc, unused);
+            slope_faces5(limiter, ldrow(jb - 2), uc, un, pc, unused);
         }
         V5 gb;  // flux of the y face below row j, grid frame
         for (int j = jb - 1; j < je; ++j) {
@@ -299,11 +305,11 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
                 Q5<double> xl = xq5(ul), xr = xq5(uc);
                 if (MUSCL) {
                     V5 pp, mm;
-                    slope_faces5(ph.limiter, ul, uc, ur, pp, mm);
+                    slope_faces5(limiter, ul, uc, ur, pp, mm);
                     V5 lp = shfl_up5(pp, 1);
                     if (lane == 0) {
                         V5 unused;
-                        slope_faces5(ph.limiter, ull, ul, uc, lp, unused);
+                        slope_faces5(limiter, ull, ul, uc, lp, unused);
                     }
                     xl = xq5(rec_l ? lp : ul);
                     xr = xq5(rec_r ? mm : uc);
@@ -351,7 +357,7 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
                         V5 pl = c, mi = c;
                         if (MUSCL) {
                             V5 sp, sm;
-                            slope_faces5(ph.limiter, m, c, p, sp, sm);
+                            slope_faces5(limiter, m, c, p, sp, sm);
                             if (dk < 0 ? zrA[0] : zrA[1]) pl = sp;
                             if (dk > 0 ? zrB[1] : zrB[0]) mi = sm;
                         }
@@ -395,7 +401,7 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
             Q5<double> yb_, yt_;
             if (MUSCL) {
                 V5 mn;
-                slope_faces5(ph.limiter, uc, un, un2, pn, mn);
+                slope_faces5(limiter, uc, un, un2, pn, mn);
                 const bool lo_edge = j == -1, hi_edge = j + 1 == g.ny;
                 const bool rb = lo_edge ? seam_rec_y : (hi_edge ? edge_rec_y : true);
                 const bool rt = lo_edge ? edge_rec_y : (hi_edge ? seam_rec_y : true);
@@ -518,7 +524,7 @@ __global__ void __launch_bounds__(32 * WPB3, MINB3) stage3_kernel(StageArgs a, i
                     }
                 }
                 store5(a.uout, P, o, nwu);
-                write_ghosts3(g, ph, a.uout, i, j, k, nwu);
+                write_ghosts3<PXYZ>(g, ph, a.uout, i, j, k, nwu);
                 int bad = 0;
                 if (!(nwu.r > 0.0)) bad |= 1;
                 if (!(2.0 * nwu.E * nwu.r > nwu.mx * nwu.mx + nwu.my * nwu.my + nwu.mz * nwu.mz)) bad |= 2;
@@ -789,12 +795,35 @@ static int rows_per_warp3(int nx, int ny, int nz) {
     return (int)rows;
 }
 
-template <int SCHEME, int RECON, bool VISC>
-static void launch_stage3_t(const StageArgs& a, bool pdl, cudaStream_t s) {
+template <int SCHEME, int RECON, bool VISC, int LIM, bool PXYZ>
+static void launch_stage3_k(const StageArgs& a, bool pdl, cudaStream_t s) {
     const int rows = rows_per_warp3(a.g.nx, a.g.ny, a.g.nz);
     const long long blocks = (long long)((a.g.nx + STRIP - 1) / STRIP) * ((a.g.nz + WPB3 - 1) / WPB3);
     dim3 grid((unsigned)blocks, (a.g.ny + rows - 1) / rows);
-    launch_k(stage3_kernel<SCHEME, RECON, VISC>, grid, dim3(32 * WPB3), s, pdl, a, rows);
+    launch_k(stage3_kernel<SCHEME, RECON, VISC, LIM, PXYZ>, grid, dim3(32 * WPB3), s, pdl, a, rows);
+}
+
+// The inviscid forms are built per limiter (MUSCL) and for fully periodic
+// meshes, so those branches are decided at compile time (as the 2-D TMA-fed
+// form is); the viscous forms read them at run time.
+template <int SCHEME, int RECON, bool VISC>
+static void launch_stage3_t(const StageArgs& a, bool pdl, cudaStream_t s) {
+    if constexpr (VISC) {
+        launch_stage3_k<SCHEME, RECON, VISC, -1, false>(a, pdl, s);
+    } else {
+        const bool pxyz = a.ph.periodic_x && a.ph.periodic_y && a.ph.periodic_z;
+        if constexpr (RECON == EFVM_RECON_MUSCL) {
+            if (a.ph.limiter == EFVM_LIMITER_MC)
+                pxyz ? launch_stage3_k<SCHEME, RECON, VISC, EFVM_LIMITER_MC, true>(a, pdl, s)
+                     : launch_stage3_k<SCHEME, RECON, VISC, EFVM_LIMITER_MC, false>(a, pdl, s);
+            else
+                pxyz ? launch_stage3_k<SCHEME, RECON, VISC, EFVM_LIMITER_MINMOD, true>(a, pdl, s)
+                     : launch_stage3_k<SCHEME, RECON, VISC, EFVM_LIMITER_MINMOD, false>(a, pdl, s);
+        } else {
+            pxyz ? launch_stage3_k<SCHEME, RECON, VISC, -1, true>(a, pdl, s)
+                 : launch_stage3_k<SCHEME, RECON, VISC, -1, false>(a, pdl, s);
+        }
+    }
 }
 
 template <bool VISC>
