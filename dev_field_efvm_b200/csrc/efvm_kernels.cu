@@ -533,8 +533,9 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         // formed.  The FP32-flux forms keep them in registers.  The FP64 forms
         // keep them in shared memory, one slot per thread (12 doubles, 12 KB per
         // block): that frees 24 registers through both flux evaluations, halves
-        // the FP64 inviscid form's spills, and took the 4096^2 vortex from 2.64
-        // to 2.52 ms per step (FP32 fluxes: 1.73 -> 1.90 ms, so not there).
+        // the FP64 inviscid form's spills, and took the 4096^2 FP64 strip step
+        // from 2.73 to 2.58 ms (FP32 fluxes, TMA form: 1.73 -> 1.90 ms, so not
+        // there).
         constexpr bool CARRY_GB = FP64, CARRY_PC = FP64, CARRY_PART = FP64;
         constexpr int SLOT_GB = 0, SLOT_PC = SLOT_GB + (CARRY_GB ? 4 : 0), SLOT_PART = SLOT_PC + (CARRY_PC ? 4 : 0);
         constexpr int CARRY_SLOTS = SLOT_PART + (CARRY_PART ? 4 : 0);
@@ -545,8 +546,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         // interior face reconstructs both sides under MUSCL.  x: this lane's face,
         // between columns i-1 and i, takes column i-1's +x state (rec_l) and
         // column i's -x state (rec_r), or the cell values where they are false.
-        // y: the faces below row 0 and above row ny-1, whose flags become the
-        // slope factors of the row states (fy_below, fy_above).
+        // y: the faces below row 0 and above row ny-1 (rec_below, rec_above).
         bool rec_l = true, rec_r = true;  // face i: column i-1's +x state, column i's -x state
         if (i == 0) {
             rec_l = ph.periodic_x && true_seam;
@@ -597,7 +597,7 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
         src.release(jb - 2);
         const double dt = gld<CG>(&a.st->dt);  // set by the step's set-up, constant during the stage
         Q4<R> gb{R(0), R(0), R(0), R(0)};
-        // carry slots: 0-3 gb (r, mn, mt, E), 4-7 pc (r, mx, my, E), 8-11 the x part
+        // carry slots: gb (r, mn, mt, E), pc (r, mx, my, E), the x part (4 planes)
         auto put_gb = [&](const Q4<R>& q) {
             if constexpr (CARRY_GB) {
                 carry_s[SLOT_GB][tq] = q.r; carry_s[SLOT_GB + 1][tq] = q.mn;
