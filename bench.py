@@ -505,7 +505,8 @@ def hold_stream(n_steps):
     then never waits on the host between its events, so the events time the
     device.  Outside every timed pair of events."""
     import torch
-    torch.cuda._sleep(int(2.0e6 * max(5.0, 0.2 * n_steps)))  # ~2e6 cycles per ms
+    if hasattr(torch.cuda, "_sleep"):
+        torch.cuda._sleep(int(2.0e6 * max(5.0, 0.2 * n_steps)))  # ~2e6 cycles per ms
 
 
 def fp32_leg(args, grid, params, u, ex, flush, world, cells):
