@@ -5,7 +5,8 @@ shared-memory ring, so it is held to the same bars as the strip kernel: within
 1e-12 of the CPU oracle per cell after one RK3 step and 1e-10 after twenty (FP64),
 FP32 face fluxes within 5e-5 of the FP64 oracle after ten steps, the same bits
 for any rows per warp, and a step that commutes with a whole-cell shift of a
-periodic grid bit for bit.  The sizes cover blocks whose last strips are empty
+periodic grid bit for bit.  The kernel's builds per limiter and for fully
+periodic grids are each compared with the oracle.  The sizes cover blocks whose last strips are empty
 (nx not a multiple of 124), grids narrower than one block, and fewer rows than a
 warp marches.  Against the strip form the fields agree to 1e-13.  The autotuner
 leaves the state and the clock as it found them.
@@ -46,6 +47,29 @@ def test_periodic_vortex_matches_oracle(seam, n, ny):
     assert rel_err(d.download(), o.download()) < TOL_MANY_STEPS
     so, sd = o.solver_state(), d.solver_state()
     assert sd.step == so.step == 20 and abs(sd.time - so.time) <= 1e-13 * so.time
+
+
+@pytest.mark.parametrize("scheme,muscl,limiter", [
+    (abi.FLUX_HLLC, True, abi.LIMITER_MC),
+    (abi.FLUX_HLLC, False, abi.LIMITER_MINMOD),
+    (abi.FLUX_RUSANOV, True, abi.LIMITER_MINMOD),
+])
+def test_periodic_builds_per_limiter_and_first_order_match_oracle(scheme, muscl, limiter):
+    """The TMA-fed kernel is built per limiter and for fully periodic grids
+    (those branches decided at compile time): the MC limiter, first order and
+    Rusanov on a periodic grid run those builds, against the oracle."""
+    grid, params, u, ex = cases.vortex_case(140, periodic=True, muscl=muscl, limiter=limiter, mean=(1.0, 1.0),
+                                            cfl=0.4, ny=53)
+    params.flux_scheme = scheme
+    o = po.OracleCase(grid, params)
+    o.upload(u)
+    d = tma_context(grid, params, u)
+    o.step(1)
+    d.step(1)
+    assert rel_err(d.download(), o.download()) < TOL_ONE_STEP
+    o.step(9)
+    d.step(9)
+    assert rel_err(d.download(), o.download()) < TOL_MANY_STEPS
 
 
 @pytest.mark.parametrize("scheme,muscl,limiter", [
