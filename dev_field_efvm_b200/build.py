@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libefvm_b200.so")
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ["efvm_kernels.cu", "efvm_api.cu", "efvm_batch.cu", "efvm_nn.cu", "efvm_noalloc.cu"]
-HEADERS = ["efvm_internal.h", "efvm_math.cuh", "efvm_kernels3d.cuh", "efvm_tc.cuh", "../../include/efvm.h"]
+HEADERS = ["efvm_internal.h", "efvm_math.cuh", "efvm_kernels3d.cuh", "efvm_tc.cuh", "efvm_tma.cuh", "../../include/efvm.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
