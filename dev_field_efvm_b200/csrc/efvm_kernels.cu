@@ -886,17 +886,18 @@ __device__ __forceinline__ void stage_strip_src(const A& a, int rows, int strip,
 }
 
 // The strip code reading its rows from global memory.
-template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true, bool CG = false>
+template <int SCHEME, int RECON, class R, bool VISC, class A, bool CORR = false, bool XFIRST = true, bool CG = false,
+          int LIM = -1>
 __device__ __forceinline__ void stage_strip(const A& a, int rows, int strip, int by) {
     GlobalSrc<CG> src{a.uin, a.u0};
-    stage_strip_src<SCHEME, RECON, R, VISC, A, CORR, XFIRST, CG>(a, rows, strip, by, src);
+    stage_strip_src<SCHEME, RECON, R, VISC, A, CORR, XFIRST, CG, GlobalSrc<CG>, LIM>(a, rows, strip, by, src);
 }
 
-template <int SCHEME, int RECON, class R, int MINB, bool VISC, bool CORR = false, bool XFIRST = true>
+template <int SCHEME, int RECON, class R, int MINB, bool VISC, bool CORR = false, bool XFIRST = true, int LIM = -1>
 __global__ void __launch_bounds__(32 * WPB, MINB) stage_kernel(StageArgs a, int rows) {
     pdl_wait_then_release();
-    stage_strip<SCHEME, RECON, R, VISC, StageArgs, CORR, XFIRST>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5),
-                                                                   blockIdx.y);
+    stage_strip<SCHEME, RECON, R, VISC, StageArgs, CORR, XFIRST, false, LIM>(a, rows, blockIdx.x * WPB + (threadIdx.x >> 5),
+                                                                            blockIdx.y);
 }
 
 // The same stage with its rows fed by TMA (2-D meshes without viscous terms,
@@ -1647,6 +1648,17 @@ static void launch_stage_t(const StageArgs& a, bool pdl, cudaStream_t s) {
             launch_k(stage_kernel<SCHEME, RECON, R, F::ALT, VISC, false, F::XFIRST>, grid, block, s, pdl, a, rows);
             return;
         }
+    }
+    // the viscous MUSCL forms (the strip kernel is the only form of their cases)
+    // are built per limiter, as the TMA-fed form is
+    if constexpr (VISC && RECON == EFVM_RECON_MUSCL) {
+        if (a.ph.limiter == EFVM_LIMITER_MC)
+            launch_k(stage_kernel<SCHEME, RECON, R, F::MINB, VISC, false, F::XFIRST, EFVM_LIMITER_MC>, grid, block, s,
+                     pdl, a, rows);
+        else
+            launch_k(stage_kernel<SCHEME, RECON, R, F::MINB, VISC, false, F::XFIRST, EFVM_LIMITER_MINMOD>, grid, block,
+                     s, pdl, a, rows);
+        return;
     }
     launch_k(stage_kernel<SCHEME, RECON, R, F::MINB, VISC, false, F::XFIRST>, grid, block, s, pdl, a, rows);
 }
