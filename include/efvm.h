@@ -355,8 +355,9 @@ int efvm_profile_steps(efvm_ctx* ctx, int64_t n_steps, double out_ms[4]);
  * EFVM_STAGE_AUTO is the built-in choice: the TMA-fed form wherever the case
  * allows it (the faster of the two at 4096^2 in both precisions), else the
  * strip form.  Both give the reference's results
- * (the forms differ from each other by a few ulps at most; a form gives the
- * same bits for any rows per warp). */
+ * (the forms, and the strip form's builds for different block counts, differ
+ * from each other by a few ulps at most; a form gives the same bits for any
+ * rows per warp). */
 typedef enum { EFVM_STAGE_AUTO = 0, EFVM_STAGE_STRIP = 1, EFVM_STAGE_TMA = 2 } efvm_stage_form;
 /* Select the form, the rows each warp marches and the strip form's resident
  * blocks per SM (0 = built-in choice for each; the FP64 inviscid strip form is
